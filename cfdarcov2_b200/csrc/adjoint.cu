@@ -1,0 +1,105 @@
+// Discrete adjoint of the acoustic step on uniform meshes (speed_mode 1,
+// c_f = (c_P + c_N)/2), FP32.  With q' = q + dt A(c) q the reverse step is
+//   lam  = lam' + dt A(c)^T lam'
+//   g_c += dt (d(A(c) q)/dc)^T lam'
+// A^T is applied as a gather: each cell collects the flux sensitivities of
+// its six faces from both sides, so no scatter or atomics are needed.  Uses
+// the volume-scaled adjoint lt = lam / V (R(N) carries 1/V_N).  The same
+// arithmetic on the general geometry is plain_ops.cu's wave_adjoint_plain_k.
+#include "cfdb_internal.hpp"
+
+namespace {
+
+constexpr int kThreads = 256;
+
+struct AdjArgs {
+  int X, Y, Z;
+  long long n;
+  float A[3];  // face areas normal to x, y, z
+  float iV;    // 1 / cell volume
+  float dt;
+};
+
+__global__ void __launch_bounds__(kThreads)
+    wave_adjoint_k(AdjArgs a, const float* __restrict__ q, const float* __restrict__ lam1, float* __restrict__ lam0,
+                   const float* __restrict__ cf, float* __restrict__ gc) {
+  const long long n = a.n;
+  const long long yz = (long long)a.Y * a.Z;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int x = int(i / yz);
+    const int rem = int(i - (long long)x * yz);
+    const int y = rem / a.Z;
+    const int z = rem - y * a.Z;
+    const int coord[3] = {x, y, z};
+    const int ext[3] = {a.X, a.Y, a.Z};
+    const long long stride[3] = {yz, (long long)a.Z, 1};
+    const float cP = cf[i];
+    float lP[4], qP[4];
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+      lP[f] = lam1[f * n + i] * a.iV;
+      qP[f] = q[f * n + i];
+    }
+    float ap = 0.f, au[3] = {0.f, 0.f, 0.f}, gg = 0.f;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const float A = a.A[d];
+#pragma unroll
+      for (int side = 0; side < 2; ++side) {
+        const float s = side ? 1.f : -1.f;  // outward normal = s e_d
+        const bool wall = side ? (coord[d] == ext[d] - 1) : (coord[d] == 0);
+        if (!wall) {
+          const long long j = side ? i + stride[d] : i - stride[d];
+          const float cN = cf[j];
+          float lN[4], qN[4];
+#pragma unroll
+          for (int f = 0; f < 4; ++f) {
+            lN[f] = lam1[f * n + j] * a.iV;
+            qN[f] = q[f * n + j];
+          }
+          const float h = 0.25f * (cP + cN) * A;
+          ap += h * (lN[0] - lP[0]) + 0.5f * s * A * (lN[1 + d] - lP[1 + d]);
+          const float sp = 0.5f * (cN * cN * lN[0] - cP * cP * lP[0]);
+#pragma unroll
+          for (int e = 0; e < 3; ++e) au[e] += h * (lN[1 + e] - lP[1 + e]);
+          au[d] += sp * s * A;
+          gg -= cP * s * A * (qP[1 + d] + qN[1 + d]) * lP[0];
+          const float jp = qN[0] - qP[0];
+          float ju_self = 0.f, ju_nb = 0.f;
+#pragma unroll
+          for (int e = 0; e < 3; ++e) {
+            ju_self += (qN[1 + e] - qP[1 + e]) * lP[1 + e];
+            ju_nb += (qP[1 + e] - qN[1 + e]) * lN[1 + e];
+          }
+          gg += 0.25f * A * ((jp * lP[0] + ju_self) + (ju_nb - jp * lN[0]));
+        } else {
+          ap -= s * A * lP[1 + d];
+          au[d] -= cP * A * lP[1 + d];
+          gg -= A * qP[1 + d] * lP[1 + d];
+        }
+      }
+    }
+    lam0[i] = lam1[i] + a.dt * ap;
+#pragma unroll
+    for (int e = 0; e < 3; ++e) lam0[(1 + e) * n + i] = lam1[(1 + e) * n + i] + a.dt * au[e];
+    gc[i] += a.dt * gg;
+  }
+}
+
+}  // namespace
+
+int fused_wave_adjoint(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* q, const void* lam1, void* lam0,
+                       const void* c, void* gc, double dt) {
+  (void)dtype;
+  AdjArgs a;
+  a.X = int(m->nx); a.Y = int(m->ny); a.Z = int(m->nz);
+  a.n = (long long)m->n;
+  a.A[0] = float(m->dy * m->dz); a.A[1] = float(m->dx * m->dz); a.A[2] = float(m->dx * m->dy);
+  a.iV = float(1.0 / (m->dx * m->dy * m->dz));
+  a.dt = float(dt);
+  wave_adjoint_k<<<grid_for(ctx, m->n, kThreads, 8), kThreads, 0, ctx->stream>>>(
+      a, static_cast<const float*>(q), static_cast<const float*>(lam1), static_cast<float*>(lam0),
+      static_cast<const float*>(c), static_cast<float*>(gc));
+  CFDB_LAUNCHED(ctx);
+  return CFDB_OK;
+}

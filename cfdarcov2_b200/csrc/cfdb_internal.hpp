@@ -1,0 +1,139 @@
+// Internal declarations shared by the host runtime and the kernel files of
+// libcfdb.  Nothing here is part of the C ABI (include/cfdb.h).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "cfdb.h"
+
+// ---------------------------------------------------------------------------
+// Host-side geometry in double: the reference's flattened N x 6 arrays
+// (entry (i, f) at f*n + i; per-dimension arrays stacked d*6n + f*n + i).
+// ---------------------------------------------------------------------------
+struct HostGeom {
+  int64_t nx = 0, ny = 0, nz = 0, n = 0;
+  std::vector<double> normal, normal_alt;  // 3 * 6n
+  std::vector<double> area, alpha, len;    // 6n
+  std::vector<double> volume, center, isb; // n, 3n, n
+  std::vector<int64_t> ids, ibf;           // 6n
+};
+
+// Builds HostGeom (geometry.cpp).  verts may be null (uniform lattice).  mode:
+// 0 reference formulas, 1 reference with component-sum areas, 2 exact vector
+// areas (default of vertex meshes).  Returns false if memory runs out.
+bool cfdb_build_geometry(HostGeom& g, int64_t nx, int64_t ny, int64_t nz, double dx, double dy, double dz,
+                         const double* verts, int mode);
+
+// Device copy of the geometry for the plain (per-operator) kernels in one
+// precision.  ids are int32 (self on boundary faces, as the reference's _ids).
+struct PlainGeomDev {
+  bool ready = false;
+  void* normal = nullptr;      // 3 * 6n
+  void* normal_alt = nullptr;  // 3 * 6n
+  void* area = nullptr;        // 6n
+  void* alpha = nullptr;       // 6n
+  void* len = nullptr;         // 6n
+  void* volume = nullptr;      // n
+  void* isb = nullptr;         // n
+  void* stab_tmp = nullptr;    // 3 * 6n, allocated on first stab call
+};
+
+// Compact FP32 geometry of vertex meshes for the fused gather kernels: the
+// outward area vector of each cell's +x/+y/+z face (the -faces are the
+// neighbours' +faces negated), 1/V, and the area vectors of the boundary
+// faces on the -x/-y/-z walls.
+struct CompactGeomDev {
+  bool ready = false;
+  float* S = nullptr;      // 9n: [Sx.x|Sx.y|Sx.z|Sy.x|...|Sz.z]
+  float* inv_vol = nullptr;
+  float* wall_x = nullptr; // 3 * ny*nz  (cells x = 0, index y*nz+z)
+  float* wall_y = nullptr; // 3 * nx*nz  (cells y = 0, index x*nz+z)
+  float* wall_z = nullptr; // 3 * nx*ny  (cells z = 0, index x*ny+y)
+};
+
+struct cfdb_ctx {
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  int64_t budget = 0;
+  int64_t allocated = 0;
+  std::unordered_map<void*, int64_t> allocs;
+  int* d_error = nullptr;  // device error word written by bounded waits
+};
+
+struct cfdb_mesh {
+  cfdb_ctx* ctx = nullptr;
+  int64_t nx = 0, ny = 0, nz = 0, n = 0;
+  double dx = 0, dy = 0, dz = 0;
+  bool uniform = true;
+  int geom_mode = 0;  // see cfdb_build_geometry
+  std::vector<double> verts;  // vertex meshes only
+  std::unique_ptr<HostGeom> geom;
+  int32_t* d_ids = nullptr;
+  PlainGeomDev plain[2];
+  CompactGeomDev compact;
+};
+
+// ---- error plumbing --------------------------------------------------------
+int cfdb_fail(cfdb_ctx* ctx, int code, const char* fmt, ...);
+int cfdb_cuda_fail(cfdb_ctx* ctx, cudaError_t e, const char* what);
+
+#define CFDB_CUDA(ctx, call)                                       \
+  do {                                                             \
+    cudaError_t e__ = (call);                                      \
+    if (e__ != cudaSuccess) return cfdb_cuda_fail((ctx), e__, #call); \
+  } while (0)
+
+// Checks for a launch error right after a kernel launch.
+#define CFDB_LAUNCHED(ctx) CFDB_CUDA(ctx, cudaGetLastError())
+
+// ---- memory ---------------------------------------------------------------
+int cfdb_dev_alloc(cfdb_ctx* ctx, int64_t bytes, void** out);
+void cfdb_dev_free(cfdb_ctx* ctx, void* p);
+
+// ---- geometry helpers ------------------------------------------------------
+int cfdb_mesh_need_host_geom(cfdb_mesh* m);
+int cfdb_mesh_need_plain(cfdb_mesh* m, int dtype);
+int cfdb_mesh_need_compact(cfdb_mesh* m);
+
+inline size_t dtype_size(int dtype) { return dtype == CFDB_F64 ? 8 : 4; }
+inline bool dtype_ok(int dtype) { return dtype == CFDB_F32 || dtype == CFDB_F64; }
+
+int cfdb_check_mesh(cfdb_ctx* ctx, cfdb_mesh* m);
+
+// ---- launchers implemented in the kernel files ------------------------------
+// plain_ops.cu
+int plain_lapl(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* phi, void* out, int mask);
+int plain_heat_update(cfdb_ctx* ctx, int dtype, const void* L, const void* T, double k, double dt, void* Tn,
+                      int64_t n);
+int plain_wave_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* q, void* qn, const void* c,
+                    double cconst, int mode, double dt);
+int plain_wave_adjoint(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* q, const void* lam1, void* lam0,
+                       const void* c, void* gc, double dt);
+// fused_tma.cu
+int fused_heat_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* T, void* Tn, double k, double dt);
+int fused_wave_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* q, void* qn, const void* c,
+                    double cconst, int mode, double dt);
+// distorted.cu
+int compact_wave_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* q, void* qn, const void* c,
+                      double cconst, int mode, double dt);
+// adjoint.cu
+int fused_wave_adjoint(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* q, const void* lam1, void* lam0,
+                       const void* c, void* gc, double dt);
+
+// Shared launch-size helper: a grid-stride grid of at most `per_sm` CTAs per SM.
+inline int grid_for(const cfdb_ctx* ctx, int64_t n, int threads, int per_sm = 8) {
+  int64_t want = (n + threads - 1) / threads;
+  int64_t cap = int64_t(ctx->num_sms > 0 ? ctx->num_sms : 148) * per_sm;
+  if (want > cap) want = cap;
+  if (want < 1) want = 1;
+  return int(want);
+}

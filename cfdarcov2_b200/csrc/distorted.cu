@@ -1,0 +1,107 @@
+// Fused acoustic step on vertex (distorted) meshes.  Geometry is the compact
+// FP32 form built by cfdb_mesh_need_compact: per cell the outward area
+// vectors S = n_alt A of its +x/+y/+z faces and 1/V (40 B/cell); the -faces
+// are the neighbours' +faces negated (the reference computes one normal and
+// one area per face object and gives the two cells opposite outward normals,
+// src/mesh3d.cpp:69-105), boundary -faces come from three wall tables.
+// Warps cover consecutive z cells, so every neighbour gather is a coalesced
+// row segment.
+#include "cfdb_internal.hpp"
+
+namespace {
+
+constexpr int kThreads = 256;
+
+struct CompactArgs {
+  const float* __restrict__ S;
+  const float* __restrict__ iv;
+  const float* __restrict__ wx;
+  const float* __restrict__ wy;
+  const float* __restrict__ wz;
+  int X, Y, Z;
+  long long n;
+};
+
+__global__ void __launch_bounds__(kThreads)
+    compact_wave_k(CompactArgs g, const float* __restrict__ q, float* __restrict__ qn, const float* __restrict__ cf,
+                   float cconst, int mode, float dt) {
+  const long long n = g.n;
+  const long long yz = (long long)g.Y * g.Z;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int x = int(i / yz);
+    const int rem = int(i - (long long)x * yz);
+    const int y = rem / g.Z;
+    const int z = rem - y * g.Z;
+    const float pP = q[i], uP = q[n + i], vP = q[2 * n + i], wP = q[3 * n + i];
+    const float cP = cf ? cf[i] : cconst;
+    const float c2 = cP * cP;
+    float ap = 0.f, au = 0.f, av = 0.f, aw = 0.f;
+    const long long stride[3] = {yz, (long long)g.Z, 1};
+    const int coord[3] = {x, y, z};
+    const int ext[3] = {g.X, g.Y, g.Z};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+#pragma unroll
+      for (int side = 0; side < 2; ++side) {
+        float Sx, Sy, Sz;
+        bool wall;
+        long long j;
+        if (side == 1) {  // +face: own area vector
+          Sx = g.S[(3 * d + 0) * n + i]; Sy = g.S[(3 * d + 1) * n + i]; Sz = g.S[(3 * d + 2) * n + i];
+          wall = coord[d] == ext[d] - 1;
+          j = i + stride[d];
+        } else {          // -face: neighbour's +face negated, or the wall table
+          wall = coord[d] == 0;
+          j = i - stride[d];
+          if (!wall) {
+            Sx = -g.S[(3 * d + 0) * n + j]; Sy = -g.S[(3 * d + 1) * n + j]; Sz = -g.S[(3 * d + 2) * n + j];
+          } else {
+            const float* w = d == 0 ? g.wx : (d == 1 ? g.wy : g.wz);
+            const long long cnt = d == 0 ? yz : (d == 1 ? (long long)g.X * g.Z : (long long)g.X * g.Y);
+            const long long k = d == 0 ? (long long)y * g.Z + z : (d == 1 ? (long long)x * g.Z + z : (long long)x * g.Y + y);
+            Sx = w[k]; Sy = w[cnt + k]; Sz = w[2 * cnt + k];
+          }
+        }
+        const float A = sqrtf(Sx * Sx + Sy * Sy + Sz * Sz);
+        const float unPA = uP * Sx + vP * Sy + wP * Sz;
+        float pN, uN, vN, wN, cN;
+        if (!wall) {
+          pN = q[j]; uN = q[n + j]; vN = q[2 * n + j]; wN = q[3 * n + j];
+          cN = cf ? cf[j] : cconst;
+        } else {
+          const float k2 = 2.f * unPA / (A * A);  // reflect about the unit normal S/A
+          pN = pP; uN = uP - k2 * Sx; vN = vP - k2 * Sy; wN = wP - k2 * Sz; cN = cP;
+        }
+        const float unNA = uN * Sx + vN * Sy + wN * Sz;
+        const float cfc = mode == 0 ? fmaxf(cP, cN) : 0.5f * (cP + cN);
+        const float hA = 0.5f * cfc * A;
+        const float pm = 0.5f * (pP + pN);
+        ap += c2 * 0.5f * (unPA + unNA) - hA * (pN - pP);
+        au += pm * Sx - hA * (uN - uP);
+        av += pm * Sy - hA * (vN - vP);
+        aw += pm * Sz - hA * (wN - wP);
+      }
+    }
+    const float s = -dt * g.iv[i];
+    qn[i] = pP + s * ap;
+    qn[n + i] = uP + s * au;
+    qn[2 * n + i] = vP + s * av;
+    qn[3 * n + i] = wP + s * aw;
+  }
+}
+
+}  // namespace
+
+int compact_wave_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* q, void* qn, const void* c, double cconst,
+                      int mode, double dt) {
+  if (dtype != CFDB_F32)
+    return cfdb_fail(ctx, CFDB_EUNSUPPORTED, "the fused vertex-mesh wave step computes in float32 only");
+  if (int rc = cfdb_mesh_need_compact(m)) return rc;
+  const CompactGeomDev& cg = m->compact;
+  CompactArgs a{cg.S, cg.inv_vol, cg.wall_x, cg.wall_y, cg.wall_z, int(m->nx), int(m->ny), int(m->nz), (long long)m->n};
+  compact_wave_k<<<grid_for(ctx, m->n, kThreads, 8), kThreads, 0, ctx->stream>>>(
+      a, static_cast<const float*>(q), static_cast<float*>(qn), static_cast<const float*>(c), float(cconst), mode,
+      float(dt));
+  CFDB_LAUNCHED(ctx);
+  return CFDB_OK;
+}

@@ -1,0 +1,343 @@
+// Compressible Euler solver object (cfdb_euler_*) and its fused FP32 step:
+// one TMA sweep per step (tma_stencil.cuh) that reads the device clock, does
+// the Rusanov update of all five conserved fields in one HBM pass and, in its
+// epilogue, reduces the new state's per-direction signal speeds (for the next
+// dt) and its FP64 Neumaier totals.  The plain path lives in euler_plain.cu.
+#include <cmath>
+#include <new>
+
+#include "euler_internal.hpp"
+#include "tma_host.hpp"
+
+namespace {
+
+__device__ __forceinline__ double bits_to_double(unsigned long long b) { return __longlong_as_double((long long)b); }
+
+__device__ __forceinline__ void comp_add(double& s, double& c, double x) {
+  const double t = s + x;
+  if (fabs(s) >= fabs(x)) c += (s - t) + x; else c += (x - t) + s;
+  s = t;
+}
+
+struct EulerPhys {
+  static constexpr int NF = 5;
+  static constexpr bool HAS_C = false;
+  struct Params {
+    float ih[3];
+    float gamma;
+    float dt;  // filled per launch by begin()
+    double dx, dy, dz, cfl, t_end, vconst;
+    EulerClock* clock;
+    double* totals;
+    Comp2* part;
+    long long s;
+    long long max_steps;
+  };
+  struct Acc {
+    float l[3];
+    double s0, c0, s1, c1;
+  };
+
+  __device__ static bool first_thread() {
+    return blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0;
+  }
+
+  __device__ static bool begin(Params& p) {
+    EulerClock* ck = p.clock;
+    const int ts = int(p.s & 1);
+    if (ck->finished[ts]) {
+      if (first_thread()) {
+        ck->t[ts ^ 1] = ck->t[ts];
+        ck->steps[ts ^ 1] = ck->steps[ts];
+        ck->finished[ts ^ 1] = 1;
+      }
+      return false;
+    }
+    if (first_thread()) {
+      const int z = int((p.s + 2) % 3);
+      ck->lam[z][0] = ck->lam[z][1] = ck->lam[z][2] = 0ull;
+    }
+    const int ls = int(p.s % 3);
+    const double lam[3] = {bits_to_double(ck->lam[ls][0]), bits_to_double(ck->lam[ls][1]),
+                           bits_to_double(ck->lam[ls][2])};
+    bool last;
+    p.dt = float(euler_dt(lam, p.dx, p.dy, p.dz, p.cfl, ck->t[ts], p.t_end, &last));
+    return true;
+  }
+
+  // zero-gradient at the x ends, reflective walls in y and z
+  __device__ static void ghost(float g[NF], const float q[NF], int dir) {
+#pragma unroll
+    for (int f = 0; f < NF; ++f) g[f] = q[f];
+    if (dir != 0) g[1 + dir] = -q[1 + dir];
+  }
+
+  __device__ static void prim(const float q[NF], float gm1, float gamma, float& ir, float u[3], float& p, float& a) {
+    ir = 1.0f / q[0];
+    u[0] = q[1] * ir; u[1] = q[2] * ir; u[2] = q[3] * ir;
+    p = gm1 * (q[4] - 0.5f * (q[1] * u[0] + q[2] * u[1] + q[3] * u[2]));
+    a = sqrtf(gamma * p * ir);
+  }
+
+  __device__ static void cell(const float P[NF], const float nb[6][NF], const float*, const Params& a, float o[NF]) {
+    const float gm1 = a.gamma - 1.0f;
+    float irP, uP[3], pP, aP;
+    prim(P, gm1, a.gamma, irP, uP, pP, aP);
+    float acc[NF] = {0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+#pragma unroll
+      for (int side = 0; side < 2; ++side) {
+        const float* N = nb[2 * d + side];
+        const float sg = side ? 1.0f : -1.0f;
+        float irN, uN[3], pN, aN;
+        prim(N, gm1, a.gamma, irN, uN, pN, aN);
+        const float unP = sg * uP[d], unN = sg * uN[d];
+        const float hl = 0.5f * fmaxf(fabsf(uP[d]) + aP, fabsf(uN[d]) + aN);
+        float f[NF];
+        f[0] = 0.5f * (P[0] * unP + N[0] * unN) - hl * (N[0] - P[0]);
+#pragma unroll
+        for (int e = 0; e < 3; ++e) f[1 + e] = 0.5f * (P[1 + e] * unP + N[1 + e] * unN) - hl * (N[1 + e] - P[1 + e]);
+        f[1 + d] += 0.5f * sg * (pP + pN);
+        f[4] = 0.5f * ((P[4] + pP) * unP + (N[4] + pN) * unN) - hl * (N[4] - P[4]);
+        const float ih = a.ih[d];
+#pragma unroll
+        for (int c = 0; c < NF; ++c) acc[c] += f[c] * ih;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < NF; ++c) o[c] = P[c] - a.dt * acc[c];
+  }
+
+  __device__ static void acc_init(Acc& s) {
+    s.l[0] = s.l[1] = s.l[2] = 0.f;
+    s.s0 = s.c0 = s.s1 = s.c1 = 0.0;
+  }
+
+  __device__ static void acc_cell(Acc& s, const float o[NF], const Params& a) {
+    float ir, u[3], p, c;
+    prim(o, a.gamma - 1.0f, a.gamma, ir, u, p, c);
+    s.l[0] = fmaxf(s.l[0], fabsf(u[0]) + c);
+    s.l[1] = fmaxf(s.l[1], fabsf(u[1]) + c);
+    s.l[2] = fmaxf(s.l[2], fabsf(u[2]) + c);
+    comp_add(s.s0, s.c0, double(o[0]) * a.vconst);
+    comp_add(s.s1, s.c1, double(o[4]) * a.vconst);
+  }
+
+  __device__ static void finish(Acc& s, const Params& a, bool) {
+    __shared__ double sh[32][4];
+    __shared__ float shl[32][3];
+    __shared__ bool is_last;
+    for (int o = 16; o > 0; o >>= 1) {
+      s.l[0] = fmaxf(s.l[0], __shfl_xor_sync(0xffffffffu, s.l[0], o));
+      s.l[1] = fmaxf(s.l[1], __shfl_xor_sync(0xffffffffu, s.l[1], o));
+      s.l[2] = fmaxf(s.l[2], __shfl_xor_sync(0xffffffffu, s.l[2], o));
+      const double a0 = __shfl_xor_sync(0xffffffffu, s.s0, o), b0 = __shfl_xor_sync(0xffffffffu, s.c0, o);
+      const double a1 = __shfl_xor_sync(0xffffffffu, s.s1, o), b1 = __shfl_xor_sync(0xffffffffu, s.c1, o);
+      comp_add(s.s0, s.c0, a0); s.c0 += b0;
+      comp_add(s.s1, s.c1, a1); s.c1 += b1;
+    }
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+      sh[w][0] = s.s0; sh[w][1] = s.c0; sh[w][2] = s.s1; sh[w][3] = s.c1;
+      shl[w][0] = s.l[0]; shl[w][1] = s.l[1]; shl[w][2] = s.l[2];
+    }
+    __syncthreads();
+    EulerClock* ck = a.clock;
+    const unsigned nblocks = gridDim.x * gridDim.y;
+    const unsigned bid = blockIdx.y * gridDim.x + blockIdx.x;
+    if (threadIdx.x == 0) {
+      double S0 = 0, C0 = 0, S1 = 0, C1 = 0;
+      float L0 = 0, L1 = 0, L2 = 0;
+      for (int k = 0; k < int(blockDim.x / 32); ++k) {
+        comp_add(S0, C0, sh[k][0]); C0 += sh[k][1];
+        comp_add(S1, C1, sh[k][2]); C1 += sh[k][3];
+        L0 = fmaxf(L0, shl[k][0]); L1 = fmaxf(L1, shl[k][1]); L2 = fmaxf(L2, shl[k][2]);
+      }
+      a.part[bid] = Comp2{S0, C0, S1, C1};
+      const int target = int((a.s + 1) % 3);
+      atomicMax(&ck->lam[target][0], (unsigned long long)__double_as_longlong(double(L0)));
+      atomicMax(&ck->lam[target][1], (unsigned long long)__double_as_longlong(double(L1)));
+      atomicMax(&ck->lam[target][2], (unsigned long long)__double_as_longlong(double(L2)));
+      __threadfence();
+      is_last = atomicAdd(&ck->counter, 1u) == nblocks - 1;
+    }
+    __syncthreads();
+    if (is_last && threadIdx.x == 0) {
+      __threadfence();
+      double S0 = 0, C0 = 0, S1 = 0, C1 = 0;
+      for (unsigned k = 0; k < nblocks; ++k) {
+        const Comp2 q = a.part[k];
+        comp_add(S0, C0, q.s0); C0 += q.c0;
+        comp_add(S1, C1, q.s1); C1 += q.c1;
+      }
+      ck->counter = 0;
+      const int ts = int(a.s & 1);
+      const int ls = int(a.s % 3);
+      const double lam[3] = {bits_to_double(ck->lam[ls][0]), bits_to_double(ck->lam[ls][1]),
+                             bits_to_double(ck->lam[ls][2])};
+      bool last;
+      const double t = ck->t[ts];
+      const double dt = euler_dt(lam, a.dx, a.dy, a.dz, a.cfl, t, a.t_end, &last);
+      const long long step = ck->steps[ts] + 1;
+      ck->t[ts ^ 1] = last ? a.t_end : t + dt;
+      ck->steps[ts ^ 1] = step;
+      ck->finished[ts ^ 1] = (last || !(t + dt < a.t_end) || step >= a.max_steps) ? 1 : 0;
+      a.totals[2 * step] = S0 + C0;
+      a.totals[2 * step + 1] = S1 + C1;
+    }
+  }
+};
+
+constexpr int kEulerCtasPerSm = 2;
+
+template <int TZ>
+int launch_euler(cfdb_euler* e, const void* U, void* Un, int64_t s) {
+  cfdb_mesh* m = e->mesh;
+  EulerPhys::Params p;
+  p.ih[0] = float(1.0 / m->dx); p.ih[1] = float(1.0 / m->dy); p.ih[2] = float(1.0 / m->dz);
+  p.gamma = float(e->gamma);
+  p.dt = 0.f;
+  p.dx = m->dx; p.dy = m->dy; p.dz = m->dz;
+  p.cfl = e->cfl; p.t_end = e->t_end; p.vconst = m->dx * m->dy * m->dz;
+  p.clock = e->clock; p.totals = e->totals; p.part = e->part;
+  p.s = (long long)s;
+  p.max_steps = (long long)e->max_steps;
+  return stencil::launch_sweep<EulerPhys, TZ, 8, 4>(e->ctx, m, U, Un, nullptr, p, kEulerCtasPerSm);
+}
+
+int tz_for(const cfdb_mesh* m) { return m->nz >= 128 ? 128 : (m->nz >= 64 ? 64 : 32); }
+
+}  // namespace
+
+int euler_fused_grid(const cfdb_euler* e) {
+  const int tz = tz_for(e->mesh);
+  const stencil::SweepShape sh = stencil::sweep_shape(e->ctx, e->mesh, tz, 8, kEulerCtasPerSm);
+  return sh.tiles * sh.chunks;
+}
+
+int euler_fused_step(cfdb_euler* e, const void* U, void* Un, int64_t s) {
+  switch (tz_for(e->mesh)) {
+    case 128: return launch_euler<128>(e, U, Un, s);
+    case 64: return launch_euler<64>(e, U, Un, s);
+    default: return launch_euler<32>(e, U, Un, s);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// object API
+// ---------------------------------------------------------------------------
+extern "C" int cfdb_euler_create(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, int path, double gamma, double cfl,
+                                 double t_end, int64_t max_steps, cfdb_euler** out) {
+  if (!out) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_euler_create: out is NULL");
+  *out = nullptr;
+  if (int rc = cfdb_check_mesh(ctx, m)) return rc;
+  if (!dtype_ok(dtype)) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_euler_create: unknown dtype %d", dtype);
+  if (path != CFDB_PATH_PLAIN && path != CFDB_PATH_FUSED)
+    return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_euler_create: unknown path %d", path);
+  if (!(gamma > 1.0) || !(cfl > 0.0) || !(t_end > 0.0) || !std::isfinite(t_end) || max_steps < 1)
+    return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_euler_create: need gamma > 1, cfl > 0, finite t_end > 0, max_steps >= 1");
+  if (path == CFDB_PATH_FUSED) {
+    if (dtype != CFDB_F32) return cfdb_fail(ctx, CFDB_EUNSUPPORTED, "the fused Euler step computes in float32 only");
+    if (int rc = stencil::check_sweep(ctx, m, {})) return rc;
+  }
+  CFDB_CUDA(ctx, cudaSetDevice(ctx->device));
+  auto* e = new (std::nothrow) cfdb_euler();
+  if (!e) return cfdb_fail(ctx, CFDB_ENOMEM, "host allocation failed");
+  e->ctx = ctx; e->mesh = m; e->dtype = dtype; e->path = path;
+  e->gamma = gamma; e->cfl = cfl; e->t_end = t_end; e->max_steps = max_steps;
+  const int grid = std::max(euler_reduce_grid(e), path == CFDB_PATH_FUSED ? euler_fused_grid(e) : 0);
+  e->part_cap = grid;
+  int rc = cfdb_dev_alloc(ctx, sizeof(EulerClock), reinterpret_cast<void**>(&e->clock));
+  if (!rc) rc = cfdb_dev_alloc(ctx, int64_t(sizeof(double)) * 2 * (max_steps + 1), reinterpret_cast<void**>(&e->totals));
+  if (!rc) rc = cfdb_dev_alloc(ctx, int64_t(sizeof(Comp2)) * grid, reinterpret_cast<void**>(&e->part));
+  if (rc) {
+    cfdb_euler_destroy(e);
+    return rc;
+  }
+  cudaMemsetAsync(e->clock, 0, sizeof(EulerClock), ctx->stream);
+  *out = e;
+  return CFDB_OK;
+}
+
+extern "C" int cfdb_euler_destroy(cfdb_euler* e) {
+  if (!e) return CFDB_OK;
+  cudaStreamSynchronize(e->ctx->stream);
+  cfdb_dev_free(e->ctx, e->clock);
+  cfdb_dev_free(e->ctx, e->totals);
+  cfdb_dev_free(e->ctx, e->part);
+  delete e;
+  return CFDB_OK;
+}
+
+extern "C" int cfdb_euler_begin(cfdb_euler* e, const void* U0) {
+  if (!e) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_euler_begin: handle is NULL");
+  if (!U0) return cfdb_fail(e->ctx, CFDB_EINVAL, "cfdb_euler_begin: U0 is NULL");
+  if (e->path == CFDB_PATH_FUSED && (reinterpret_cast<uintptr_t>(U0) & 15u))
+    return cfdb_fail(e->ctx, CFDB_EINVAL, "the fused Euler path needs 16-byte aligned states");
+  CFDB_CUDA(e->ctx, cudaSetDevice(e->ctx->device));
+  CFDB_CUDA(e->ctx, cudaMemsetAsync(e->clock, 0, sizeof(EulerClock), e->ctx->stream));
+  e->launches = 0;
+  return euler_reduce(e, U0, 0, 1);
+}
+
+extern "C" int cfdb_euler_step(cfdb_euler* e, const void* U, void* Un) {
+  if (!e) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_euler_step: handle is NULL");
+  if (!U || !Un || U == Un) return cfdb_fail(e->ctx, CFDB_EINVAL, "cfdb_euler_step: need distinct U and U_next");
+  CFDB_CUDA(e->ctx, cudaSetDevice(e->ctx->device));
+  const int64_t s = e->launches;
+  int rc = e->path == CFDB_PATH_FUSED ? euler_fused_step(e, U, Un, s) : euler_plain_step(e, U, Un, s);
+  if (rc) return rc;
+  e->launches = s + 1;
+  return CFDB_OK;
+}
+
+extern "C" int cfdb_euler_status(cfdb_euler* e, double* t, int64_t* steps_done, int* finished) {
+  if (!e) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_euler_status: handle is NULL");
+  EulerClock ck;
+  CFDB_CUDA(e->ctx, cudaMemcpyAsync(&ck, e->clock, sizeof(ck), cudaMemcpyDeviceToHost, e->ctx->stream));
+  CFDB_CUDA(e->ctx, cudaStreamSynchronize(e->ctx->stream));
+  int err = 0;
+  CFDB_CUDA(e->ctx, cudaMemcpy(&err, e->ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err) {
+    cudaMemset(e->ctx->d_error, 0, sizeof(int));
+    return cfdb_fail(e->ctx, CFDB_ETIMEOUT, "a bounded device wait gave up (error word %d)", err);
+  }
+  const int sl = euler_slot(e->launches);
+  if (t) *t = ck.t[sl];
+  if (steps_done) *steps_done = ck.steps[sl];
+  if (finished) *finished = ck.finished[sl];
+  return CFDB_OK;
+}
+
+extern "C" int cfdb_euler_totals(cfdb_euler* e, double* out, int64_t max_rows, int64_t* rows) {
+  if (!e || !out || max_rows < 0) return cfdb_fail(e ? e->ctx : nullptr, CFDB_EINVAL, "cfdb_euler_totals: bad arguments");
+  int64_t steps = 0;
+  if (int rc = cfdb_euler_status(e, nullptr, &steps, nullptr)) return rc;
+  const int64_t n = std::min<int64_t>(steps + 1, max_rows);
+  if (n > 0) CFDB_CUDA(e->ctx, cudaMemcpy(out, e->totals, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost));
+  if (rows) *rows = n;
+  return CFDB_OK;
+}
+
+extern "C" int cfdb_euler_run(cfdb_euler* e, void* Ua, void* Ub, int64_t check_every, int64_t* steps_done,
+                              int* final_in_b) {
+  if (!e) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_euler_run: handle is NULL");
+  if (!Ua || !Ub || Ua == Ub || check_every < 1)
+    return cfdb_fail(e->ctx, CFDB_EINVAL, "cfdb_euler_run: need distinct buffers and check_every >= 1");
+  if (e->launches & 1) return cfdb_fail(e->ctx, CFDB_EINVAL, "cfdb_euler_run: call after cfdb_euler_begin or an even number of steps");
+  int finished = 0;
+  int64_t steps = 0;
+  while (!finished) {
+    for (int64_t k = 0; k < check_every; ++k) {
+      const bool even = (e->launches & 1) == 0;
+      if (int rc = cfdb_euler_step(e, even ? Ua : Ub, even ? Ub : Ua)) return rc;
+    }
+    if (int rc = cfdb_euler_status(e, nullptr, &steps, &finished)) return rc;
+    if (!finished && e->launches > e->max_steps + check_every)
+      return cfdb_fail(e->ctx, CFDB_ENUMERIC, "cfdb_euler_run: the clock did not reach t_end within max_steps");
+  }
+  if (steps_done) *steps_done = steps;
+  if (final_in_b) *final_in_b = int(steps & 1);
+  return CFDB_OK;
+}

@@ -1,0 +1,446 @@
+// Host runtime of libcfdb: contexts, errors, device memory, meshes and their
+// geometry uploads.  Replaces CFDArcoGlobalInit (src/cfdarcho_main_3d.cpp),
+// CudaDataMatrix + the RMM pool (include/cuda_data_matrix.hpp,
+// include/pool_allocator.hpp) and CudaMesh3D::host_to_device
+// (include/mesh3d.hpp:209-236) with library-owned buffers, status codes and
+// no per-step allocation.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "cfdb_internal.hpp"
+
+namespace {
+thread_local std::string g_err_noctx;
+
+std::string vformat(const char* fmt, va_list ap) {
+  char buf[1024];
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  return std::string(buf);
+}
+}  // namespace
+
+int cfdb_fail(cfdb_ctx* ctx, int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  std::string s = vformat(fmt, ap);
+  va_end(ap);
+  if (ctx) ctx->err = s; else g_err_noctx = s;
+  return code;
+}
+
+int cfdb_cuda_fail(cfdb_ctx* ctx, cudaError_t e, const char* what) {
+  cudaGetLastError();  // clear a sticky-free error so the next call starts clean
+  return cfdb_fail(ctx, e == cudaErrorMemoryAllocation ? CFDB_ENOMEM : CFDB_ECUDA, "%s: %s (%s)", what,
+                   cudaGetErrorString(e), cudaGetErrorName(e));
+}
+
+int cfdb_dev_alloc(cfdb_ctx* ctx, int64_t bytes, void** out) {
+  *out = nullptr;
+  if (bytes <= 0) bytes = 16;
+  if (ctx->budget > 0 && ctx->allocated + bytes > ctx->budget)
+    return cfdb_fail(ctx, CFDB_ENOMEM, "allocation of %lld bytes exceeds the context budget (%lld of %lld used)",
+                     (long long)bytes, (long long)ctx->allocated, (long long)ctx->budget);
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, size_t(bytes));
+  if (e != cudaSuccess) return cfdb_cuda_fail(ctx, e, "cudaMalloc");
+  ctx->allocs[p] = bytes;
+  ctx->allocated += bytes;
+  *out = p;
+  return CFDB_OK;
+}
+
+void cfdb_dev_free(cfdb_ctx* ctx, void* p) {
+  if (!p || !ctx) return;
+  auto it = ctx->allocs.find(p);
+  if (it != ctx->allocs.end()) {
+    ctx->allocated -= it->second;
+    ctx->allocs.erase(it);
+  }
+  cudaFree(p);
+}
+
+extern "C" int cfdb_abi_version(void) { return CFDB_ABI_VERSION; }
+
+extern "C" int cfdb_ctx_create(int device, cfdb_ctx** out) {
+  if (!out) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_ctx_create: out is NULL");
+  *out = nullptr;
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess) return cfdb_cuda_fail(nullptr, e, "cudaGetDeviceCount");
+  if (device < 0 || device >= count)
+    return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_ctx_create: device %d out of range (%d devices)", device, count);
+  e = cudaSetDevice(device);
+  if (e != cudaSuccess) return cfdb_cuda_fail(nullptr, e, "cudaSetDevice");
+  auto* ctx = new (std::nothrow) cfdb_ctx();
+  if (!ctx) return cfdb_fail(nullptr, CFDB_ENOMEM, "cfdb_ctx_create: host allocation failed");
+  ctx->device = device;
+  cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+  int rc = cfdb_dev_alloc(ctx, sizeof(int) * 4, reinterpret_cast<void**>(&ctx->d_error));
+  if (rc) {
+    g_err_noctx = ctx->err;
+    delete ctx;
+    return rc;
+  }
+  e = cudaMemset(ctx->d_error, 0, sizeof(int) * 4);
+  if (e != cudaSuccess) {
+    int r = cfdb_cuda_fail(nullptr, e, "cudaMemset");
+    delete ctx;
+    return r;
+  }
+  *out = ctx;
+  return CFDB_OK;
+}
+
+extern "C" int cfdb_ctx_destroy(cfdb_ctx* ctx) {
+  if (!ctx) return CFDB_OK;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  for (auto& kv : ctx->allocs) cudaFree(kv.first);
+  ctx->allocs.clear();
+  delete ctx;
+  return CFDB_OK;
+}
+
+extern "C" const char* cfdb_last_error(const cfdb_ctx* ctx) {
+  return ctx ? ctx->err.c_str() : g_err_noctx.c_str();
+}
+
+extern "C" int cfdb_ctx_set_stream(cfdb_ctx* ctx, void* stream) {
+  if (!ctx) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_ctx_set_stream: ctx is NULL");
+  ctx->stream = static_cast<cudaStream_t>(stream);
+  return CFDB_OK;
+}
+
+extern "C" int cfdb_sync(cfdb_ctx* ctx) {
+  if (!ctx) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_sync: ctx is NULL");
+  CFDB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return CFDB_OK;
+}
+
+extern "C" int cfdb_ctx_set_alloc_budget(cfdb_ctx* ctx, int64_t bytes) {
+  if (!ctx || bytes < 0) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_ctx_set_alloc_budget: bad arguments");
+  ctx->budget = bytes;
+  return CFDB_OK;
+}
+
+extern "C" int cfdb_ctx_allocated_bytes(const cfdb_ctx* ctx, int64_t* out) {
+  if (!ctx || !out) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_ctx_allocated_bytes: bad arguments");
+  *out = ctx->allocated;
+  return CFDB_OK;
+}
+
+extern "C" int cfdb_alloc(cfdb_ctx* ctx, int64_t bytes, void** out) {
+  if (!ctx || !out || bytes < 0) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_alloc: bad arguments");
+  return cfdb_dev_alloc(ctx, bytes, out);
+}
+
+extern "C" int cfdb_free(cfdb_ctx* ctx, void* ptr) {
+  if (!ctx) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_free: ctx is NULL");
+  if (ptr && !ctx->allocs.count(ptr)) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_free: pointer not owned by ctx");
+  cudaStreamSynchronize(ctx->stream);
+  cfdb_dev_free(ctx, ptr);
+  return CFDB_OK;
+}
+
+extern "C" int cfdb_upload(cfdb_ctx* ctx, void* dst, const void* src, int64_t bytes) {
+  if (!ctx || !dst || !src || bytes < 0) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_upload: bad arguments");
+  CFDB_CUDA(ctx, cudaMemcpyAsync(dst, src, size_t(bytes), cudaMemcpyHostToDevice, ctx->stream));
+  CFDB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return CFDB_OK;
+}
+
+extern "C" int cfdb_download(cfdb_ctx* ctx, void* dst, const void* src, int64_t bytes) {
+  if (!ctx || !dst || !src || bytes < 0) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_download: bad arguments");
+  CFDB_CUDA(ctx, cudaMemcpyAsync(dst, src, size_t(bytes), cudaMemcpyDeviceToHost, ctx->stream));
+  CFDB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return CFDB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// meshes
+// ---------------------------------------------------------------------------
+namespace {
+int check_dims(cfdb_ctx* ctx, int64_t nx, int64_t ny, int64_t nz, double dx, double dy, double dz) {
+  if (nx < 1 || ny < 1 || nz < 1)
+    return cfdb_fail(ctx, CFDB_EINVAL, "mesh dimensions must be >= 1 (got %lld x %lld x %lld)", (long long)nx,
+                     (long long)ny, (long long)nz);
+  if (!(dx > 0) || !(dy > 0) || !(dz > 0) || !std::isfinite(dx) || !std::isfinite(dy) || !std::isfinite(dz))
+    return cfdb_fail(ctx, CFDB_EINVAL, "mesh spacings must be finite and > 0");
+  const double cells = double(nx) * double(ny) * double(nz);
+  if (cells > double(INT32_MAX))
+    return cfdb_fail(ctx, CFDB_EINVAL, "mesh of %.0f cells exceeds the 2^31-1 cell limit of int32 indexing", cells);
+  return CFDB_OK;
+}
+}  // namespace
+
+extern "C" int cfdb_mesh_create_structured(cfdb_ctx* ctx, int64_t nx, int64_t ny, int64_t nz, double dx,
+                                           double dy, double dz, cfdb_mesh** out) {
+  if (!out) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_mesh_create_structured: out is NULL");
+  *out = nullptr;
+  if (int rc = check_dims(ctx, nx, ny, nz, dx, dy, dz)) return rc;
+  auto* m = new (std::nothrow) cfdb_mesh();
+  if (!m) return cfdb_fail(ctx, CFDB_ENOMEM, "host allocation failed");
+  m->ctx = ctx;
+  m->nx = nx; m->ny = ny; m->nz = nz; m->n = nx * ny * nz;
+  m->dx = dx; m->dy = dy; m->dz = dz;
+  m->uniform = true;
+  *out = m;
+  return CFDB_OK;
+}
+
+extern "C" int cfdb_mesh_create_from_vertices(cfdb_ctx* ctx, int64_t nx, int64_t ny, int64_t nz, double dx,
+                                              double dy, double dz, const double* vertices, int flags,
+                                              cfdb_mesh** out) {
+  if (!out || !vertices) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_mesh_create_from_vertices: NULL argument");
+  *out = nullptr;
+  if (int rc = check_dims(ctx, nx, ny, nz, dx, dy, dz)) return rc;
+  if (flags & ~CFDB_MESH_COMPAT_AREA) return cfdb_fail(ctx, CFDB_EINVAL, "unknown mesh flags 0x%x", flags);
+  const int64_t nv = (nx + 1) * (ny + 1) * (nz + 1);
+  for (int64_t k = 0; k < 3 * nv; ++k)
+    if (!std::isfinite(vertices[k])) return cfdb_fail(ctx, CFDB_EINVAL, "vertex coordinate %lld is not finite", (long long)k);
+  auto* m = new (std::nothrow) cfdb_mesh();
+  if (!m) return cfdb_fail(ctx, CFDB_ENOMEM, "host allocation failed");
+  m->ctx = ctx;
+  m->nx = nx; m->ny = ny; m->nz = nz; m->n = nx * ny * nz;
+  m->dx = dx; m->dy = dy; m->dz = dz;
+  m->uniform = false;
+  m->geom_mode = (flags & CFDB_MESH_COMPAT_AREA) ? 1 : 2;
+  try {
+    m->verts.assign(vertices, vertices + 3 * nv);
+  } catch (const std::bad_alloc&) {
+    delete m;
+    return cfdb_fail(ctx, CFDB_ENOMEM, "host allocation failed");
+  }
+  if (int rc = cfdb_mesh_need_host_geom(m)) {
+    delete m;
+    return rc;
+  }
+  // Reject tangled cells.  The outward normal comes from a sign test against
+  // the cell centre (src/mesh3d.cpp:84-88), so the volume stays positive even
+  // when a face has folded over; instead every face's outward normal must lie
+  // on its topological side: along the unsigned normal for the +x/+y/+z slots
+  // (1, 3, 5), against it for the -slots (0, 2, 4).
+  {
+    const HostGeom& g = *m->geom;
+    const int64_t n = m->n;
+    for (int64_t i = 0; i < n; ++i) {
+      bool ok = g.volume[i] > 0;
+      for (int f = 0; f < 6 && ok; ++f) {
+        const int64_t k6 = int64_t(f) * n + i;
+        const double d = g.normal_alt[k6] * g.normal[k6] + g.normal_alt[6 * n + k6] * g.normal[6 * n + k6] +
+                         g.normal_alt[12 * n + k6] * g.normal[12 * n + k6];
+        ok = (f & 1) ? d > 0 : d < 0;
+      }
+      if (!ok) {
+        delete m;
+        return cfdb_fail(ctx, CFDB_EINVAL, "cell %lld is tangled (a face normal or the volume is inverted)",
+                         (long long)i);
+      }
+    }
+  }
+  *out = m;
+  return CFDB_OK;
+}
+
+static void free_plain(cfdb_ctx* ctx, PlainGeomDev& p) {
+  void** ptrs[] = {&p.normal, &p.normal_alt, &p.area, &p.alpha, &p.len, &p.volume, &p.isb, &p.stab_tmp};
+  for (void** q : ptrs) {
+    cfdb_dev_free(ctx, *q);
+    *q = nullptr;
+  }
+  p.ready = false;
+}
+
+extern "C" int cfdb_mesh_destroy(cfdb_mesh* m) {
+  if (!m) return CFDB_OK;
+  if (m->ctx) {
+    cudaStreamSynchronize(m->ctx->stream);
+    free_plain(m->ctx, m->plain[0]);
+    free_plain(m->ctx, m->plain[1]);
+    cfdb_dev_free(m->ctx, m->d_ids);
+    CompactGeomDev& c = m->compact;
+    float** ptrs[] = {&c.S, &c.inv_vol, &c.wall_x, &c.wall_y, &c.wall_z};
+    for (float** q : ptrs) cfdb_dev_free(m->ctx, *q);
+  }
+  delete m;
+  return CFDB_OK;
+}
+
+extern "C" int cfdb_mesh_info(const cfdb_mesh* m, int64_t dims[3], double spacing[3], int* is_uniform) {
+  if (!m) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_mesh_info: mesh is NULL");
+  if (dims) { dims[0] = m->nx; dims[1] = m->ny; dims[2] = m->nz; }
+  if (spacing) { spacing[0] = m->dx; spacing[1] = m->dy; spacing[2] = m->dz; }
+  if (is_uniform) *is_uniform = m->uniform ? 1 : 0;
+  return CFDB_OK;
+}
+
+int cfdb_mesh_need_host_geom(cfdb_mesh* m) {
+  if (m->geom) return CFDB_OK;
+  auto g = std::unique_ptr<HostGeom>(new (std::nothrow) HostGeom());
+  if (!g) return cfdb_fail(m->ctx, CFDB_ENOMEM, "host allocation failed");
+  if (!cfdb_build_geometry(*g, m->nx, m->ny, m->nz, m->dx, m->dy, m->dz, m->uniform ? nullptr : m->verts.data(),
+                           m->geom_mode))
+    return cfdb_fail(m->ctx, CFDB_ENOMEM, "host geometry of %lld cells does not fit in host memory", (long long)m->n);
+  m->geom = std::move(g);
+  return CFDB_OK;
+}
+
+extern "C" int cfdb_mesh_geometry(const cfdb_mesh* cm, int which, double* out) {
+  cfdb_mesh* m = const_cast<cfdb_mesh*>(cm);
+  if (!m || !out) return cfdb_fail(m ? m->ctx : nullptr, CFDB_EINVAL, "cfdb_mesh_geometry: NULL argument");
+  if (int rc = cfdb_mesh_need_host_geom(m)) return rc;
+  const HostGeom& g = *m->geom;
+  const std::vector<double>* src = nullptr;
+  switch (which) {
+    case CFDB_GEOM_NORMAL: src = &g.normal; break;
+    case CFDB_GEOM_NORMAL_ALT: src = &g.normal_alt; break;
+    case CFDB_GEOM_AREA: src = &g.area; break;
+    case CFDB_GEOM_ALPHA_D: src = &g.alpha; break;
+    case CFDB_GEOM_LEN_C2F: src = &g.len; break;
+    case CFDB_GEOM_VOLUME: src = &g.volume; break;
+    case CFDB_GEOM_CENTER: src = &g.center; break;
+    case CFDB_GEOM_IS_BOUNDARY: src = &g.isb; break;
+    default: return cfdb_fail(m->ctx, CFDB_EINVAL, "cfdb_mesh_geometry: unknown array %d", which);
+  }
+  std::memcpy(out, src->data(), sizeof(double) * src->size());
+  return CFDB_OK;
+}
+
+extern "C" int cfdb_mesh_ids(const cfdb_mesh* cm, int64_t* ids, int64_t* ibf) {
+  cfdb_mesh* m = const_cast<cfdb_mesh*>(cm);
+  if (!m) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_mesh_ids: mesh is NULL");
+  if (int rc = cfdb_mesh_need_host_geom(m)) return rc;
+  if (ids) std::memcpy(ids, m->geom->ids.data(), sizeof(int64_t) * 6 * m->n);
+  if (ibf) std::memcpy(ibf, m->geom->ibf.data(), sizeof(int64_t) * 6 * m->n);
+  return CFDB_OK;
+}
+
+int cfdb_check_mesh(cfdb_ctx* ctx, cfdb_mesh* m) {
+  if (!ctx) return cfdb_fail(nullptr, CFDB_EINVAL, "ctx is NULL");
+  if (!m) return cfdb_fail(ctx, CFDB_EINVAL, "mesh is NULL");
+  if (m->ctx != ctx) return cfdb_fail(ctx, CFDB_EINVAL, "mesh belongs to another context (or is host-only)");
+  return CFDB_OK;
+}
+
+namespace {
+template <class T>
+int upload_as(cfdb_ctx* ctx, const double* src, int64_t count, void** dst) {
+  std::vector<T> tmp;
+  try {
+    tmp.resize(size_t(count));
+  } catch (const std::bad_alloc&) {
+    return cfdb_fail(ctx, CFDB_ENOMEM, "host staging allocation failed");
+  }
+  for (int64_t k = 0; k < count; ++k) tmp[k] = T(src[k]);
+  if (int rc = cfdb_dev_alloc(ctx, int64_t(sizeof(T)) * count, dst)) return rc;
+  CFDB_CUDA(ctx, cudaMemcpy(*dst, tmp.data(), sizeof(T) * size_t(count), cudaMemcpyHostToDevice));
+  return CFDB_OK;
+}
+}  // namespace
+
+int cfdb_mesh_need_plain(cfdb_mesh* m, int dtype) {
+  PlainGeomDev& p = m->plain[dtype == CFDB_F64 ? 1 : 0];
+  if (p.ready) return CFDB_OK;
+  if (int rc = cfdb_mesh_need_host_geom(m)) return rc;
+  const HostGeom& g = *m->geom;
+  cfdb_ctx* ctx = m->ctx;
+  if (!m->d_ids) {
+    std::vector<int32_t> ids(size_t(6 * m->n));
+    for (int64_t k = 0; k < 6 * m->n; ++k) ids[k] = int32_t(g.ids[k]);
+    if (int rc = cfdb_dev_alloc(ctx, int64_t(sizeof(int32_t)) * 6 * m->n, reinterpret_cast<void**>(&m->d_ids)))
+      return rc;
+    CFDB_CUDA(ctx, cudaMemcpy(m->d_ids, ids.data(), sizeof(int32_t) * ids.size(), cudaMemcpyHostToDevice));
+  }
+  auto up = [&](const std::vector<double>& v, void** dst) {
+    return dtype == CFDB_F64 ? upload_as<double>(ctx, v.data(), int64_t(v.size()), dst)
+                             : upload_as<float>(ctx, v.data(), int64_t(v.size()), dst);
+  };
+  int rc = CFDB_OK;
+  if (!rc) rc = up(g.normal, &p.normal);
+  if (!rc) rc = up(g.normal_alt, &p.normal_alt);
+  if (!rc) rc = up(g.area, &p.area);
+  if (!rc) rc = up(g.alpha, &p.alpha);
+  if (!rc) rc = up(g.len, &p.len);
+  if (!rc) rc = up(g.volume, &p.volume);
+  if (!rc) rc = up(g.isb, &p.isb);
+  if (rc) {
+    free_plain(ctx, p);
+    return rc;
+  }
+  p.ready = true;
+  return CFDB_OK;
+}
+
+int cfdb_mesh_need_compact(cfdb_mesh* m) {
+  CompactGeomDev& c = m->compact;
+  if (c.ready) return CFDB_OK;
+  if (int rc = cfdb_mesh_need_host_geom(m)) return rc;
+  const HostGeom& g = *m->geom;
+  const int64_t n = m->n, nx = m->nx, ny = m->ny, nz = m->nz;
+  std::vector<double> S(static_cast<size_t>(9 * n)), iv(static_cast<size_t>(n));
+  std::vector<double> wx(static_cast<size_t>(3 * ny * nz)), wy(static_cast<size_t>(3 * nx * nz));
+  std::vector<double> wz(static_cast<size_t>(3 * nx * ny));
+  // +x face = slot 5, +y = slot 3, +z = slot 1; wall -x = 4, -y = 2, -z = 0
+  const int plus_slot[3] = {5, 3, 1};
+  for (int64_t i = 0; i < n; ++i) {
+    for (int d = 0; d < 3; ++d) {
+      const int64_t k6 = int64_t(plus_slot[d]) * n + i;
+      for (int c3 = 0; c3 < 3; ++c3) S[(3 * d + c3) * n + i] = g.normal_alt[c3 * 6 * n + k6] * g.area[k6];
+    }
+    iv[i] = 1.0 / g.volume[i];
+  }
+  for (int64_t y = 0; y < ny; ++y)
+    for (int64_t z = 0; z < nz; ++z) {
+      const int64_t i = nz * y + z, k6 = 4 * n + i;
+      for (int c3 = 0; c3 < 3; ++c3) wx[c3 * ny * nz + (y * nz + z)] = g.normal_alt[c3 * 6 * n + k6] * g.area[k6];
+    }
+  for (int64_t x = 0; x < nx; ++x)
+    for (int64_t z = 0; z < nz; ++z) {
+      const int64_t i = nz * ny * x + z, k6 = 2 * n + i;
+      for (int c3 = 0; c3 < 3; ++c3) wy[c3 * nx * nz + (x * nz + z)] = g.normal_alt[c3 * 6 * n + k6] * g.area[k6];
+    }
+  for (int64_t x = 0; x < nx; ++x)
+    for (int64_t y = 0; y < ny; ++y) {
+      const int64_t i = nz * ny * x + nz * y, k6 = 0 * n + i;
+      for (int c3 = 0; c3 < 3; ++c3) wz[c3 * nx * ny + (x * ny + y)] = g.normal_alt[c3 * 6 * n + k6] * g.area[k6];
+    }
+  cfdb_ctx* ctx = m->ctx;
+  int rc = upload_as<float>(ctx, S.data(), int64_t(S.size()), reinterpret_cast<void**>(&c.S));
+  if (!rc) rc = upload_as<float>(ctx, iv.data(), int64_t(iv.size()), reinterpret_cast<void**>(&c.inv_vol));
+  if (!rc) rc = upload_as<float>(ctx, wx.data(), int64_t(wx.size()), reinterpret_cast<void**>(&c.wall_x));
+  if (!rc) rc = upload_as<float>(ctx, wy.data(), int64_t(wy.size()), reinterpret_cast<void**>(&c.wall_y));
+  if (!rc) rc = upload_as<float>(ctx, wz.data(), int64_t(wz.size()), reinterpret_cast<void**>(&c.wall_z));
+  if (rc) return rc;
+  c.ready = true;
+  return CFDB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// wave dt (host; setup-time)
+// ---------------------------------------------------------------------------
+extern "C" int cfdb_wave_dt(const cfdb_mesh* cm, const double* c_host, double c_const, double cfl, double* dt_out) {
+  cfdb_mesh* m = const_cast<cfdb_mesh*>(cm);
+  if (!m || !dt_out || !(cfl > 0)) return cfdb_fail(m ? m->ctx : nullptr, CFDB_EINVAL, "cfdb_wave_dt: bad arguments");
+  if (m->uniform && !c_host) {
+    if (!(c_const > 0)) return cfdb_fail(m->ctx, CFDB_EINVAL, "cfdb_wave_dt: c must be > 0");
+    // 2V / sum_f c A_f = 1 / (c (1/dx + 1/dy + 1/dz)) on a uniform mesh
+    const double s = (c_const / m->dx + c_const / m->dy) + c_const / m->dz;
+    *dt_out = cfl / s;
+    return CFDB_OK;
+  }
+  if (int rc = cfdb_mesh_need_host_geom(m)) return rc;
+  const HostGeom& g = *m->geom;
+  double best = INFINITY;
+  for (int64_t i = 0; i < m->n; ++i) {
+    const double c = c_host ? c_host[i] : c_const;
+    if (!(c > 0)) return cfdb_fail(m->ctx, CFDB_EINVAL, "cfdb_wave_dt: c[%lld] must be > 0", (long long)i);
+    double s = 0;
+    for (int f = 0; f < 6; ++f) s += c * g.area[int64_t(f) * m->n + i];
+    best = std::min(best, 2.0 * g.volume[i] / s);
+  }
+  *dt_out = cfl * best;
+  return CFDB_OK;
+}

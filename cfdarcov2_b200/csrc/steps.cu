@@ -1,0 +1,53 @@
+// Entry points of the time steps: argument checks and dispatch between the
+// plain (per-operator, general geometry) and fused paths.
+#include "cfdb_internal.hpp"
+
+namespace {
+
+int check_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, int path, const char* fn) {
+  if (int rc = cfdb_check_mesh(ctx, m)) return rc;
+  if (!dtype_ok(dtype)) return cfdb_fail(ctx, CFDB_EINVAL, "%s: unknown dtype %d", fn, dtype);
+  if (path != CFDB_PATH_PLAIN && path != CFDB_PATH_FUSED) return cfdb_fail(ctx, CFDB_EINVAL, "%s: unknown path %d", fn, path);
+  CFDB_CUDA(ctx, cudaSetDevice(ctx->device));
+  return CFDB_OK;
+}
+
+}  // namespace
+
+extern "C" int cfdb_heat_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, int path, const void* T, void* Tn, double k,
+                              double dt) {
+  if (int rc = check_step(ctx, m, dtype, path, "cfdb_heat_step")) return rc;
+  if (!T || !Tn) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_heat_step: NULL field pointer");
+  if (T == Tn) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_heat_step: T and T_next must differ (no in-place stencil writes)");
+  if (!std::isfinite(k) || !std::isfinite(dt)) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_heat_step: k and dt must be finite");
+  if (path == CFDB_PATH_FUSED) return fused_heat_step(ctx, m, dtype, T, Tn, k, dt);
+  if (int rc = cfdb_mesh_need_plain(m, dtype)) return rc;
+  PlainGeomDev& p = m->plain[dtype == CFDB_F64 ? 1 : 0];
+  if (!p.stab_tmp)
+    if (int rc = cfdb_dev_alloc(ctx, int64_t(dtype_size(dtype)) * 18 * m->n, &p.stab_tmp)) return rc;
+  if (int rc = plain_lapl(ctx, m, dtype, T, p.stab_tmp, 7)) return rc;
+  return plain_heat_update(ctx, dtype, p.stab_tmp, T, k, dt, Tn, m->n);
+}
+
+extern "C" int cfdb_wave_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, int path, const void* q, void* qn,
+                              const void* c, double cconst, int mode, double dt) {
+  if (int rc = check_step(ctx, m, dtype, path, "cfdb_wave_step")) return rc;
+  if (!q || !qn) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_wave_step: NULL state pointer");
+  if (q == qn) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_wave_step: q and q_next must differ (no in-place stencil writes)");
+  if (mode != 0 && mode != 1) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_wave_step: speed_mode must be 0 or 1");
+  if (!c && !(cconst > 0)) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_wave_step: c_const must be > 0");
+  if (!std::isfinite(dt)) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_wave_step: dt must be finite");
+  if (path == CFDB_PATH_PLAIN) return plain_wave_step(ctx, m, dtype, q, qn, c, cconst, mode, dt);
+  if (m->uniform) return fused_wave_step(ctx, m, dtype, q, qn, c, cconst, mode, dt);
+  return compact_wave_step(ctx, m, dtype, q, qn, c, cconst, mode, dt);
+}
+
+extern "C" int cfdb_wave_adjoint_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, int path, const void* q,
+                                      const void* lam1, void* lam0, const void* c, void* gc, double dt) {
+  if (int rc = check_step(ctx, m, dtype, path, "cfdb_wave_adjoint_step")) return rc;
+  if (!q || !lam1 || !lam0 || !c || !gc) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_wave_adjoint_step: NULL pointer");
+  if (lam1 == lam0) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_wave_adjoint_step: lam_next and lam_n must differ");
+  if (path == CFDB_PATH_FUSED && m->uniform && dtype == CFDB_F32)
+    return fused_wave_adjoint(ctx, m, dtype, q, lam1, lam0, c, gc, dt);
+  return plain_wave_adjoint(ctx, m, dtype, q, lam1, lam0, c, gc, dt);
+}

@@ -1,0 +1,117 @@
+// Host side of the TMA stencil sweep: tensor-map encoding through the driver
+// entry point (no libcuda link), tile/chunk selection and the launch.
+#pragma once
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "cfdb_internal.hpp"
+#include "tma_stencil.cuh"
+
+namespace stencil {
+
+inline PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// 4-D map over a float32 state of nf fields stored field after field:
+// dims (z, y, x, field), box (TZ+8, TY+2, 1, nf).
+inline int encode_state(cfdb_ctx* ctx, CUtensorMap* map, const void* base, const cfdb_mesh* m, int nf, int tz,
+                        int ty) {
+  auto fn = encode_fn();
+  if (!fn) return cfdb_fail(ctx, CFDB_ECUDA, "cuTensorMapEncodeTiled entry point unavailable");
+  cuuint64_t dims[4] = {cuuint64_t(m->nz), cuuint64_t(m->ny), cuuint64_t(m->nx), cuuint64_t(nf)};
+  cuuint64_t strides[3] = {cuuint64_t(m->nz) * 4, cuuint64_t(m->nz * m->ny) * 4, cuuint64_t(m->n) * 4};
+  cuuint32_t box[4] = {cuuint32_t(tz + 8), cuuint32_t(ty + 2), 1, cuuint32_t(nf)};
+  cuuint32_t es[4] = {1, 1, 1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<void*>(base), dims, strides, box, es,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return cfdb_fail(ctx, CFDB_ECUDA, "cuTensorMapEncodeTiled (state) failed with %d", int(r));
+  return CFDB_OK;
+}
+
+// 3-D map over one float32 field: dims (z, y, x), box (TZ+8, TY+2, 1).
+inline int encode_field(cfdb_ctx* ctx, CUtensorMap* map, const void* base, const cfdb_mesh* m, int tz, int ty) {
+  auto fn = encode_fn();
+  if (!fn) return cfdb_fail(ctx, CFDB_ECUDA, "cuTensorMapEncodeTiled entry point unavailable");
+  cuuint64_t dims[3] = {cuuint64_t(m->nz), cuuint64_t(m->ny), cuuint64_t(m->nx)};
+  cuuint64_t strides[2] = {cuuint64_t(m->nz) * 4, cuuint64_t(m->nz * m->ny) * 4};
+  cuuint32_t box[3] = {cuuint32_t(tz + 8), cuuint32_t(ty + 2), 1};
+  cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void*>(base), dims, strides, box, es,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return cfdb_fail(ctx, CFDB_ECUDA, "cuTensorMapEncodeTiled (field) failed with %d", int(r));
+  return CFDB_OK;
+}
+
+// Checks the layout requirements of the sweep.
+inline int check_sweep(cfdb_ctx* ctx, const cfdb_mesh* m, std::initializer_list<const void*> ptrs) {
+  if (!m->uniform) return cfdb_fail(ctx, CFDB_EUNSUPPORTED, "the TMA sweep needs a uniform (structured) mesh");
+  if (m->nz % 4 != 0)
+    return cfdb_fail(ctx, CFDB_EUNSUPPORTED,
+                     "the TMA sweep needs nz %% 4 == 0 (16-byte rows); nz = %lld: use CFDB_PATH_PLAIN",
+                     (long long)m->nz);
+  if (m->nx > 2147483647LL / 2) return cfdb_fail(ctx, CFDB_EUNSUPPORTED, "mesh too large for int32 TMA coordinates");
+  for (const void* p : ptrs)
+    if (p && (reinterpret_cast<uintptr_t>(p) & 15u))
+      return cfdb_fail(ctx, CFDB_EINVAL, "the TMA sweep needs 16-byte aligned field pointers");
+  return CFDB_OK;
+}
+
+struct SweepShape {
+  int tiles, chunks, chunk;
+};
+
+// Chunks along x so that the grid covers ~ctas_per_sm CTAs per SM.
+inline SweepShape sweep_shape(const cfdb_ctx* ctx, const cfdb_mesh* m, int tz, int ty, int ctas_per_sm) {
+  SweepShape s;
+  s.tiles = int(((m->nz + tz - 1) / tz) * ((m->ny + ty - 1) / ty));
+  const int target = std::max(1, ctx->num_sms) * ctas_per_sm;
+  int chunks = std::max(1, (target + s.tiles - 1) / s.tiles);
+  chunks = int(std::min<int64_t>(chunks, m->nx));
+  chunks = std::min(chunks, 65535);
+  s.chunk = int((m->nx + chunks - 1) / chunks);
+  s.chunks = int((m->nx + s.chunk - 1) / s.chunk);
+  return s;
+}
+
+template <class Phys, int TZ, int TY, int S>
+int launch_sweep(cfdb_ctx* ctx, const cfdb_mesh* m, const void* q, void* out, const void* c,
+                 const typename Phys::Params& prm, int ctas_per_sm, int* launched_grid = nullptr) {
+  using L = Layout<TZ, TY, S, Phys::NF, Phys::HAS_C>;
+  CUtensorMap tq, tc;
+  if (int rc = encode_state(ctx, &tq, q, m, Phys::NF, TZ, TY)) return rc;
+  if constexpr (Phys::HAS_C) {
+    if (int rc = encode_field(ctx, &tc, c, m, TZ, TY)) return rc;
+  } else {
+    tc = tq;
+  }
+  auto kern = sweep_kernel<Phys, TZ, TY, S>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    CFDB_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L::SMEM_BYTES)));
+    attr_set = true;
+  }
+  const SweepShape sh = sweep_shape(ctx, m, TZ, TY, ctas_per_sm);
+  Geometry g{int(m->nx), int(m->ny), int(m->nz), sh.chunk, (long long)m->n};
+  dim3 grid(sh.tiles, sh.chunks);
+  kern<<<grid, L::THREADS, L::SMEM_BYTES, ctx->stream>>>(tq, tc, g, static_cast<float*>(out), prm, ctx->d_error);
+  CFDB_LAUNCHED(ctx);
+  if (launched_grid) *launched_grid = sh.tiles * sh.chunks;
+  return CFDB_OK;
+}
+
+}  // namespace stencil

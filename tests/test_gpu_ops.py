@@ -1,0 +1,253 @@
+"""GPU parity of the plain operator layer and the heat / wave time steps
+against the CPU oracle, through the C ABI.
+
+Bars: FP64 plain path bit-identical to the FP64 oracle (the north-star bar
+is 1e-12 relative; identical operation order makes it exact); FP32 plain
+path bit-identical to the FP32 oracle on power-of-two uniform meshes; FP32
+fused path within L2 relative error 1e-5 of the FP64 oracle."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_l2, rel_linf
+
+pytestmark = pytest.mark.gpu
+
+DEV = "cuda:0"
+
+
+def dev(a, dtype):
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype, device=DEV)
+
+
+def host(t):
+    torch.cuda.synchronize()
+    return t.detach().cpu().numpy()
+
+
+MESHES = [
+    dict(shape=(5, 6, 7), spacing=(0.2, 1 / 6, 1 / 7), verts=None),
+    dict(shape=(8, 8, 8), spacing=(1 / 8, 1 / 8, 1 / 8), verts=None),
+    dict(shape=(6, 6, 6), spacing=(1 / 6, 1 / 6, 1 / 6), verts="jitter"),
+]
+
+
+def make_pair(cfdb, oracle, ctx, spec, np_dtype):
+    from cfdarcov2_b200.workloads import jittered_vertices
+    shape, spacing = spec["shape"], spec["spacing"]
+    if spec["verts"] == "jitter":
+        V = jittered_vertices(shape[0], seed=2)
+        return (cfdb.Mesh.from_vertices(ctx, *shape, *spacing, V),
+                oracle.Mesh(*shape, *spacing, vertices=V, dtype=np_dtype))
+    return cfdb.Mesh.structured(ctx, *shape, *spacing), oracle.Mesh(*shape, *spacing, dtype=np_dtype)
+
+
+@pytest.mark.parametrize("spec", MESHES, ids=["aniso", "cube8", "jitter6"])
+@pytest.mark.parametrize("op", ["grad", "lapl", "stab"])
+@pytest.mark.parametrize("mask", [7, 1, 6])
+def test_plain_operators_fp64_bitwise(cfdb, oracle, ctx, spec, op, mask):
+    m, o = make_pair(cfdb, oracle, ctx, spec, np.float64)
+    rng = np.random.default_rng(7)
+    phi = rng.standard_normal(m.n)
+    got = host(getattr(ctx, op)(m, dev(phi, torch.float64), mask=mask))
+    ref = getattr(o, op)(phi, mask)
+    assert np.array_equal(got, ref), np.abs(got - ref).max()
+
+
+@pytest.mark.parametrize("op", ["grad", "lapl", "stab"])
+def test_plain_operators_fp32_bitwise_on_pow2_mesh(cfdb, oracle, ctx, op):
+    m, o = make_pair(cfdb, oracle, ctx, MESHES[1], np.float32)
+    rng = np.random.default_rng(8)
+    phi = rng.standard_normal(m.n).astype(np.float32)
+    got = host(getattr(ctx, op)(m, dev(phi, torch.float32)))
+    ref = getattr(o, op)(phi)
+    assert np.array_equal(got, ref), np.abs(got - ref).max()
+
+
+def test_elementwise_and_time_operators(cfdb, ctx):
+    cap = cfdb.capi
+    rng = np.random.default_rng(9)
+    for tdt, ndt in [(torch.float64, np.float64), (torch.float32, np.float32)]:
+        a = rng.standard_normal(1000).astype(ndt)
+        b = (rng.uniform(0.5, 2, 1000)).astype(ndt)
+        ta, tb = dev(a, tdt), dev(b, tdt)
+        assert np.array_equal(host(ctx.binary(cap.OP_ADD, ta, tb)), a + b)
+        assert np.array_equal(host(ctx.binary(cap.OP_SUB, ta, tb)), a - b)
+        assert np.array_equal(host(ctx.binary(cap.OP_MUL, ta, tb)), a * b)
+        assert np.array_equal(host(ctx.binary(cap.OP_DIV, ta, tb)), a / b)
+        s = ndt(0.37)
+        assert np.array_equal(host(ctx.scalar(cap.OP_MUL, ta, float(s))), a * s)
+        assert np.array_equal(host(ctx.scalar(cap.OP_RSUB, ta, float(s))), s - a)
+        assert np.array_equal(host(ctx.scalar(cap.OP_RDIV, tb, float(s))), s / b)
+        assert np.array_equal(host(ctx.neg(ta)), -a)
+        assert np.all(host(ctx.fill(torch.empty_like(ta), 2.5)) == 2.5)
+        dt = ndt(0.01)
+        assert np.array_equal(host(ctx.d1t(ta, tb, float(dt))), dt * a + b)
+        c = rng.standard_normal(1000).astype(ndt)
+        tc = dev(c, tdt)
+        assert np.array_equal(host(ctx.d2t(ta, tb, tc, float(dt), 1)), (dt * dt * a + ndt(2) * b) - c)
+        assert np.array_equal(host(ctx.d2t(ta, tb, None, float(dt), 0)), dt * a + b)
+
+
+def test_boundary_copy_and_cfl(cfdb, oracle, ctx):
+    m = cfdb.Mesh.structured(ctx, 6, 5, 4, 0.1, 0.2, 0.3)
+    o = oracle.Mesh(6, 5, 4, 0.1, 0.2, 0.3)
+    rng = np.random.default_rng(10)
+    arr, cp = rng.standard_normal(m.n), rng.standard_normal(m.n)
+    isb = o.geometry()["is_boundary"]
+    got = host(ctx.boundary_copy(m, dev(arr, torch.float64), dev(cp, torch.float64)))
+    assert np.array_equal(got, arr * (1 - isb) + cp * isb)
+    p, rho = rng.uniform(0.5, 2, m.n), rng.uniform(0.5, 2, m.n)
+    u, v, w = rng.standard_normal((3, m.n))
+    d = lambda x: dev(x, torch.float64)  # noqa: E731
+    assert ctx.cfl_dt(m, 0.4, 5 / 3, d(p), d(rho), d(u), d(v), d(w)) == o.cfl_reference(0.4, 5 / 3, p, rho, u, v, w)
+    assert ctx.cfl_dt(m, 0.4, 5 / 3, d(p), d(rho), d(u)) == o.cfl_reference(0.4, 5 / 3, p, rho, u)
+
+
+def test_total_fp64(cfdb, oracle, ctx):
+    m = cfdb.Mesh.structured(ctx, 32, 16, 8, 1 / 32, 1 / 16, 1 / 8)
+    o = oracle.Mesh(32, 16, 8, 1 / 32, 1 / 16, 1 / 8)
+    rng = np.random.default_rng(11)
+    f = rng.uniform(0, 1, m.n)
+    assert ctx.total_fp64(m, dev(f, torch.float64)) == pytest.approx(o.total(f), rel=1e-14)
+    f32 = f.astype(np.float32)
+    assert ctx.total_fp64(m, dev(f32, torch.float32)) == pytest.approx(o.total(f32.astype(np.float64)), rel=1e-14)
+
+
+def run_steps(step, a, b, steps):
+    for _ in range(steps):
+        step(a, b)
+        a, b = b, a
+    return a
+
+
+def test_heat_plain_fp64_matches_oracle_bitwise_config1(cfdb, oracle, ctx):
+    """The heat workload (64^3, k = 0.01, dt = 0.1 dx^2/k, 200 steps) on the
+    FP64 plain path is bit-identical to the FP64 oracle (bar: 1e-12 rel)."""
+    from cfdarcov2_b200.workloads import heat_config
+    cfg = heat_config()
+    n = cfg["n"]
+    m = cfdb.Mesh.structured(ctx, n, n, n, cfg["dx"], cfg["dx"], cfg["dx"])
+    o = oracle.Mesh(n, n, n, cfg["dx"], cfg["dx"], cfg["dx"])
+    a = dev(cfg["T0"], torch.float64)
+    b = torch.empty_like(a)
+    out = run_steps(lambda x, y: ctx.heat_step(m, x, y, cfg["k"], cfg["dt"], path=cfdb.PLAIN), a, b, cfg["steps"])
+    ref = o.heat_solve(cfg["T0"], cfg["k"], cfg["dt"], cfg["steps"])
+    got = host(out)
+    assert rel_linf(got, ref) <= 1e-12
+    assert np.array_equal(got, ref)
+
+
+def test_heat_fused_fp32_within_tolerance(cfdb, oracle, ctx):
+    from cfdarcov2_b200.workloads import heat_config
+    cfg = heat_config(n=32, steps=100)
+    n = cfg["n"]
+    m = cfdb.Mesh.structured(ctx, n, n, n, cfg["dx"], cfg["dx"], cfg["dx"])
+    o = oracle.Mesh(n, n, n, cfg["dx"], cfg["dx"], cfg["dx"])
+    a = dev(cfg["T0"], torch.float32)
+    b = torch.empty_like(a)
+    out = run_steps(lambda x, y: ctx.heat_step(m, x, y, cfg["k"], cfg["dt"], path=cfdb.FUSED), a, b, cfg["steps"])
+    ref = o.heat_solve(cfg["T0"], cfg["k"], cfg["dt"], cfg["steps"])
+    assert rel_l2(host(out), ref) <= 1e-5
+    assert rel_linf(host(out), ref) <= 1e-5
+
+
+@pytest.mark.parametrize("shape", [(12, 8, 16), (9, 5, 4), (3, 17, 36), (20, 3, 132)])
+def test_heat_fused_edge_shapes(cfdb, oracle, ctx, shape):
+    """Partial tiles in y and z, thin meshes, chunk boundaries in x."""
+    nx, ny, nz = shape
+    m = cfdb.Mesh.structured(ctx, nx, ny, nz, 1 / nx, 1 / ny, 1 / nz)
+    o = oracle.Mesh(nx, ny, nz, 1 / nx, 1 / ny, 1 / nz)
+    rng = np.random.default_rng(12)
+    T0 = rng.uniform(size=m.n)
+    dt = 0.1 / (nx * nx + ny * ny + nz * nz)
+    a = dev(T0, torch.float32)
+    b = torch.empty_like(a)
+    out = run_steps(lambda x, y: ctx.heat_step(m, x, y, 1.0, dt, path=cfdb.FUSED), a, b, 7)
+    ref = o.heat_solve(T0, 1.0, dt, 7)
+    assert rel_linf(host(out), ref) <= 3e-6
+
+
+def test_fused_requires_nz_multiple_of_4(cfdb, ctx):
+    m = cfdb.Mesh.structured(ctx, 4, 4, 6, 0.25, 0.25, 1 / 6)
+    a = torch.zeros(m.n, device=DEV)
+    b = torch.zeros(m.n, device=DEV)
+    with pytest.raises(cfdb.CfdbError) as e:
+        ctx.heat_step(m, a, b, 1.0, 0.001, path=cfdb.FUSED)
+    assert e.value.code == cfdb.capi.EUNSUPPORTED
+    ctx.heat_step(m, a, b, 1.0, 0.001, path=cfdb.PLAIN)  # the plain path serves any shape
+
+
+@pytest.mark.parametrize("spec", MESHES, ids=["aniso", "cube8", "jitter6"])
+@pytest.mark.parametrize("mode", [0, 1])
+def test_wave_plain_fp64_bitwise(cfdb, oracle, ctx, spec, mode):
+    m, o = make_pair(cfdb, oracle, ctx, spec, np.float64)
+    rng = np.random.default_rng(13)
+    q0 = rng.standard_normal(4 * m.n)
+    c = np.exp(0.2 * rng.standard_normal(m.n))
+    dt = o.wave_dt(0.4, c=c)
+    a = dev(q0, torch.float64)
+    b = torch.empty_like(a)
+    tc = dev(c, torch.float64)
+    out = run_steps(lambda x, y: ctx.wave_step(m, x, y, dt, c=tc, speed_mode=mode, path=cfdb.PLAIN), a, b, 6)
+    ref = o.wave_solve(q0, dt, 6, c=c, speed_mode=mode)
+    assert np.array_equal(host(out), ref)
+
+
+@pytest.mark.parametrize("shape", [(16, 16, 16), (10, 7, 20), (24, 9, 132)])
+@pytest.mark.parametrize("cfield", [False, True])
+def test_wave_fused_fp32_vs_fp64_oracle(cfdb, oracle, ctx, shape, cfield):
+    nx, ny, nz = shape
+    m = cfdb.Mesh.structured(ctx, nx, ny, nz, 1 / nx, 1 / ny, 1 / nz)
+    o = oracle.Mesh(nx, ny, nz, 1 / nx, 1 / ny, 1 / nz)
+    rng = np.random.default_rng(14)
+    q0 = rng.standard_normal(4 * m.n)
+    c = np.exp(0.2 * rng.standard_normal(m.n)) if cfield else None
+    mode = 1 if cfield else 0
+    dt = o.wave_dt(0.4, c=c)
+    a = dev(q0, torch.float32)
+    b = torch.empty_like(a)
+    tc = None if c is None else dev(c, torch.float32)
+    out = run_steps(lambda x, y: ctx.wave_step(m, x, y, dt, c=tc, speed_mode=mode, path=cfdb.FUSED), a, b, 10)
+    ref = o.wave_solve(q0, dt, 10, c=c, speed_mode=mode)
+    assert rel_l2(host(out), ref) <= 1e-5
+
+
+def test_wave_fused_distorted_vs_fp64_oracle(cfdb, oracle, ctx):
+    from cfdarcov2_b200.workloads import jittered_vertices, wave_state
+    n = 16
+    V = jittered_vertices(n, seed=2)
+    m = cfdb.Mesh.from_vertices(ctx, n, n, n, 1 / n, 1 / n, 1 / n, V)
+    o = oracle.Mesh(n, n, n, 1 / n, 1 / n, 1 / n, vertices=V)
+    q0 = wave_state(n, sigma=0.1)
+    dt = o.wave_dt(0.4)
+    a = dev(q0, torch.float32)
+    b = torch.empty_like(a)
+    out = run_steps(lambda x, y: ctx.wave_step(m, x, y, dt, path=cfdb.FUSED), a, b, 20)
+    ref = o.wave_solve(q0, dt, 20)
+    assert rel_l2(host(out), ref) <= 1e-5
+
+
+def test_wave_config2_fused_fp32_vs_fp64_plain_full_size(cfdb, ctx):
+    """The wave workload at full size (128^3, 500 steps): FP32 fused vs the
+    FP64 plain GPU path (bit-identical to the FP64 oracle on the small cases
+    above), L2 relative error <= 1e-5, and the pressure integral conserved."""
+    from cfdarcov2_b200.workloads import wave_config
+    cfg = wave_config()
+    n = cfg["n"]
+    m = cfdb.Mesh.structured(ctx, n, n, n, cfg["dx"], cfg["dx"], cfg["dx"])
+    a64 = dev(cfg["q0"], torch.float64)
+    b64 = torch.empty_like(a64)
+    ref = run_steps(lambda x, y: ctx.wave_step(m, x, y, cfg["dt"], c_const=cfg["c"], path=cfdb.PLAIN), a64, b64,
+                    cfg["steps"])
+    a32 = dev(cfg["q0"], torch.float32)
+    b32 = torch.empty_like(a32)
+    got = run_steps(lambda x, y: ctx.wave_step(m, x, y, cfg["dt"], c_const=cfg["c"], path=cfdb.FUSED), a32, b32,
+                    cfg["steps"])
+    r, g = host(ref), host(got)
+    assert rel_l2(g, r) <= 1e-5
+    N = m.n
+    p0 = cfg["q0"][:N].sum()
+    assert abs(r[:N].sum() - p0) <= 1e-10 * p0

@@ -1,0 +1,208 @@
+"""Known-answer tests that pin the CPU oracle (the reference itself cannot be
+built here and ships no golden vectors, so the oracle is pinned by analytic
+results and by its committed golden fixtures)."""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def centers(m):
+    return m.geometry()["center"].reshape(3, m.n)
+
+
+def interior(m):
+    return m.geometry()["is_boundary"] == 0
+
+
+@pytest.mark.parametrize("dtype,tol", [(np.float64, 1e-12), (np.float32, 2e-4)])
+def test_uniform_geometry_exact(oracle, dtype, tol):
+    m = oracle.Mesh(4, 5, 6, 0.25, 0.2, 1 / 6, dtype=dtype)
+    g = m.geometry()
+    n = m.n
+    assert np.allclose(g["volume"], 0.25 * 0.2 / 6, rtol=tol)
+    areas = [0.25 * 0.2, 0.25 * 0.2, 0.25 / 6, 0.25 / 6, 0.2 / 6, 0.2 / 6]
+    for f in range(6):
+        assert np.allclose(g["area"][f * n:(f + 1) * n], areas[f], rtol=tol)
+    # unsigned normals are +1 along their axis (src/mesh3d.cpp:86-90)
+    nrm = g["normal"].reshape(3, 6, n)
+    for f, d in [(0, 2), (1, 2), (2, 1), (3, 1), (4, 0), (5, 0)]:
+        assert np.allclose(nrm[d, f], 1.0)
+    # outward normals point away from the cell
+    alt = g["normal_alt"].reshape(3, 6, n)
+    for f, d, s in [(0, 2, -1), (1, 2, 1), (2, 1, -1), (3, 1, 1), (4, 0, -1), (5, 0, 1)]:
+        assert np.allclose(alt[d, f], s)
+    # alpha_d = 1/h on interior and boundary faces alike
+    for f, h in [(0, 1 / 6), (1, 1 / 6), (2, 0.2), (3, 0.2), (4, 0.25), (5, 0.25)]:
+        assert np.allclose(g["alpha_d"][f * n:(f + 1) * n], 1 / h, rtol=tol)
+
+
+def test_linear_field_exact_gradient_and_zero_laplacian(oracle):
+    m = oracle.Mesh(6, 7, 8, 0.1, 0.2, 0.3)
+    c = centers(m)
+    phi = 2.0 * c[0] + 3.0 * c[1] - c[2] + 0.5
+    inner = interior(m)
+    assert np.abs(m.grad(phi, 1)[inner] - 2.0).max() < 1e-12
+    assert np.abs(m.grad(phi, 2)[inner] - 3.0).max() < 1e-12
+    assert np.abs(m.grad(phi, 4)[inner] + 1.0).max() < 1e-12
+    assert np.abs(m.lapl(phi)[inner]).max() < 1e-11
+    # a linear field also has zero stabilisation in the interior away from walls
+    g = m.geometry()
+    ids = g["ids"].reshape(6, m.n)
+    deep = inner & np.all(interior(m)[ids], axis=0)
+    assert np.abs(m.stab(phi)[deep]).max() < 1e-11
+
+
+def test_quadratic_field_exact_laplacian(oracle):
+    m = oracle.Mesh(8, 8, 8, 1 / 8, 1 / 8, 1 / 8)
+    c = centers(m)
+    q = c[0] ** 2 + 2 * c[1] ** 2 + 3 * c[2] ** 2
+    assert np.abs(m.lapl(q)[interior(m)] - 12.0).max() < 1e-10
+
+
+def test_xramp_d2dx_matches_testing_grad_example(oracle):
+    # examples/main_3d_testing_grad.cpp:35-46 prints d2dx of x + 1 on both
+    # paths: 0 inside, (phi_N - phi_P)/dx^2 from one side at the x walls.
+    m = oracle.Mesh(8, 4, 4, 1.0, 1.0, 1.0)
+    c = centers(m)
+    L = m.lapl(c[0] + 1.0, 1).reshape(8, 4, 4)
+    assert np.all(L[0] == 1.0) and np.all(L[-1] == -1.0) and np.all(L[1:-1] == 0.0)
+
+
+def test_heat_conserves_and_decays_cosine_mode(oracle):
+    n = 16
+    m = oracle.Mesh(n, n, n, 1 / n, 1 / n, 1 / n)
+    c = centers(m)
+    T0 = np.cos(np.pi * c[0]) + 1.0
+    k, dt, steps = 0.01, 0.1 * (1 / n) ** 2 / 0.01, 50
+    T = m.heat_solve(T0, k, dt, steps)
+    assert abs(m.total(T) - m.total(T0)) < 1e-12 * m.total(T0)
+    # discrete decay of the x cosine mode: modified wavenumber 2(1-cos(pi dx))/dx^2
+    dx = 1 / n
+    lam = 2 * (1 - np.cos(np.pi * dx)) / dx ** 2
+    expect = (1 - k * dt * lam) ** steps
+    amp = (T - 1.0) / np.cos(np.pi * c[0])
+    assert np.allclose(amp, expect, rtol=1e-10)
+
+
+def test_heat_faithful_equals_fused(oracle):
+    m = oracle.Mesh(10, 9, 8, 0.1, 0.1, 0.1)
+    rng = np.random.default_rng(0)
+    T0 = rng.uniform(size=m.n)
+    a = m.heat_solve(T0, 0.01, 0.05, 10, faithful=False)
+    b = m.heat_solve(T0, 0.01, 0.05, 10, faithful=True)
+    assert np.array_equal(a, b)
+
+
+def test_wave_conserves_pressure_integral(oracle):
+    n = 12
+    m = oracle.Mesh(n, n, n, 1 / n, 1 / n, 1 / n)
+    rng = np.random.default_rng(1)
+    q0 = rng.standard_normal(4 * m.n)
+    dt = m.wave_dt(0.4)
+    q = m.wave_solve(q0, dt, 20)
+    assert abs(m.total(q[: m.n]) - m.total(q0[: m.n])) < 1e-12 * np.abs(q0[: m.n]).sum() / m.n
+    assert np.array_equal(m.wave_solve(q0, dt, 5), m.wave_solve(q0, dt, 5, faithful=True))
+
+
+def test_wave_dt_matches_uniform_formula(oracle):
+    m = oracle.Mesh(8, 8, 8, 1 / 8, 1 / 8, 1 / 8)
+    assert m.wave_dt(0.4, cconst=2.0) == pytest.approx(0.4 / (3 * 2.0 * 8))
+
+
+def test_sod_matches_exact_riemann(oracle):
+    from oracle import riemann
+    from cfdarcov2_b200.workloads import sod_state
+    nx = 400
+    U0, (dx, dy, dz) = sod_state(nx, 2, 2, 1.0, 2 / nx)
+    m = oracle.Mesh(nx, 2, 2, dx, dy, dz)
+    U, steps, t, tot = m.euler_solve(U0, 1.4, 0.4, 0.2)
+    assert t == 0.2 and steps > 100
+    xc = (np.arange(nx) + 0.5) * dx
+    ex = riemann.sample(xc, 0.2, 0.5, (1.0, 0.0, 1.0), (0.125, 0.0, 0.1))
+    rho = U[: m.n].reshape(nx, 4)[:, 0]
+    assert np.mean(np.abs(rho - ex[0])) < 0.012
+    # mass and energy are exactly conserved until waves reach the x ends
+    assert np.abs(tot[:, 0] - tot[0, 0]).max() < 1e-13 * tot[0, 0]
+    assert np.abs(tot[:, 1] - tot[0, 1]).max() < 1e-13 * tot[0, 1]
+
+
+def test_riemann_star_state_toro_test1(oracle):
+    from oracle import riemann
+    # Toro table 4.2, test 1 (the Sod problem): p* = 0.30313, u* = 0.92745
+    p, u = riemann.star_state(1.0, 0.0, 1.0, 0.125, 0.0, 0.1, 1.4)
+    assert p == pytest.approx(0.30313, abs=1e-5) and u == pytest.approx(0.92745, abs=1e-5)
+
+
+def test_adjoint_dot_product(oracle):
+    """<A v, w> == <v, A^T w> for the linear wave step (dt fixed, mode 1)."""
+    n = 6
+    m = oracle.Mesh(n, n + 1, n + 2, 1 / n, 1 / n, 1 / n)
+    rng = np.random.default_rng(3)
+    c = np.exp(0.2 * rng.standard_normal(m.n))
+    v = rng.standard_normal(4 * m.n)
+    w = rng.standard_normal(4 * m.n)
+    dt = m.wave_dt(0.4, c=c)
+    Av = m.wave_solve(v, dt, 1, c=c, speed_mode=1)
+    ATw, _ = m.wave_adjoint_step(v, w, c, np.zeros(m.n), dt)
+    assert np.dot(Av, w) == pytest.approx(np.dot(v, ATw), rel=1e-12)
+
+
+def test_adjoint_gradient_matches_finite_differences(oracle):
+    n, steps = 8, 12
+    m = oracle.Mesh(n, n, n, 1 / n, 1 / n, 1 / n)
+    rng = np.random.default_rng(5)
+    c = np.exp(0.2 * rng.standard_normal(m.n))
+    from cfdarcov2_b200.workloads import wave_state
+    q0 = wave_state(n, sigma=0.2)
+    target = rng.standard_normal(m.n) * 0.01
+    dt = m.wave_dt(0.4, c=c * 1.1)
+    J, gc, gp = m.wave_gradient(q0, c, target, dt, steps)
+    assert J == pytest.approx(m.wave_objective(q0, c, target, dt, steps), rel=1e-14)
+    d = rng.standard_normal(m.n)
+    eps = 1e-6
+    fd = (m.wave_objective(q0, c + eps * d, target, dt, steps) - m.wave_objective(q0, c - eps * d, target, dt, steps)) / (2 * eps)
+    assert np.dot(gc, d) == pytest.approx(fd, rel=1e-7)
+    dp = np.zeros(4 * m.n)
+    dp[: m.n] = rng.standard_normal(m.n)
+    fdp = (m.wave_objective(q0 + eps * dp, c, target, dt, steps) - m.wave_objective(q0 - eps * dp, c, target, dt, steps)) / (2 * eps)
+    assert np.dot(gp, dp[: m.n]) == pytest.approx(fdp, rel=1e-7)
+
+
+def test_distorted_mesh_geometry_closes(oracle):
+    """On a jittered mesh every cell's outward area vectors sum to zero
+    (closed surface) only approximately for non-planar faces, but the shared
+    faces are exactly antisymmetric between the two cells."""
+    from cfdarcov2_b200.workloads import jittered_vertices
+    n = 6
+    V = jittered_vertices(n, seed=2)
+    m = oracle.Mesh(n, n, n, 1 / n, 1 / n, 1 / n, vertices=V)
+    g = m.geometry()
+    N = m.n
+    alt = g["normal_alt"].reshape(3, 6, N)
+    A = g["area"].reshape(6, N)
+    ids = g["ids"].reshape(6, N)
+    ibf = g["ids_bound_free"].reshape(6, N)
+    for f in range(6):
+        inner = ibf[f] >= 0
+        j = ids[f][inner]
+        S_self = alt[:, f, inner] * A[f, inner]
+        S_nb = alt[:, f ^ 1, j] * A[f ^ 1, j]
+        assert np.allclose(S_self, -S_nb, atol=1e-15)
+    assert np.all(g["volume"] > 0)
+    assert g["volume"].sum() == pytest.approx(1.0, rel=1e-12)
+
+
+def test_golden_fixtures(oracle):
+    path = os.path.join(GOLDEN, "oracle_golden.npz")
+    data = np.load(path)
+    from golden.make_golden import compute_cases
+    now = compute_cases(oracle)
+    for k in data.files:
+        assert np.array_equal(data[k], now[k]), k
