@@ -32,8 +32,11 @@ class Context:
     """cfdb_ctx bound to one CUDA device and torch's current stream on it."""
 
     def __init__(self, device: int = 0):
+        import weakref
+
         import torch
         self.device = device
+        self._children = weakref.WeakSet()
         self.h = C.c_void_p()
         call("cfdb_ctx_create", device, C.byref(self.h))
         self.set_stream(torch.cuda.current_stream(device).cuda_stream)
@@ -55,8 +58,13 @@ class Context:
         call("cfdb_ctx_allocated_bytes", self.h, C.byref(v), ctx=self.h)
         return v.value
 
+    def adopt(self, child) -> None:
+        self._children.add(child)
+
     def close(self) -> None:
         if self.h:
+            for child in list(self._children):
+                child.close()
             lib().cfdb_ctx_destroy(self.h)
             self.h = C.c_void_p()
 
@@ -143,6 +151,20 @@ class Context:
         call("cfdb_wave_step", self.h, mesh.h, _dtype_code(q), int(path), _ptr(q), _ptr(qn), _ptr(c), float(c_const),
              int(speed_mode), float(dt), ctx=self.h)
 
+    def heat_run(self, mesh, Ta, Tb, k, dt, steps, path=FUSED, use_graph=True):
+        """Advances `steps` steps; returns the tensor that holds the final state."""
+        fb = C.c_int()
+        call("cfdb_heat_run", self.h, mesh.h, _dtype_code(Ta), int(path), _ptr(Ta), _ptr(Tb), float(k), float(dt),
+             int(steps), int(bool(use_graph)), C.byref(fb), ctx=self.h)
+        return Tb if fb.value else Ta
+
+    def wave_run(self, mesh, qa, qb, dt, steps, c=None, c_const=1.0, speed_mode=0, path=FUSED, use_graph=True):
+        """Advances `steps` steps; returns the tensor that holds the final state."""
+        fb = C.c_int()
+        call("cfdb_wave_run", self.h, mesh.h, _dtype_code(qa), int(path), _ptr(qa), _ptr(qb), _ptr(c), float(c_const),
+             int(speed_mode), float(dt), int(steps), int(bool(use_graph)), C.byref(fb), ctx=self.h)
+        return qb if fb.value else qa
+
     def wave_adjoint_step(self, mesh, q, lam1, lam0, c, gc, dt, path=FUSED):
         call("cfdb_wave_adjoint_step", self.h, mesh.h, _dtype_code(q), int(path), _ptr(q), _ptr(lam1), _ptr(lam0),
              _ptr(c), _ptr(gc), float(dt), ctx=self.h)
@@ -171,6 +193,8 @@ class Mesh:
         self.n = nx * ny * nz
         self.dx, self.dy, self.dz = dx, dy, dz
         self.uniform = uniform
+        if ctx is not None:
+            ctx.adopt(self)
 
     @classmethod
     def structured(cls, ctx, nx, ny, nz, dx, dy, dz):
@@ -226,6 +250,7 @@ class Euler:
 
     def __init__(self, ctx, mesh, dtype=F32, path=FUSED, gamma=1.4, cfl=0.4, t_end=0.2, max_steps=100000):
         self.ctx = ctx
+        ctx.adopt(self)
         self.h = C.c_void_p()
         call("cfdb_euler_create", ctx.h, mesh.h, int(dtype), int(path), float(gamma), float(cfl), float(t_end),
              int(max_steps), C.byref(self.h), ctx=ctx.h)
@@ -274,6 +299,7 @@ class Batch:
 
     def __init__(self, ctx, problems):
         self.ctx = ctx
+        ctx.adopt(self)
         arr = (capi.Problem * len(problems))()
         for i, p in enumerate(problems):
             arr[i].n, arr[i].kind, arr[i].param, arr[i].dt = int(p["n"]), int(p["kind"]), float(p["param"]), float(p["dt"])

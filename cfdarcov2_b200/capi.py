@@ -82,6 +82,8 @@ PROTOTYPES = {
     "cfdb_heat_step": (_I, [_P, _P, _I, _I, _P, _P, _D, _D]),
     "cfdb_wave_step": (_I, [_P, _P, _I, _I, _P, _P, _P, _D, _I, _D]),
     "cfdb_wave_dt": (_I, [_P, _P, _D, _D, _PD]),
+    "cfdb_heat_run": (_I, [_P, _P, _I, _I, _P, _P, _D, _D, _I32, _I, _PI]),
+    "cfdb_wave_run": (_I, [_P, _P, _I, _I, _P, _P, _P, _D, _I, _D, _I32, _I, _PI]),
     "cfdb_euler_create": (_I, [_P, _P, _I, _I, _D, _D, _D, _I64, _PP]),
     "cfdb_euler_destroy": (_I, [_P]),
     "cfdb_euler_begin": (_I, [_P, _P]),

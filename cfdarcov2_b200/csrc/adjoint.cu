@@ -6,11 +6,90 @@
 // its six faces from both sides, so no scatter or atomics are needed.  Uses
 // the volume-scaled adjoint lt = lam / V (R(N) carries 1/V_N).  The same
 // arithmetic on the general geometry is plain_ops.cu's wave_adjoint_plain_k.
-#include "cfdb_internal.hpp"
+#include "tma_host.hpp"
 
 namespace {
 
 constexpr int kThreads = 256;
+
+// TMA-sweep form of the same adjoint step: lam (4 fields) is the swept state,
+// the forward state q_n (4 fields) is staged as auxiliary data and c as the
+// coefficient field, all with their halos; the c-gradient of each cell is
+// accumulated in place.
+struct AdjPhys {
+  static constexpr int NF = 4;
+  static constexpr int NA = 4;
+  static constexpr bool HAS_C = true;
+  static constexpr int FT = 9;
+  static constexpr int MIN_BLOCKS = 2;
+  struct Params {
+    float A[3];  // face areas normal to x, y, z
+    float iV;    // 1 / cell volume
+    float dt;
+    float* gc;
+  };
+  struct Acc {};
+  __device__ static bool begin(Params&) { return true; }
+  __device__ static void ghost(float g[FT], const float p[FT], int) {
+#pragma unroll
+    for (int f = 0; f < FT; ++f) g[f] = p[f];
+  }
+  __device__ static void cell(const stencil::CellIn<FT>& in, const Params& a, float o[NF]) {
+    const float cP = in.P[8];
+    float lP[4], qP[4];
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+      lP[f] = in.P[f] * a.iV;
+      qP[f] = in.P[4 + f];
+    }
+    float ap = 0.f, au[3] = {0.f, 0.f, 0.f}, gg = 0.f;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const float Ad = a.A[d];
+#pragma unroll
+      for (int side = 0; side < 2; ++side) {
+        const int k = 2 * d + side;
+        const float s = side ? 1.f : -1.f;
+        if ((in.walls >> k) & 1) {
+          ap -= s * Ad * lP[1 + d];
+          au[d] -= cP * Ad * lP[1 + d];
+          gg -= Ad * qP[1 + d] * lP[1 + d];
+        } else {
+          const float* N = in.nb[k];
+          const float cN = N[8];
+          float lN[4], qN[4];
+#pragma unroll
+          for (int f = 0; f < 4; ++f) {
+            lN[f] = N[f] * a.iV;
+            qN[f] = N[4 + f];
+          }
+          const float h = 0.25f * (cP + cN) * Ad;
+          ap += h * (lN[0] - lP[0]) + 0.5f * s * Ad * (lN[1 + d] - lP[1 + d]);
+          const float sp = 0.5f * (cN * cN * lN[0] - cP * cP * lP[0]);
+#pragma unroll
+          for (int e = 0; e < 3; ++e) au[e] += h * (lN[1 + e] - lP[1 + e]);
+          au[d] += sp * s * Ad;
+          gg -= cP * s * Ad * (qP[1 + d] + qN[1 + d]) * lP[0];
+          const float jp = qN[0] - qP[0];
+          float ju_self = 0.f, ju_nb = 0.f;
+#pragma unroll
+          for (int e = 0; e < 3; ++e) {
+            ju_self += (qN[1 + e] - qP[1 + e]) * lP[1 + e];
+            ju_nb += (qP[1 + e] - qN[1 + e]) * lN[1 + e];
+          }
+          gg += 0.25f * Ad * ((jp * lP[0] + ju_self) + (ju_nb - jp * lN[0]));
+        }
+      }
+    }
+    o[0] = in.P[0] + a.dt * ap;
+#pragma unroll
+    for (int e = 0; e < 3; ++e) o[1 + e] = in.P[1 + e] + a.dt * au[e];
+    a.gc[in.idx] += a.dt * gg;
+  }
+  __device__ static void acc_init(Acc&) {}
+  __device__ static void acc_cell(Acc&, const float*, const Params&) {}
+  __device__ static void finish(Acc&, const Params&, bool) {}
+};
 
 struct AdjArgs {
   int X, Y, Z;
@@ -91,6 +170,16 @@ __global__ void __launch_bounds__(kThreads)
 int fused_wave_adjoint(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* q, const void* lam1, void* lam0,
                        const void* c, void* gc, double dt) {
   (void)dtype;
+  if (stencil::check_sweep(ctx, m, {q, lam1, lam0, c}) == CFDB_OK) {
+    AdjPhys::Params p;
+    p.A[0] = float(m->dy * m->dz); p.A[1] = float(m->dx * m->dz); p.A[2] = float(m->dx * m->dy);
+    p.iV = float(1.0 / (m->dx * m->dy * m->dz));
+    p.dt = float(dt);
+    p.gc = static_cast<float*>(gc);
+    if (m->nz >= 64) return stencil::launch_sweep<AdjPhys, 64, 8, 4, 2>(ctx, m, lam1, q, c, lam0, p, 0);
+    return stencil::launch_sweep<AdjPhys, 32, 8, 4, 2>(ctx, m, lam1, q, c, lam0, p, 0);
+  }
+  // shapes the sweep cannot stage (nz % 4 != 0 or unaligned pointers): gather form
   AdjArgs a;
   a.X = int(m->nx); a.Y = int(m->ny); a.Z = int(m->nz);
   a.n = (long long)m->n;

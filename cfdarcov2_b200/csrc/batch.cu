@@ -1,0 +1,429 @@
+// Batched ensemble of independent small problems (cubes of n^3 cells on
+// [0,1]^3, heat or the acoustic wave system) advanced together: one
+// persistent launch per step walks a table of work items (problem, first
+// cell), each covering `cells_per_item` consecutive cells of one problem.
+// Per-problem constants (dt, k or c, spacing) live in a device table, so
+// uneven sizes and parameters share one kernel; the step is replayed from a
+// captured CUDA graph.  cells_per_item, the CTA size and the CTAs per SM are
+// chosen by an autotuner that times candidates on the real pools and caches
+// the winner per device and problem set.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <new>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "cfdb_internal.hpp"
+
+namespace {
+
+struct ProbDev {
+  int32_t n;
+  int32_t kind;
+  float c0, c1, c2;  // heat: c0 = dt k / dx^2; wave: c0 = dt c^2 / (2 dx), c1 = dt c / (2 dx), c2 = dt / (2 dx)
+  int64_t offset;
+};
+
+struct ItemDev {
+  int32_t prob;
+  int32_t start;
+};
+
+// Heat: T' = T + c0 sum_faces (T_N - T), zero-gradient walls.
+__device__ __forceinline__ void heat_cell(const ProbDev& P, const float* __restrict__ a, float* __restrict__ b,
+                                          int x, int y, int z, int c) {
+  const int n = P.n, n2 = n * n;
+  const float* T = a + P.offset;
+  const float t = __ldg(T + c);
+  float s = 0.f;
+  if (x > 0) s += __ldg(T + c - n2) - t;
+  if (x < n - 1) s += __ldg(T + c + n2) - t;
+  if (y > 0) s += __ldg(T + c - n) - t;
+  if (y < n - 1) s += __ldg(T + c + n) - t;
+  if (z > 0) s += __ldg(T + c - 1) - t;
+  if (z < n - 1) s += __ldg(T + c + 1) - t;
+  b[P.offset + c] = t + P.c0 * s;
+}
+
+// Acoustic system with constant c (Rusanov dissipation = weighted Laplacian),
+// reflective walls (ghost: wall-normal velocity negated).
+__device__ __forceinline__ void wave_cell(const ProbDev& P, const float* __restrict__ a, float* __restrict__ b,
+                                          int x, int y, int z, int c) {
+  const int n = P.n;
+  const int64_t n3 = int64_t(n) * n * n;
+  const float* q = a + P.offset;
+  float C[4];
+#pragma unroll
+  for (int f = 0; f < 4; ++f) C[f] = __ldg(q + f * n3 + c);
+  const int coord[3] = {x, y, z};
+  const int stride[3] = {n * n, n, 1};
+  float op = C[0], ou[3] = {C[1], C[2], C[3]};
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    float m[4], p[4];
+    if (coord[d] > 0) {
+#pragma unroll
+      for (int f = 0; f < 4; ++f) m[f] = __ldg(q + f * n3 + c - stride[d]);
+    } else {
+#pragma unroll
+      for (int f = 0; f < 4; ++f) m[f] = C[f];
+      m[1 + d] = -C[1 + d];
+    }
+    if (coord[d] < n - 1) {
+#pragma unroll
+      for (int f = 0; f < 4; ++f) p[f] = __ldg(q + f * n3 + c + stride[d]);
+    } else {
+#pragma unroll
+      for (int f = 0; f < 4; ++f) p[f] = C[f];
+      p[1 + d] = -C[1 + d];
+    }
+    op -= P.c0 * (p[1 + d] - m[1 + d]) - P.c1 * ((p[0] + m[0]) - 2.0f * C[0]);
+    ou[d] -= P.c2 * (p[0] - m[0]);
+#pragma unroll
+    for (int e = 0; e < 3; ++e) ou[e] += P.c1 * ((p[1 + e] + m[1 + e]) - 2.0f * C[1 + e]);
+  }
+  float* o = b + P.offset;
+  o[c] = op;
+  o[n3 + c] = ou[0];
+  o[2 * n3 + c] = ou[1];
+  o[3 * n3 + c] = ou[2];
+}
+
+__global__ void batch_step_k(const ProbDev* __restrict__ probs, const ItemDev* __restrict__ items, int n_items,
+                             int cells_per_item, const float* __restrict__ a, float* __restrict__ b) {
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const ItemDev I = items[it];
+    const ProbDev P = probs[I.prob];
+    const int n = P.n, n2 = n * n, n3 = n2 * n;
+    const int end = min(I.start + cells_per_item, n3);
+    for (int c = I.start + threadIdx.x; c < end; c += blockDim.x) {
+      const int x = c / n2;
+      const int r = c - x * n2;
+      const int y = r / n;
+      const int z = r - y * n;
+      if (P.kind == 0) heat_cell(P, a, b, x, y, z, c);
+      else wave_cell(P, a, b, x, y, z, c);
+    }
+  }
+}
+
+}  // namespace
+
+struct cfdb_batch {
+  cfdb_ctx* ctx = nullptr;
+  std::vector<cfdb_problem> probs;
+  int64_t pool = 0;
+  ProbDev* d_probs = nullptr;
+  ItemDev* d_items = nullptr;
+  int n_items = 0;
+  int items_cap = 0;
+  int cells_per_item = 2048, threads = 256, ctas_per_sm = 4;
+  int64_t last_launches = 0;
+  cudaGraphExec_t graph = nullptr;
+  const void* graph_a = nullptr;
+  const void* graph_b = nullptr;
+  int graph_cfg[3] = {0, 0, 0};
+};
+
+namespace {
+
+int build_items(cfdb_batch* b) {
+  std::vector<ItemDev> items;
+  for (size_t p = 0; p < b->probs.size(); ++p) {
+    const int64_t n3 = int64_t(b->probs[p].n) * b->probs[p].n * b->probs[p].n;
+    for (int64_t s = 0; s < n3; s += b->cells_per_item) items.push_back(ItemDev{int32_t(p), int32_t(s)});
+  }
+  if (int(items.size()) > b->items_cap) {
+    cfdb_dev_free(b->ctx, b->d_items);
+    b->d_items = nullptr;
+    if (int rc = cfdb_dev_alloc(b->ctx, int64_t(sizeof(ItemDev)) * items.size(), reinterpret_cast<void**>(&b->d_items)))
+      return rc;
+    b->items_cap = int(items.size());
+  }
+  CFDB_CUDA(b->ctx, cudaMemcpy(b->d_items, items.data(), sizeof(ItemDev) * items.size(), cudaMemcpyHostToDevice));
+  b->n_items = int(items.size());
+  return CFDB_OK;
+}
+
+void drop_graph(cfdb_batch* b) {
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  b->graph = nullptr;
+}
+
+int launch(cfdb_batch* b, const void* a, void* out) {
+  const int grid = std::max(1, b->ctx->num_sms) * b->ctas_per_sm;
+  batch_step_k<<<grid, b->threads, 0, b->ctx->stream>>>(b->d_probs, b->d_items, b->n_items, b->cells_per_item,
+                                                        static_cast<const float*>(a), static_cast<float*>(out));
+  CFDB_LAUNCHED(b->ctx);
+  return CFDB_OK;
+}
+
+std::string cache_key(const cfdb_batch* b) {
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, b->ctx->device);
+  uint64_t h = 1469598103934665603ull;  // FNV-1a over (n, kind) of every problem
+  for (const auto& p : b->probs) {
+    for (int32_t v : {p.n, p.kind}) {
+      for (int k = 0; k < 4; ++k) {
+        h ^= uint64_t((v >> (8 * k)) & 0xff);
+        h *= 1099511628211ull;
+      }
+    }
+  }
+  char buf[256];
+  std::string name(prop.name);
+  for (auto& ch : name)
+    if (ch == '"' || ch == ' ') ch = '_';
+  snprintf(buf, sizeof(buf), "%s:%d:%016llx", name.c_str(), int(b->probs.size()), (unsigned long long)h);
+  return buf;
+}
+
+// The cache file is a flat JSON object {"key": [cells_per_item, threads, ctas_per_sm], ...}.
+std::map<std::string, std::vector<int>> read_cache(const char* path) {
+  std::map<std::string, std::vector<int>> out;
+  if (!path) return out;
+  std::ifstream f(path);
+  if (!f) return out;
+  std::stringstream ss;
+  ss << f.rdbuf();
+  const std::string s = ss.str();
+  size_t pos = 0;
+  while ((pos = s.find('"', pos)) != std::string::npos) {
+    const size_t end = s.find('"', pos + 1);
+    if (end == std::string::npos) break;
+    const std::string key = s.substr(pos + 1, end - pos - 1);
+    const size_t lb = s.find('[', end), rb = s.find(']', end);
+    if (lb == std::string::npos || rb == std::string::npos) break;
+    int v0 = 0, v1 = 0, v2 = 0;
+    if (sscanf(s.c_str() + lb, "[%d , %d , %d]", &v0, &v1, &v2) == 3) out[key] = {v0, v1, v2};
+    pos = rb + 1;
+  }
+  return out;
+}
+
+void write_cache(const char* path, const std::map<std::string, std::vector<int>>& m) {
+  if (!path) return;
+  std::ofstream f(path);
+  f << "{\n";
+  size_t k = 0;
+  for (const auto& kv : m) {
+    f << "  \"" << kv.first << "\": [" << kv.second[0] << ", " << kv.second[1] << ", " << kv.second[2] << "]"
+      << (++k < m.size() ? ",\n" : "\n");
+  }
+  f << "}\n";
+}
+
+}  // namespace
+
+extern "C" int cfdb_batch_create(cfdb_ctx* ctx, cfdb_problem* probs, int32_t count, int64_t* pool_elems,
+                                 cfdb_batch** out) {
+  if (!out) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_batch_create: out is NULL");
+  *out = nullptr;
+  if (!ctx || !probs || count < 1) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_batch_create: need a context and >= 1 problem");
+  int64_t off = 0;
+  for (int32_t i = 0; i < count; ++i) {
+    cfdb_problem& p = probs[i];
+    if (p.n < 2 || p.n > 1024) return cfdb_fail(ctx, CFDB_EINVAL, "problem %d: n = %d outside [2, 1024]", i, p.n);
+    if (p.kind != 0 && p.kind != 1) return cfdb_fail(ctx, CFDB_EINVAL, "problem %d: kind %d is not 0 (heat) or 1 (wave)", i, p.kind);
+    if (!(p.param > 0) || !(p.dt > 0) || !std::isfinite(p.param) || !std::isfinite(p.dt))
+      return cfdb_fail(ctx, CFDB_EINVAL, "problem %d: param and dt must be finite and > 0", i);
+    p.offset = off;
+    off += int64_t(p.n) * p.n * p.n * (p.kind == 1 ? 4 : 1);
+  }
+  CFDB_CUDA(ctx, cudaSetDevice(ctx->device));
+  auto* b = new (std::nothrow) cfdb_batch();
+  if (!b) return cfdb_fail(ctx, CFDB_ENOMEM, "host allocation failed");
+  b->ctx = ctx;
+  b->probs.assign(probs, probs + count);
+  b->pool = off;
+  std::vector<ProbDev> pd(count);
+  for (int32_t i = 0; i < count; ++i) {
+    const cfdb_problem& p = probs[i];
+    const double dx = 1.0 / p.n;
+    ProbDev d{p.n, p.kind, 0.f, 0.f, 0.f, p.offset};
+    if (p.kind == 0) {
+      d.c0 = float(p.dt * p.param / (dx * dx));
+    } else {
+      d.c0 = float(0.5 * p.dt * p.param * p.param / dx);
+      d.c1 = float(0.5 * p.dt * p.param / dx);
+      d.c2 = float(0.5 * p.dt / dx);
+    }
+    pd[i] = d;
+  }
+  int rc = cfdb_dev_alloc(ctx, int64_t(sizeof(ProbDev)) * count, reinterpret_cast<void**>(&b->d_probs));
+  if (!rc) {
+    cudaError_t e = cudaMemcpy(b->d_probs, pd.data(), sizeof(ProbDev) * count, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) rc = cfdb_cuda_fail(ctx, e, "cudaMemcpy");
+  }
+  if (!rc) rc = build_items(b);
+  if (rc) {
+    cfdb_batch_destroy(b);
+    return rc;
+  }
+  if (pool_elems) *pool_elems = off;
+  cfdb_adopt(ctx, b, [b] {
+    drop_graph(b);
+    b->ctx = nullptr;
+    b->d_probs = nullptr;
+    b->d_items = nullptr;
+  });
+  *out = b;
+  return CFDB_OK;
+}
+
+extern "C" int cfdb_batch_destroy(cfdb_batch* b) {
+  if (!b) return CFDB_OK;
+  drop_graph(b);
+  if (b->ctx) {
+    cfdb_release(b->ctx, b);
+    cudaStreamSynchronize(b->ctx->stream);
+    cfdb_dev_free(b->ctx, b->d_probs);
+    cfdb_dev_free(b->ctx, b->d_items);
+  }
+  delete b;
+  return CFDB_OK;
+}
+
+extern "C" int cfdb_batch_set_config(cfdb_batch* b, int32_t cells_per_item, int32_t threads, int32_t ctas_per_sm) {
+  if (!b || !b->ctx) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_batch_set_config: handle is NULL or its context was destroyed");
+  if (cells_per_item < 32 || cells_per_item > (1 << 22) || threads < 32 || threads > 1024 || threads % 32 ||
+      ctas_per_sm < 1 || ctas_per_sm > 32 || threads * ctas_per_sm > 2048)
+    return cfdb_fail(b->ctx, CFDB_EINVAL, "cfdb_batch_set_config: configuration out of range");
+  const bool items_change = cells_per_item != b->cells_per_item;
+  b->cells_per_item = cells_per_item;
+  b->threads = threads;
+  b->ctas_per_sm = ctas_per_sm;
+  drop_graph(b);
+  return items_change ? build_items(b) : CFDB_OK;
+}
+
+extern "C" int cfdb_batch_get_config(const cfdb_batch* b, int32_t* cells_per_item, int32_t* threads, int32_t* ctas) {
+  if (!b || !b->ctx) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_batch_get_config: handle is NULL or its context was destroyed");
+  if (cells_per_item) *cells_per_item = b->cells_per_item;
+  if (threads) *threads = b->threads;
+  if (ctas) *ctas = b->ctas_per_sm;
+  return CFDB_OK;
+}
+
+extern "C" int cfdb_batch_step(cfdb_batch* b, const void* a, void* out) {
+  if (!b || !b->ctx) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_batch_step: handle is NULL or its context was destroyed");
+  if (!a || !out || a == out) return cfdb_fail(b->ctx, CFDB_EINVAL, "cfdb_batch_step: need distinct pools");
+  CFDB_CUDA(b->ctx, cudaSetDevice(b->ctx->device));
+  return launch(b, a, out);
+}
+
+extern "C" int cfdb_batch_run(cfdb_batch* b, void* a, void* out, int32_t steps, int use_graph) {
+  if (!b || !b->ctx) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_batch_run: handle is NULL or its context was destroyed");
+  if (!a || !out || a == out || steps < 0) return cfdb_fail(b->ctx, CFDB_EINVAL, "cfdb_batch_run: bad arguments");
+  CFDB_CUDA(b->ctx, cudaSetDevice(b->ctx->device));
+  b->last_launches = 0;
+  if (!use_graph) {
+    for (int32_t k = 0; k < steps; ++k) {
+      if (int rc = (k & 1) ? launch(b, out, a) : launch(b, a, out)) return rc;
+      ++b->last_launches;
+    }
+    return CFDB_OK;
+  }
+  // (re)record the two-step graph a -> out -> a when pools or config changed
+  if (!b->graph || b->graph_a != a || b->graph_b != out || b->graph_cfg[0] != b->cells_per_item ||
+      b->graph_cfg[1] != b->threads || b->graph_cfg[2] != b->ctas_per_sm) {
+    drop_graph(b);
+    cfdb_ctx* ctx = b->ctx;
+    if (!ctx->capture_stream)
+      CFDB_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->capture_stream, cudaStreamNonBlocking));
+    cudaStream_t user = ctx->stream;
+    ctx->stream = ctx->capture_stream;
+    cudaGraph_t g = nullptr;
+    int rc = CFDB_OK;
+    cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      rc = launch(b, a, out);
+      if (!rc) rc = launch(b, out, a);
+      cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &g);
+      if (!rc && e2 != cudaSuccess) rc = cfdb_cuda_fail(ctx, e2, "cudaStreamEndCapture");
+    } else {
+      rc = cfdb_cuda_fail(ctx, e, "cudaStreamBeginCapture");
+    }
+    ctx->stream = user;
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    e = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      b->graph = nullptr;
+      return cfdb_cuda_fail(ctx, e, "cudaGraphInstantiate");
+    }
+    b->graph_a = a;
+    b->graph_b = out;
+    b->graph_cfg[0] = b->cells_per_item; b->graph_cfg[1] = b->threads; b->graph_cfg[2] = b->ctas_per_sm;
+  }
+  for (int32_t k = 0; k + 1 < steps; k += 2) {
+    CFDB_CUDA(b->ctx, cudaGraphLaunch(b->graph, b->ctx->stream));
+    b->last_launches += 2;
+  }
+  if (steps & 1) {
+    if (int rc = launch(b, a, out)) return rc;
+    ++b->last_launches;
+  }
+  return CFDB_OK;
+}
+
+extern "C" int cfdb_batch_launch_count(const cfdb_batch* b, int64_t* out) {
+  if (!b || !out) return cfdb_fail(b ? b->ctx : nullptr, CFDB_EINVAL, "cfdb_batch_launch_count: bad arguments");
+  *out = b->last_launches;
+  return CFDB_OK;
+}
+
+extern "C" int cfdb_batch_tune(cfdb_batch* b, void* a, void* out, const char* cache_path) {
+  if (!b || !b->ctx) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_batch_tune: handle is NULL or its context was destroyed");
+  if (!a || !out || a == out) return cfdb_fail(b->ctx, CFDB_EINVAL, "cfdb_batch_tune: need distinct pools");
+  cfdb_ctx* ctx = b->ctx;
+  CFDB_CUDA(ctx, cudaSetDevice(ctx->device));
+  auto cache = read_cache(cache_path);
+  const std::string key = cache_key(b);
+  auto hit = cache.find(key);
+  if (hit != cache.end() && hit->second.size() == 3)
+    if (cfdb_batch_set_config(b, hit->second[0], hit->second[1], hit->second[2]) == CFDB_OK) return CFDB_OK;
+  cudaEvent_t e0, e1;
+  CFDB_CUDA(ctx, cudaEventCreate(&e0));
+  CFDB_CUDA(ctx, cudaEventCreate(&e1));
+  float best = INFINITY;
+  int bc[3] = {b->cells_per_item, b->threads, b->ctas_per_sm};
+  const int cpis[] = {512, 1024, 2048, 4096, 8192};
+  const int ths[] = {128, 256, 512};
+  const int ctas[] = {2, 4, 8, 16};
+  int rc = CFDB_OK;
+  for (int cpi : cpis)
+    for (int th : ths)
+      for (int ct : ctas) {
+        if (th * ct > 2048) continue;
+        if ((rc = cfdb_batch_set_config(b, cpi, th, ct))) break;
+        if ((rc = launch(b, a, out))) break;  // warm-up
+        cudaEventRecord(e0, ctx->stream);
+        for (int k = 0; k < 4 && !rc; ++k) rc = (k & 1) ? launch(b, out, a) : launch(b, a, out);
+        cudaEventRecord(e1, ctx->stream);
+        cudaError_t e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) rc = cfdb_cuda_fail(ctx, e, "cudaEventSynchronize");
+        if (rc) break;
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) {
+          best = ms;
+          bc[0] = cpi; bc[1] = th; bc[2] = ct;
+        }
+      }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  if ((rc = cfdb_batch_set_config(b, bc[0], bc[1], bc[2]))) return rc;
+  cache[key] = {bc[0], bc[1], bc[2]};
+  write_cache(cache_path, cache);
+  return CFDB_OK;
+}

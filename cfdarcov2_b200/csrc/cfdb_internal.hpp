@@ -6,6 +6,7 @@
 
 #include <cstdarg>
 #include <cstdint>
+#include <functional>
 #include <memory>
 #include <string>
 #include <unordered_map>
@@ -67,7 +68,26 @@ struct cfdb_ctx {
   int64_t allocated = 0;
   std::unordered_map<void*, int64_t> allocs;
   int* d_error = nullptr;  // device error word written by bounded waits
+  cudaStream_t capture_stream = nullptr;  // private stream used to record CUDA graphs
+  // Objects created on this context (meshes, Euler solvers, batches) with a
+  // callback that detaches them when the context is destroyed first: their
+  // device memory goes with the context, their own destroy then frees only
+  // host memory.
+  std::unordered_map<void*, std::function<void()>> children;
 };
+
+inline void cfdb_adopt(cfdb_ctx* ctx, void* child, std::function<void()> orphan) {
+  if (ctx) ctx->children[child] = std::move(orphan);
+}
+inline void cfdb_release(cfdb_ctx* ctx, void* child) {
+  if (ctx) ctx->children.erase(child);
+}
+
+// Runs `steps` calls of step(src, dst) alternating a -> b -> a ..., eagerly or
+// replayed from a captured CUDA graph (graphs.cpp).
+#include <functional>
+int cfdb_run_steps(cfdb_ctx* ctx, void* a, void* b, int32_t steps, int use_graph,
+                   const std::function<int(const void*, void*)>& step, int64_t* launches = nullptr);
 
 struct cfdb_mesh {
   cfdb_ctx* ctx = nullptr;
@@ -108,6 +128,7 @@ inline size_t dtype_size(int dtype) { return dtype == CFDB_F64 ? 8 : 4; }
 inline bool dtype_ok(int dtype) { return dtype == CFDB_F32 || dtype == CFDB_F64; }
 
 int cfdb_check_mesh(cfdb_ctx* ctx, cfdb_mesh* m);
+void cfdb_mesh_orphan(cfdb_mesh* m);
 
 // ---- launchers implemented in the kernel files ------------------------------
 // plain_ops.cu

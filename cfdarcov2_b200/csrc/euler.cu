@@ -21,7 +21,9 @@ __device__ __forceinline__ void comp_add(double& s, double& c, double x) {
 
 struct EulerPhys {
   static constexpr int NF = 5;
+  static constexpr int NA = 0;
   static constexpr bool HAS_C = false;
+  static constexpr int MIN_BLOCKS = 1;
   struct Params {
     float ih[3];
     float gamma;
@@ -79,7 +81,8 @@ struct EulerPhys {
     a = sqrtf(gamma * p * ir);
   }
 
-  __device__ static void cell(const float P[NF], const float nb[6][NF], const float*, const Params& a, float o[NF]) {
+  __device__ static void cell(const stencil::CellIn<NF>& in, const Params& a, float o[NF]) {
+    const float* P = in.P;
     const float gm1 = a.gamma - 1.0f;
     float irP, uP[3], pP, aP;
     prim(P, gm1, a.gamma, irP, uP, pP, aP);
@@ -88,7 +91,7 @@ struct EulerPhys {
     for (int d = 0; d < 3; ++d) {
 #pragma unroll
       for (int side = 0; side < 2; ++side) {
-        const float* N = nb[2 * d + side];
+        const float* N = in.nb[2 * d + side];
         const float sg = side ? 1.0f : -1.0f;
         float irN, uN[3], pN, aN;
         prim(N, gm1, a.gamma, irN, uN, pN, aN);
@@ -190,6 +193,7 @@ struct EulerPhys {
 };
 
 constexpr int kEulerCtasPerSm = 2;
+constexpr int kEulerVZ = 4;
 
 template <int TZ>
 int launch_euler(cfdb_euler* e, const void* U, void* Un, int64_t s) {
@@ -203,13 +207,15 @@ int launch_euler(cfdb_euler* e, const void* U, void* Un, int64_t s) {
   p.clock = e->clock; p.totals = e->totals; p.part = e->part;
   p.s = (long long)s;
   p.max_steps = (long long)e->max_steps;
-  return stencil::launch_sweep<EulerPhys, TZ, 8, 4>(e->ctx, m, U, Un, nullptr, p, kEulerCtasPerSm);
+  return stencil::launch_sweep<EulerPhys, TZ, 8, 4, kEulerVZ>(e->ctx, m, U, nullptr, nullptr, Un, p, kEulerCtasPerSm);
 }
 
 int tz_for(const cfdb_mesh* m) { return m->nz >= 128 ? 128 : (m->nz >= 64 ? 64 : 32); }
 
 }  // namespace
 
+// Upper bound of the fused Euler grid (sizes the per-CTA partials): at most
+// kEulerCtasPerSm resident CTAs per SM are ever requested.
 int euler_fused_grid(const cfdb_euler* e) {
   const int tz = tz_for(e->mesh);
   const stencil::SweepShape sh = stencil::sweep_shape(e->ctx, e->mesh, tz, 8, kEulerCtasPerSm);
@@ -256,22 +262,26 @@ extern "C" int cfdb_euler_create(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, int pat
     return rc;
   }
   cudaMemsetAsync(e->clock, 0, sizeof(EulerClock), ctx->stream);
+  cfdb_adopt(ctx, e, [e] { e->ctx = nullptr; e->clock = nullptr; e->totals = nullptr; e->part = nullptr; });
   *out = e;
   return CFDB_OK;
 }
 
 extern "C" int cfdb_euler_destroy(cfdb_euler* e) {
   if (!e) return CFDB_OK;
-  cudaStreamSynchronize(e->ctx->stream);
-  cfdb_dev_free(e->ctx, e->clock);
-  cfdb_dev_free(e->ctx, e->totals);
-  cfdb_dev_free(e->ctx, e->part);
+  if (e->ctx) {
+    cfdb_release(e->ctx, e);
+    cudaStreamSynchronize(e->ctx->stream);
+    cfdb_dev_free(e->ctx, e->clock);
+    cfdb_dev_free(e->ctx, e->totals);
+    cfdb_dev_free(e->ctx, e->part);
+  }
   delete e;
   return CFDB_OK;
 }
 
 extern "C" int cfdb_euler_begin(cfdb_euler* e, const void* U0) {
-  if (!e) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_euler_begin: handle is NULL");
+  if (!e || !e->ctx) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_euler_begin: handle is NULL or its context was destroyed");
   if (!U0) return cfdb_fail(e->ctx, CFDB_EINVAL, "cfdb_euler_begin: U0 is NULL");
   if (e->path == CFDB_PATH_FUSED && (reinterpret_cast<uintptr_t>(U0) & 15u))
     return cfdb_fail(e->ctx, CFDB_EINVAL, "the fused Euler path needs 16-byte aligned states");
@@ -282,7 +292,7 @@ extern "C" int cfdb_euler_begin(cfdb_euler* e, const void* U0) {
 }
 
 extern "C" int cfdb_euler_step(cfdb_euler* e, const void* U, void* Un) {
-  if (!e) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_euler_step: handle is NULL");
+  if (!e || !e->ctx) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_euler_step: handle is NULL or its context was destroyed");
   if (!U || !Un || U == Un) return cfdb_fail(e->ctx, CFDB_EINVAL, "cfdb_euler_step: need distinct U and U_next");
   CFDB_CUDA(e->ctx, cudaSetDevice(e->ctx->device));
   const int64_t s = e->launches;
@@ -293,7 +303,7 @@ extern "C" int cfdb_euler_step(cfdb_euler* e, const void* U, void* Un) {
 }
 
 extern "C" int cfdb_euler_status(cfdb_euler* e, double* t, int64_t* steps_done, int* finished) {
-  if (!e) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_euler_status: handle is NULL");
+  if (!e || !e->ctx) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_euler_status: handle is NULL or its context was destroyed");
   EulerClock ck;
   CFDB_CUDA(e->ctx, cudaMemcpyAsync(&ck, e->clock, sizeof(ck), cudaMemcpyDeviceToHost, e->ctx->stream));
   CFDB_CUDA(e->ctx, cudaStreamSynchronize(e->ctx->stream));
@@ -311,7 +321,8 @@ extern "C" int cfdb_euler_status(cfdb_euler* e, double* t, int64_t* steps_done, 
 }
 
 extern "C" int cfdb_euler_totals(cfdb_euler* e, double* out, int64_t max_rows, int64_t* rows) {
-  if (!e || !out || max_rows < 0) return cfdb_fail(e ? e->ctx : nullptr, CFDB_EINVAL, "cfdb_euler_totals: bad arguments");
+  if (!e || !e->ctx || !out || max_rows < 0)
+    return cfdb_fail(e ? e->ctx : nullptr, CFDB_EINVAL, "cfdb_euler_totals: bad arguments");
   int64_t steps = 0;
   if (int rc = cfdb_euler_status(e, nullptr, &steps, nullptr)) return rc;
   const int64_t n = std::min<int64_t>(steps + 1, max_rows);
@@ -322,7 +333,7 @@ extern "C" int cfdb_euler_totals(cfdb_euler* e, double* out, int64_t max_rows, i
 
 extern "C" int cfdb_euler_run(cfdb_euler* e, void* Ua, void* Ub, int64_t check_every, int64_t* steps_done,
                               int* final_in_b) {
-  if (!e) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_euler_run: handle is NULL");
+  if (!e || !e->ctx) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_euler_run: handle is NULL or its context was destroyed");
   if (!Ua || !Ub || Ua == Ub || check_every < 1)
     return cfdb_fail(e->ctx, CFDB_EINVAL, "cfdb_euler_run: need distinct buffers and check_every >= 1");
   if (e->launches & 1) return cfdb_fail(e->ctx, CFDB_EINVAL, "cfdb_euler_run: call after cfdb_euler_begin or an even number of steps");

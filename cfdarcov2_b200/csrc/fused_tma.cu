@@ -4,6 +4,9 @@
 // Replaces the reference's per-equation JIT kernel (src/fvm3d.cpp:1219-1394),
 // which streamed ~180 B/cell of geometry per step; on a uniform mesh the
 // geometry reduces to three spacings.
+#include <cstdlib>
+#include <string>
+
 #include "tma_host.hpp"
 
 namespace {
@@ -13,16 +16,18 @@ namespace {
 // point to the cell itself, src/mesh3d.cpp:273-276).
 struct HeatPhys {
   static constexpr int NF = 1;
+  static constexpr int NA = 0;
   static constexpr bool HAS_C = false;
+  static constexpr int MIN_BLOCKS = 4;
   struct Params { float cx, cy, cz; };  // dt k / h_d^2
   struct Acc {};
   __device__ static bool begin(Params&) { return true; }
   __device__ static void ghost(float g[NF], const float p[NF], int) { g[0] = p[0]; }
-  __device__ static void cell(const float P[NF], const float nb[6][NF], const float*, const Params& a, float o[NF]) {
-    const float t = P[0];
-    const float lx = (nb[1][0] - t) + (nb[0][0] - t);
-    const float ly = (nb[3][0] - t) + (nb[2][0] - t);
-    const float lz = (nb[5][0] - t) + (nb[4][0] - t);
+  __device__ static void cell(const stencil::CellIn<1>& in, const Params& a, float o[NF]) {
+    const float t = in.P[0];
+    const float lx = (in.nb[1][0] - t) + (in.nb[0][0] - t);
+    const float ly = (in.nb[3][0] - t) + (in.nb[2][0] - t);
+    const float lz = (in.nb[5][0] - t) + (in.nb[4][0] - t);
     o[0] = t + (a.cx * lx + (a.cy * ly + a.cz * lz));
   }
   __device__ static void acc_init(Acc&) {}
@@ -37,26 +42,48 @@ struct HeatPhys {
 // (mode 1).  Reflective walls: ghost = P with the wall-normal velocity negated.
 template <bool C_FIELD> struct WavePhys {
   static constexpr int NF = 4;
+  static constexpr int NA = 0;
   static constexpr bool HAS_C = C_FIELD;
-  struct Params { float dt, ih[3], c; int mode; };
+  static constexpr int FT = C_FIELD ? 5 : 4;
+  static constexpr int MIN_BLOCKS = 2;
+  // k2[d] = dt c^2 ih_d / 2, kc[d] = dt c ih_d / 2, kp[d] = dt ih_d / 2 (constant c)
+  struct Params { float dt, ih[3], c; int mode; float k2[3], kc[3], kp[3]; };
   struct Acc {};
   __device__ static bool begin(Params&) { return true; }
-  __device__ static void ghost(float g[NF], const float p[NF], int dir) {
+  __device__ static void ghost(float g[FT], const float p[FT], int dir) {
 #pragma unroll
-    for (int f = 0; f < NF; ++f) g[f] = p[f];
+    for (int f = 0; f < FT; ++f) g[f] = p[f];
     g[1 + dir] = -p[1 + dir];
   }
-  __device__ static void cell(const float P[NF], const float nb[6][NF], const float* cc, const Params& a, float o[NF]) {
-    const float cP = C_FIELD ? cc[0] : a.c;
+  __device__ static void cell(const stencil::CellIn<FT>& in, const Params& a, float o[NF]) {
+    const float* P = in.P;
+    if (!C_FIELD) {
+      // constant c: the Rusanov dissipation is a 7-point Laplacian with weight c/2
+      //   p'   = p   - sum_d [k2_d (u_d+ - u_d-) - kc_d (p_d+ + p_d- - 2p)]
+      //   u_e' = u_e - kp_e (p_e+ - p_e-) + sum_d kc_d (u_e,d+ + u_e,d- - 2 u_e)
+      float op = P[0], ou[3] = {P[1], P[2], P[3]};
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const float* m = in.nb[2 * d];
+        const float* p = in.nb[2 * d + 1];
+        op -= a.k2[d] * (p[1 + d] - m[1 + d]) - a.kc[d] * ((p[0] + m[0]) - 2.0f * P[0]);
+        ou[d] -= a.kp[d] * (p[0] - m[0]);
+#pragma unroll
+        for (int e = 0; e < 3; ++e) ou[e] += a.kc[d] * ((p[1 + e] + m[1 + e]) - 2.0f * P[1 + e]);
+      }
+      o[0] = op; o[1] = ou[0]; o[2] = ou[1]; o[3] = ou[2];
+      return;
+    }
+    const float cP = C_FIELD ? P[FT - 1] : a.c;
     const float c2 = cP * cP;
     float rp = 0.f, ru[3] = {0.f, 0.f, 0.f};
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      const float* m = nb[2 * d];
-      const float* p = nb[2 * d + 1];
+      const float* m = in.nb[2 * d];
+      const float* p = in.nb[2 * d + 1];
       float hm, hp;
       if (C_FIELD) {
-        const float cm = cc[1 + 2 * d], cpl = cc[2 + 2 * d];
+        const float cm = m[FT - 1], cpl = p[FT - 1];
         hm = 0.5f * (a.mode == 0 ? fmaxf(cP, cm) : 0.5f * (cP + cm));
         hp = 0.5f * (a.mode == 0 ? fmaxf(cP, cpl) : 0.5f * (cP + cpl));
       } else {
@@ -84,9 +111,28 @@ template <bool C_FIELD> struct WavePhys {
 template <class Phys, int S>
 int dispatch_tz(cfdb_ctx* ctx, const cfdb_mesh* m, const void* q, void* out, const void* c,
                 const typename Phys::Params& prm, int ctas_per_sm) {
-  if (m->nz >= 128) return stencil::launch_sweep<Phys, 128, 8, S>(ctx, m, q, out, c, prm, ctas_per_sm);
-  if (m->nz >= 64) return stencil::launch_sweep<Phys, 64, 8, S>(ctx, m, q, out, c, prm, ctas_per_sm);
-  return stencil::launch_sweep<Phys, 32, 8, S>(ctx, m, q, out, c, prm, ctas_per_sm);
+  if (m->nz >= 128) return stencil::launch_sweep<Phys, 128, 8, S>(ctx, m, q, nullptr, c, out, prm, ctas_per_sm);
+  if (m->nz >= 64) return stencil::launch_sweep<Phys, 64, 8, S>(ctx, m, q, nullptr, c, out, prm, ctas_per_sm);
+  return stencil::launch_sweep<Phys, 32, 8, S>(ctx, m, q, nullptr, c, out, prm, ctas_per_sm);
+}
+
+// Tile shape of the constant-c wave sweep.  CFDB_WAVE_TILE=TZxTYxS picks one of
+// the instantiated shapes (for tuning sweeps); the default is 128x8x3 (three
+// staged planes: the shape that measured fastest on meshes beyond L2).
+int dispatch_wave_tiles(cfdb_ctx* ctx, const cfdb_mesh* m, const void* q, void* qn,
+                        const WavePhys<false>::Params& p) {
+  using W = WavePhys<false>;
+  static const char* env = getenv("CFDB_WAVE_TILE");
+  const std::string t = env ? env : "";
+  if (m->nz >= 128) {
+    if (t == "128x4x4") return stencil::launch_sweep<W, 128, 4, 4>(ctx, m, q, nullptr, nullptr, qn, p, 0);
+    if (t == "128x8x4") return stencil::launch_sweep<W, 128, 8, 4>(ctx, m, q, nullptr, nullptr, qn, p, 0);
+    if (t == "64x8x4") return stencil::launch_sweep<W, 64, 8, 4>(ctx, m, q, nullptr, nullptr, qn, p, 0);
+    if (t == "128x8x4v2") return stencil::launch_sweep<W, 128, 8, 4, 2>(ctx, m, q, nullptr, nullptr, qn, p, 0);
+    if (t == "64x8x4v1") return stencil::launch_sweep<W, 64, 8, 4, 1>(ctx, m, q, nullptr, nullptr, qn, p, 0);
+  }
+  if (m->nz >= 128) return stencil::launch_sweep<W, 128, 8, 3>(ctx, m, q, nullptr, nullptr, qn, p, 0);
+  return dispatch_tz<W, 4>(ctx, m, q, qn, nullptr, p, 0);
 }
 
 }  // namespace
@@ -98,17 +144,23 @@ int fused_heat_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* T, void*
   p.cx = float(dt * k / (m->dx * m->dx));
   p.cy = float(dt * k / (m->dy * m->dy));
   p.cz = float(dt * k / (m->dz * m->dz));
-  return dispatch_tz<HeatPhys, 6>(ctx, m, T, Tn, nullptr, p, 4);
+  return dispatch_tz<HeatPhys, 6>(ctx, m, T, Tn, nullptr, p, 0);
 }
 
 int fused_wave_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* q, void* qn, const void* c, double cconst,
                     int mode, double dt) {
   if (dtype != CFDB_F32) return cfdb_fail(ctx, CFDB_EUNSUPPORTED, "the fused wave step computes in float32 only");
   if (int rc = stencil::check_sweep(ctx, m, {q, qn, c})) return rc;
+  const double ih[3] = {1.0 / m->dx, 1.0 / m->dy, 1.0 / m->dz};
   if (c) {
-    WavePhys<true>::Params p{float(dt), {float(1.0 / m->dx), float(1.0 / m->dy), float(1.0 / m->dz)}, 0.f, mode};
-    return dispatch_tz<WavePhys<true>, 4>(ctx, m, q, qn, c, p, 2);
+    WavePhys<true>::Params p{float(dt), {float(ih[0]), float(ih[1]), float(ih[2])}, 0.f, mode, {}, {}, {}};
+    return dispatch_tz<WavePhys<true>, 4>(ctx, m, q, qn, c, p, 0);
   }
-  WavePhys<false>::Params p{float(dt), {float(1.0 / m->dx), float(1.0 / m->dy), float(1.0 / m->dz)}, float(cconst), mode};
-  return dispatch_tz<WavePhys<false>, 4>(ctx, m, q, qn, nullptr, p, 2);
+  WavePhys<false>::Params p{float(dt), {float(ih[0]), float(ih[1]), float(ih[2])}, float(cconst), mode, {}, {}, {}};
+  for (int d = 0; d < 3; ++d) {
+    p.k2[d] = float(0.5 * dt * cconst * cconst * ih[d]);
+    p.kc[d] = float(0.5 * dt * cconst * ih[d]);
+    p.kp[d] = float(0.5 * dt * ih[d]);
+  }
+  return dispatch_wave_tiles(ctx, m, q, qn, p);
 }

@@ -98,6 +98,9 @@ extern "C" int cfdb_ctx_destroy(cfdb_ctx* ctx) {
   if (!ctx) return CFDB_OK;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
+  if (ctx->capture_stream) cudaStreamDestroy(ctx->capture_stream);
+  auto children = std::move(ctx->children);
+  for (auto& kv : children) kv.second();
   for (auto& kv : ctx->allocs) cudaFree(kv.first);
   ctx->allocs.clear();
   delete ctx;
@@ -187,6 +190,7 @@ extern "C" int cfdb_mesh_create_structured(cfdb_ctx* ctx, int64_t nx, int64_t ny
   m->nx = nx; m->ny = ny; m->nz = nz; m->n = nx * ny * nz;
   m->dx = dx; m->dy = dy; m->dz = dz;
   m->uniform = true;
+  cfdb_adopt(ctx, m, [m] { cfdb_mesh_orphan(m); });
   *out = m;
   return CFDB_OK;
 }
@@ -241,6 +245,7 @@ extern "C" int cfdb_mesh_create_from_vertices(cfdb_ctx* ctx, int64_t nx, int64_t
       }
     }
   }
+  cfdb_adopt(ctx, m, [m] { cfdb_mesh_orphan(m); });
   *out = m;
   return CFDB_OK;
 }
@@ -254,9 +259,19 @@ static void free_plain(cfdb_ctx* ctx, PlainGeomDev& p) {
   p.ready = false;
 }
 
+// The context is going away: its allocations are freed with it.
+void cfdb_mesh_orphan(cfdb_mesh* m) {
+  m->ctx = nullptr;
+  m->plain[0] = PlainGeomDev();
+  m->plain[1] = PlainGeomDev();
+  m->d_ids = nullptr;
+  m->compact = CompactGeomDev();
+}
+
 extern "C" int cfdb_mesh_destroy(cfdb_mesh* m) {
   if (!m) return CFDB_OK;
   if (m->ctx) {
+    cfdb_release(m->ctx, m);
     cudaStreamSynchronize(m->ctx->stream);
     free_plain(m->ctx, m->plain[0]);
     free_plain(m->ctx, m->plain[1]);

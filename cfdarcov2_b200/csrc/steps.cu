@@ -51,3 +51,25 @@ extern "C" int cfdb_wave_adjoint_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, in
     return fused_wave_adjoint(ctx, m, dtype, q, lam1, lam0, c, gc, dt);
   return plain_wave_adjoint(ctx, m, dtype, q, lam1, lam0, c, gc, dt);
 }
+
+extern "C" int cfdb_heat_run(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, int path, void* Ta, void* Tb, double k, double dt,
+                             int32_t steps, int use_graph, int* final_in_b) {
+  if (int rc = check_step(ctx, m, dtype, path, "cfdb_heat_run")) return rc;
+  if (!Ta || !Tb || Ta == Tb) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_heat_run: need distinct T_a and T_b");
+  int rc = cfdb_run_steps(ctx, Ta, Tb, steps, use_graph, [&](const void* src, void* dst) {
+    return cfdb_heat_step(ctx, m, dtype, path, src, dst, k, dt);
+  });
+  if (!rc && final_in_b) *final_in_b = steps & 1;
+  return rc;
+}
+
+extern "C" int cfdb_wave_run(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, int path, void* qa, void* qb, const void* c,
+                             double cconst, int mode, double dt, int32_t steps, int use_graph, int* final_in_b) {
+  if (int rc = check_step(ctx, m, dtype, path, "cfdb_wave_run")) return rc;
+  if (!qa || !qb || qa == qb) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_wave_run: need distinct q_a and q_b");
+  int rc = cfdb_run_steps(ctx, qa, qb, steps, use_graph, [&](const void* src, void* dst) {
+    return cfdb_wave_step(ctx, m, dtype, path, src, dst, c, cconst, mode, dt);
+  });
+  if (!rc && final_in_b) *final_in_b = steps & 1;
+  return rc;
+}

@@ -72,43 +72,53 @@ inline int check_sweep(cfdb_ctx* ctx, const cfdb_mesh* m, std::initializer_list<
 }
 
 struct SweepShape {
-  int tiles, chunks, chunk;
+  int tiles, chunks;
 };
 
-// Chunks along x so that the grid covers ~ctas_per_sm CTAs per SM.
-inline SweepShape sweep_shape(const cfdb_ctx* ctx, const cfdb_mesh* m, int tz, int ty, int ctas_per_sm) {
+// Grid of tiles x chunks CTAs.  resident = CTAs of this kernel one SM holds
+// (occupancy API).  The x axis is cut into as many chunks as fill the
+// resident slots of all SMs in one wave (chunk lengths differ by at most one
+// plane, so every CTA finishes at about the same time); when the tiles alone
+// exceed one wave the grid keeps one chunk per tile.
+inline SweepShape sweep_shape(const cfdb_ctx* ctx, const cfdb_mesh* m, int tz, int ty, int resident) {
   SweepShape s;
   s.tiles = int(((m->nz + tz - 1) / tz) * ((m->ny + ty - 1) / ty));
-  const int target = std::max(1, ctx->num_sms) * ctas_per_sm;
-  int chunks = std::max(1, (target + s.tiles - 1) / s.tiles);
+  const int slots = std::max(1, ctx->num_sms) * std::max(1, resident);
+  int chunks = std::max(1, slots / s.tiles);
   chunks = int(std::min<int64_t>(chunks, m->nx));
-  chunks = std::min(chunks, 65535);
-  s.chunk = int((m->nx + chunks - 1) / chunks);
-  s.chunks = int((m->nx + s.chunk - 1) / s.chunk);
+  s.chunks = std::min(chunks, 65535);
   return s;
 }
 
-template <class Phys, int TZ, int TY, int S>
-int launch_sweep(cfdb_ctx* ctx, const cfdb_mesh* m, const void* q, void* out, const void* c,
+// Launches one sweep: q holds the NF state fields, aux the NA auxiliary
+// fields (may be NULL when NA == 0), c the coefficient field (HAS_C), out
+// receives the NF new state fields.
+template <class Phys, int TZ, int TY, int S, int VZ = 4>
+int launch_sweep(cfdb_ctx* ctx, const cfdb_mesh* m, const void* q, const void* aux, const void* c, void* out,
                  const typename Phys::Params& prm, int ctas_per_sm, int* launched_grid = nullptr) {
-  using L = Layout<TZ, TY, S, Phys::NF, Phys::HAS_C>;
-  CUtensorMap tq, tc;
+  using L = Layout<TZ, TY, S, Phys::NF, Phys::NA, Phys::HAS_C, VZ>;
+  static_assert(TZ % VZ == 0 && (VZ == 1 || VZ == 2 || VZ == 4), "bad vector width");
+  CUtensorMap tq, ta, tc;
   if (int rc = encode_state(ctx, &tq, q, m, Phys::NF, TZ, TY)) return rc;
+  ta = tq;
+  tc = tq;
+  if constexpr (Phys::NA > 0) {
+    if (int rc = encode_state(ctx, &ta, aux, m, Phys::NA, TZ, TY)) return rc;
+  }
   if constexpr (Phys::HAS_C) {
     if (int rc = encode_field(ctx, &tc, c, m, TZ, TY)) return rc;
-  } else {
-    tc = tq;
   }
-  auto kern = sweep_kernel<Phys, TZ, TY, S>;
-  static bool attr_set = false;
-  if (!attr_set) {
+  auto kern = sweep_kernel<Phys, TZ, TY, S, VZ>;
+  static int resident = 0;
+  if (!resident) {
     CFDB_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L::SMEM_BYTES)));
-    attr_set = true;
+    CFDB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kern, L::THREADS, L::SMEM_BYTES));
+    if (resident < 1) return cfdb_fail(ctx, CFDB_EUNSUPPORTED, "sweep kernel does not fit on an SM");
   }
-  const SweepShape sh = sweep_shape(ctx, m, TZ, TY, ctas_per_sm);
-  Geometry g{int(m->nx), int(m->ny), int(m->nz), sh.chunk, (long long)m->n};
+  const SweepShape sh = sweep_shape(ctx, m, TZ, TY, ctas_per_sm > 0 ? std::min(ctas_per_sm, resident) : resident);
+  Geometry g{int(m->nx), int(m->ny), int(m->nz), sh.chunks, (long long)m->n};
   dim3 grid(sh.tiles, sh.chunks);
-  kern<<<grid, L::THREADS, L::SMEM_BYTES, ctx->stream>>>(tq, tc, g, static_cast<float*>(out), prm, ctx->d_error);
+  kern<<<grid, L::THREADS, L::SMEM_BYTES, ctx->stream>>>(tq, ta, tc, g, static_cast<float*>(out), prm, ctx->d_error);
   CFDB_LAUNCHED(ctx);
   if (launched_grid) *launched_grid = sh.tiles * sh.chunks;
   return CFDB_OK;

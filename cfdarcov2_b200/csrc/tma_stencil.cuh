@@ -75,61 +75,105 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 
 // Device error word codes (ctx->d_error[0]).
 constexpr int kErrWaitTimeout = 1;
+constexpr int kErrSmemAlign = 2;
 
 // ---- the sweep -------------------------------------------------------------
 struct Geometry {
   int X, Y, Z;      // cells
-  int chunk;        // x planes per CTA
+  int chunks;       // x chunks; chunk c covers planes [c X / chunks, (c+1) X / chunks)
   long long n;      // X*Y*Z
 };
 
+// Staged fields of one cell and its six neighbours (x-, x+, y-, y+, z-, z+).
+// The FT staged fields are the NF state fields (read from `q`, written to
+// `out`), then NA auxiliary fields (read from `aux`), then the coefficient
+// field c when HAS_C.  Neighbours beyond a wall hold Phys::ghost(P, dir);
+// bit 2*dir + side of `walls` marks them.
+template <int FT> struct CellIn {
+  float P[FT];
+  float nb[6][FT];
+  int walls;
+  long long idx;  // cell id
+};
+
 // Phys provides:
-//   static constexpr int NF;            fields in the state
-//   static constexpr bool HAS_C;        per-cell coefficient field staged too
+//   static constexpr int NF, NA;        state fields (read and written), auxiliary fields (read)
+//   static constexpr bool HAS_C;        a per-cell coefficient field is staged as the last field
+//   static constexpr int MIN_BLOCKS;    resident CTAs per SM the register budget must allow
 //   struct Params;                      kernel parameters (by value)
 //   struct Acc;                         per-thread epilogue accumulator
-//   __device__ static void ghost(float g[NF], const float p[NF], int dir);   dir 0=x,1=y,2=z
-//   __device__ static void cell(const float P[NF], const float nb[6][NF], const float cc[7],
-//                               const Params&, float out[NF]);
-//        nb order: x-, x+, y-, y+, z-, z+; cc: c_P then the 6 neighbours
-//   __device__ static void acc_init(Acc&), acc_cell(Acc&, const float out[NF], const Params&)
-//   __device__ static void finish(Acc&, const Params&, bool thread_active)   (called by all threads)
 //   __device__ static bool begin(Params&)  -> false: skip the sweep (e.g. a finished clock); may
 //        fill per-launch values (a device-side dt) into its copy of the parameters
-template <int TZ, int TY, int S, int NF, bool HAS_C> struct Layout {
+//   __device__ static void ghost(float g[FT], const float p[FT], int dir);   dir 0=x,1=y,2=z
+//   __device__ static void cell(const CellIn<FT>&, const Params&, float out[NF]);
+//   __device__ static void acc_init(Acc&), acc_cell(Acc&, const float out[NF], const Params&)
+//   __device__ static void finish(Acc&, const Params&, bool thread_active)   (called by all threads)
+template <int TZ, int TY, int S, int NF, int NA, bool HAS_C, int VZ> struct Layout {
+  static constexpr int FT = NF + NA + (HAS_C ? 1 : 0);  // staged fields
   static constexpr int RL = TZ + 8;                       // row length (floats)
   static constexpr int RR = TY + 2;                       // rows
   static constexpr int TILE = RL * RR;                    // floats per field tile
-  static constexpr int C_OFF = (NF * TILE + 31) / 32 * 32;
-  static constexpr int SLOT = (C_OFF + (HAS_C ? TILE : 0) + 31) / 32 * 32;  // 128-byte multiple
-  static constexpr uint32_t TX_BYTES = uint32_t(4 * (NF * TILE + (HAS_C ? TILE : 0)));
-  static constexpr size_t SMEM_BYTES = size_t(S) * SLOT * 4 + 128;
-  static constexpr int THREADS = (TZ / 4) * TY;
+  static constexpr int A_OFF = (NF * TILE + 31) / 32 * 32;              // 128-byte aligned
+  static constexpr int C_OFF = (A_OFF + NA * TILE + 31) / 32 * 32;      // 128-byte aligned
+  static constexpr int SLOT = (C_OFF + (HAS_C ? TILE : 0) + 31) / 32 * 32;
+  static constexpr uint32_t TX_BYTES = uint32_t(4 * TILE * FT);
+  static constexpr size_t SMEM_BYTES = size_t(S) * SLOT * 4;
+  static constexpr int THREADS = (TZ / VZ) * TY;
+  __host__ __device__ static constexpr int off(int f) {
+    return f < NF ? f * TILE : (f < NF + NA ? A_OFF + (f - NF) * TILE : C_OFF);
+  }
 };
 
-template <class Phys, int TZ, int TY, int S>
-__global__ void __launch_bounds__((TZ / 4) * TY)
-    sweep_kernel(const __grid_constant__ CUtensorMap tm_q, const __grid_constant__ CUtensorMap tm_c, Geometry g,
-                 float* __restrict__ out, typename Phys::Params prm, int* __restrict__ err) {
+template <int VZ> __device__ __forceinline__ void ldv(const float* p, float* v) {
+  if constexpr (VZ == 4) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+  } else if constexpr (VZ == 2) {
+    const float2 t = *reinterpret_cast<const float2*>(p);
+    v[0] = t.x; v[1] = t.y;
+  } else {
+    v[0] = *p;
+  }
+}
+
+template <int VZ> __device__ __forceinline__ void stv(float* p, const float* v) {
+  if constexpr (VZ == 4) *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  else if constexpr (VZ == 2) *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+  else *p = v[0];
+}
+
+template <class Phys, int TZ, int TY, int S, int VZ>
+__global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
+    sweep_kernel(const __grid_constant__ CUtensorMap tm_q, const __grid_constant__ CUtensorMap tm_a,
+                 const __grid_constant__ CUtensorMap tm_c, Geometry g, float* __restrict__ out,
+                 typename Phys::Params prm, int* __restrict__ err) {
   constexpr int NF = Phys::NF;
-  using L = Layout<TZ, TY, S, NF, Phys::HAS_C>;
-  extern __shared__ unsigned char smem_raw[];
+  constexpr int NA = Phys::NA;
+  using L = Layout<TZ, TY, S, NF, NA, Phys::HAS_C, VZ>;
+  constexpr int FT = L::FT;
+  // Indexing the extern array directly keeps the accesses in the shared
+  // address space (LDS, not generic loads); its start must be 128-byte aligned
+  // for TMA, which is checked before the first copy is issued.
+  extern __shared__ __align__(128) float smem[];
   __shared__ __align__(8) uint64_t bars[S];
-  float* smem = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
 
   const int ntz = (g.Z + TZ - 1) / TZ;
   const int z0 = (blockIdx.x % ntz) * TZ;
   const int y0 = (blockIdx.x / ntz) * TY;
-  const int x0 = blockIdx.y * g.chunk;
-  const int x1 = min(g.X, x0 + g.chunk);
+  const int x0 = int((long long)blockIdx.y * g.X / g.chunks);
+  const int x1 = int((long long)(blockIdx.y + 1) * g.X / g.chunks);
   if (x0 >= x1) return;
+  if (smem_u32(smem) & 127u) {
+    if (threadIdx.x == 0) atomicExch(err, kErrSmemAlign);
+    return;
+  }
   typename Phys::Params P = prm;
   if (!Phys::begin(P)) return;
 
-  const int tz = threadIdx.x % (TZ / 4);
-  const int ty = threadIdx.x / (TZ / 4);
+  const int tz = threadIdx.x % (TZ / VZ);
+  const int ty = threadIdx.x / (TZ / VZ);
   const int y = y0 + ty;
-  const int zb = z0 + 4 * tz;
+  const int zb = z0 + VZ * tz;
   const bool active = (y < g.Y) && (zb < g.Z);
   const int kmax = x1 - x0 + 1;  // plane k <-> x = x0 - 1 + k
 
@@ -146,6 +190,7 @@ __global__ void __launch_bounds__((TZ / 4) * TY)
     float* dst = smem + s * L::SLOT;
     mbar_expect_tx(&bars[s], L::TX_BYTES);
     tma_load_4d(dst, &tm_q, z0 - 4, y0 - 1, x, 0, &bars[s]);
+    if constexpr (NA > 0) tma_load_4d(dst + L::A_OFF, &tm_a, z0 - 4, y0 - 1, x, 0, &bars[s]);
     if constexpr (Phys::HAS_C) tma_load_3d(dst + L::C_OFF, &tm_c, z0 - 4, y0 - 1, x, &bars[s]);
   };
   if (threadIdx.x == 0)
@@ -158,44 +203,32 @@ __global__ void __launch_bounds__((TZ / 4) * TY)
     if (!mbar_wait_bounded(&bars[s], (parity >> s) & 1u)) bad = true;
     parity ^= 1u << s;
   };
-  const int ctr = (ty + 1) * L::RL + 4 + 4 * tz;  // thread's float4 in a field tile
-  auto load_center = [&](int k, float v[NF][4], float c4[4]) {
+  const int ctr = (ty + 1) * L::RL + 4 + VZ * tz;  // thread's first cell in a field tile
+  auto load_center = [&](int k, float v[FT][VZ]) {
     const float* base = smem + (k % S) * L::SLOT;
 #pragma unroll
-    for (int f = 0; f < NF; ++f) {
-      const float4 t = *reinterpret_cast<const float4*>(base + f * L::TILE + ctr);
-      v[f][0] = t.x; v[f][1] = t.y; v[f][2] = t.z; v[f][3] = t.w;
-    }
-    if constexpr (Phys::HAS_C) {
-      const float4 t = *reinterpret_cast<const float4*>(base + L::C_OFF + ctr);
-      c4[0] = t.x; c4[1] = t.y; c4[2] = t.z; c4[3] = t.w;
-    }
+    for (int f = 0; f < FT; ++f) ldv<VZ>(base + L::off(f) + ctr, v[f]);
   };
-  auto ghost4 = [&](float dst[NF][4], const float src[NF][4], int dir) {
+  auto ghostv = [&](float dst[FT][VZ], const float src[FT][VZ], int dir) {
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      float a[NF], b[NF];
+    for (int j = 0; j < VZ; ++j) {
+      float a[FT], b[FT];
 #pragma unroll
-      for (int f = 0; f < NF; ++f) a[f] = src[f][j];
+      for (int f = 0; f < FT; ++f) a[f] = src[f][j];
       Phys::ghost(b, a, dir);
 #pragma unroll
-      for (int f = 0; f < NF; ++f) dst[f][j] = b[f];
+      for (int f = 0; f < FT; ++f) dst[f][j] = b[f];
     }
   };
 
-  float prv[NF][4], cur[NF][4], nxt[NF][4];
-  float cprv[4] = {0, 0, 0, 0}, ccur[4] = {0, 0, 0, 0}, cnxt[4] = {0, 0, 0, 0};
+  float prv[FT][VZ], cur[FT][VZ], nxt[FT][VZ];
   if (x0 > 0) {
     wait_plane(0);
-    load_center(0, prv, cprv);
+    load_center(0, prv);
   }
   wait_plane(1);
-  load_center(1, cur, ccur);
-  if (x0 == 0) {
-    ghost4(prv, cur, 0);
-#pragma unroll
-    for (int j = 0; j < 4; ++j) cprv[j] = ccur[j];
-  }
+  load_center(1, cur);
+  if (x0 == 0) ghostv(prv, cur, 0);
   __syncthreads();
   if (threadIdx.x == 0) {
     fence_proxy_async();
@@ -205,83 +238,64 @@ __global__ void __launch_bounds__((TZ / 4) * TY)
   typename Phys::Acc acc;
   Phys::acc_init(acc);
   const long long plane = (long long)g.Y * g.Z;
+  const int wy = (y == 0 ? 4 : 0) | (y == g.Y - 1 ? 8 : 0);
 
   for (int x = x0; x < x1; ++x) {
     const int k = x - x0 + 1;
     if (x + 1 < g.X) {
       wait_plane(k + 1);
-      load_center(k + 1, nxt, cnxt);
+      load_center(k + 1, nxt);
     } else {
-      ghost4(nxt, cur, 0);
-#pragma unroll
-      for (int j = 0; j < 4; ++j) cnxt[j] = ccur[j];
+      ghostv(nxt, cur, 0);
     }
     if (active) {
       const float* base = smem + (k % S) * L::SLOT;
-      float ym[NF][4], yp[NF][4], zl[NF], zr[NF];
-      float cym[4], cyp[4], czl = 0.f, czr = 0.f;
+      float ym[FT][VZ], yp[FT][VZ], zl[FT], zr[FT];
 #pragma unroll
-      for (int f = 0; f < NF; ++f) {
-        const float* t = base + f * L::TILE;
-        const float4 a = *reinterpret_cast<const float4*>(t + ctr - L::RL);
-        const float4 b = *reinterpret_cast<const float4*>(t + ctr + L::RL);
-        ym[f][0] = a.x; ym[f][1] = a.y; ym[f][2] = a.z; ym[f][3] = a.w;
-        yp[f][0] = b.x; yp[f][1] = b.y; yp[f][2] = b.z; yp[f][3] = b.w;
+      for (int f = 0; f < FT; ++f) {
+        const float* t = base + L::off(f);
+        ldv<VZ>(t + ctr - L::RL, ym[f]);
+        ldv<VZ>(t + ctr + L::RL, yp[f]);
         zl[f] = t[ctr - 1];
-        zr[f] = t[ctr + 4];
+        zr[f] = t[ctr + VZ];
       }
-      if constexpr (Phys::HAS_C) {
-        const float* t = base + L::C_OFF;
-        const float4 a = *reinterpret_cast<const float4*>(t + ctr - L::RL);
-        const float4 b = *reinterpret_cast<const float4*>(t + ctr + L::RL);
-        cym[0] = a.x; cym[1] = a.y; cym[2] = a.z; cym[3] = a.w;
-        cyp[0] = b.x; cyp[1] = b.y; cyp[2] = b.z; cyp[3] = b.w;
-        czl = t[ctr - 1];
-        czr = t[ctr + 4];
-      }
-      if (y == 0) {
-        ghost4(ym, cur, 1);
-        if constexpr (Phys::HAS_C) for (int j = 0; j < 4; ++j) cym[j] = ccur[j];
-      }
-      if (y == g.Y - 1) {
-        ghost4(yp, cur, 1);
-        if constexpr (Phys::HAS_C) for (int j = 0; j < 4; ++j) cyp[j] = ccur[j];
-      }
-      float res[NF][4];
+      if (wy & 4) ghostv(ym, cur, 1);
+      if (wy & 8) ghostv(yp, cur, 1);
+      const int wx = (x == 0 ? 1 : 0) | (x == g.X - 1 ? 2 : 0);
+      float res[NF][VZ];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        float Pc[NF], nb[6][NF], cc[7];
+      for (int j = 0; j < VZ; ++j) {
+        CellIn<FT> in;
 #pragma unroll
-        for (int f = 0; f < NF; ++f) {
-          Pc[f] = cur[f][j];
-          nb[0][f] = prv[f][j];
-          nb[1][f] = nxt[f][j];
-          nb[2][f] = ym[f][j];
-          nb[3][f] = yp[f][j];
-          nb[4][f] = j == 0 ? zl[f] : cur[f][j - 1];
-          nb[5][f] = j == 3 ? zr[f] : cur[f][j + 1];
+        for (int f = 0; f < FT; ++f) {
+          in.P[f] = cur[f][j];
+          in.nb[0][f] = prv[f][j];
+          in.nb[1][f] = nxt[f][j];
+          in.nb[2][f] = ym[f][j];
+          in.nb[3][f] = yp[f][j];
+          in.nb[4][f] = j == 0 ? zl[f] : cur[f][j - 1];
+          in.nb[5][f] = j == VZ - 1 ? zr[f] : cur[f][j + 1];
         }
-        if (j == 0 && zb == 0) Phys::ghost(nb[4], Pc, 2);
-        if (j == 3 && zb + 3 == g.Z - 1) Phys::ghost(nb[5], Pc, 2);
-        if constexpr (Phys::HAS_C) {
-          cc[0] = ccur[j];
-          cc[1] = cprv[j]; cc[2] = cnxt[j]; cc[3] = cym[j]; cc[4] = cyp[j];
-          cc[5] = j == 0 ? (zb == 0 ? ccur[0] : czl) : ccur[j - 1];
-          cc[6] = j == 3 ? (zb + 3 == g.Z - 1 ? ccur[3] : czr) : ccur[j + 1];
-        } else {
-#pragma unroll
-          for (int q = 0; q < 7; ++q) cc[q] = 0.f;
+        int w = wx | wy;
+        if (j == 0 && zb == 0) {
+          Phys::ghost(in.nb[4], in.P, 2);
+          w |= 16;
         }
+        if (j == VZ - 1 && zb + VZ - 1 == g.Z - 1) {
+          Phys::ghost(in.nb[5], in.P, 2);
+          w |= 32;
+        }
+        in.walls = w;
+        in.idx = (long long)x * plane + (long long)y * g.Z + zb + j;
         float o[NF];
-        Phys::cell(Pc, nb, cc, P, o);
+        Phys::cell(in, P, o);
         Phys::acc_cell(acc, o, P);
 #pragma unroll
         for (int f = 0; f < NF; ++f) res[f][j] = o[f];
       }
       const long long idx = (long long)x * plane + (long long)y * g.Z + zb;
 #pragma unroll
-      for (int f = 0; f < NF; ++f)
-        *reinterpret_cast<float4*>(out + f * g.n + idx) = make_float4(res[f][0], res[f][1], res[f][2], res[f][3]);
+      for (int f = 0; f < NF; ++f) stv<VZ>(out + f * g.n + idx, res[f]);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -289,17 +303,12 @@ __global__ void __launch_bounds__((TZ / 4) * TY)
       issue(k + S);
     }
 #pragma unroll
-    for (int f = 0; f < NF; ++f)
+    for (int f = 0; f < FT; ++f)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
+      for (int j = 0; j < VZ; ++j) {
         prv[f][j] = cur[f][j];
         cur[f][j] = nxt[f][j];
       }
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      cprv[j] = ccur[j];
-      ccur[j] = cnxt[j];
-    }
   }
   if (bad) atomicExch(err, kErrWaitTimeout);
   Phys::finish(acc, P, active);

@@ -214,6 +214,16 @@ int cfdb_heat_step(cfdb_ctx* ctx, cfdb_mesh* mesh, int dtype, int path, const vo
 int cfdb_wave_step(cfdb_ctx* ctx, cfdb_mesh* mesh, int dtype, int path, const void* q, void* q_next,
                    const void* c_field, double c_const, int speed_mode, double dt);
 
+/* The time loop of Equation::evaluate (src/fvm3d.cpp:1008-1058) for a single
+ * equation: `steps` steps alternating a -> b -> a ...; *final_in_b = 1 when
+ * the last state is in b.  use_graph captures the step launches into a CUDA
+ * graph (after two eager steps that perform any one-time setup) and replays
+ * it, so host launch latency never gaps the device.  Asynchronous. */
+int cfdb_heat_run(cfdb_ctx* ctx, cfdb_mesh* mesh, int dtype, int path, void* T_a, void* T_b, double k, double dt,
+                  int32_t steps, int use_graph, int* final_in_b);
+int cfdb_wave_run(cfdb_ctx* ctx, cfdb_mesh* mesh, int dtype, int path, void* q_a, void* q_b, const void* c_field,
+                  double c_const, int speed_mode, double dt, int32_t steps, int use_graph, int* final_in_b);
+
 /* Stable step for cfdb_wave_step: cfl * min_P 2 V_P / sum_f c_P A_f
  * (= cfl / sum_d c/dx_d on a uniform mesh).  c_host (n doubles) may be NULL. */
 int cfdb_wave_dt(const cfdb_mesh* mesh, const double* c_host, double c_const, double cfl, double* dt_out);
