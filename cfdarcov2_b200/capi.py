@@ -79,6 +79,7 @@ PROTOTYPES = {
     "cfdb_op_boundary_copy": (_I, [_P, _P, _I, _P, _P, _P]),
     "cfdb_cfl_dt": (_I, [_P, _P, _I, _D, _D, _P, _P, _P, _P, _P, _PD]),
     "cfdb_total_fp64": (_I, [_P, _P, _I, _P, _PD]),
+    "cfdb_total_fp64_noalloc": (_I, [_I, _P, _P, _D, _I64, _P, _P]),
     "cfdb_heat_step": (_I, [_P, _P, _I, _I, _P, _P, _D, _D]),
     "cfdb_wave_step": (_I, [_P, _P, _I, _I, _P, _P, _P, _D, _I, _D]),
     "cfdb_wave_dt": (_I, [_P, _P, _D, _D, _PD]),

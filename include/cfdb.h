@@ -197,6 +197,25 @@ int cfdb_cfl_dt(cfdb_ctx* ctx, cfdb_mesh* mesh, int dtype, double cfl, double ga
  * src/fvm3d.cpp:1060-1066). */
 int cfdb_total_fp64(cfdb_ctx* ctx, cfdb_mesh* mesh, int dtype, const void* field, double* out);
 
+/* The same compensated FP64 total, sum_P field_P * V_P, for callers that may
+ * not allocate device memory (a plugin whose host application owns every
+ * device allocation, a step recorded into another framework's CUDA graph, a
+ * loop that cannot pay for cudaMalloc's implicit synchronisation).  It needs
+ * no context and calls no cudaMalloc, cudaFree or allocating routine: its
+ * reduction scratch is a fixed 1 MiB array inside the library, held by every
+ * GPU that loads the library until exit.  No counterpart in the reference.
+ * field: n values of dtype on the current device; volumes: n per-cell
+ * volumes of dtype, or NULL to use `volume` for every cell; out_device: one
+ * double in device memory receiving the total; stream: a cudaStream_t (NULL =
+ * default).  Asynchronous.  n may be at most 268,435,456 cells (larger n
+ * returns CFDB_EINVAL without launching).  Every call overwrites the scratch
+ * it uses, so nothing needs clearing, but all calls share it: calls that
+ * overlap on the GPU race and must be serialised by the caller.  The first
+ * call on a device looks up the scratch's device address; make it before any
+ * stream capture.  Errors are read with cfdb_last_error(NULL). */
+int cfdb_total_fp64_noalloc(int dtype, const void* field, const void* volumes, double volume, int64_t n,
+                            void* stream, double* out_device);
+
 /* ---- fused time steps (KernelBuilder replacement, src/fvm3d.cpp:1219-1394) */
 
 /* Heat equation d1t(T) = k * lapl(T) with zero-gradient walls
