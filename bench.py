@@ -39,8 +39,13 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="native", choices=["native", "reference"])
     p.add_argument("--n", type=int, default=128, help="cells per edge")
-    p.add_argument("--tsteps", type=int, default=500, help="time steps per bench step")
+    p.add_argument("--tsteps", type=int, default=None,
+                   help="time steps per bench step (wave 500, heat 200, ensemble 300, adjoint 400; sod: cap on steps)")
     p.add_argument("--no-extras", action="store_true", help="skip the FP64, large-mesh and CPU side measurements")
+    p.add_argument("--eager", action="store_true",
+                   help="launch every step eagerly instead of replaying CUDA graphs (for profilers that skip graph nodes)")
+    p.add_argument("--workload", default="wave", choices=["wave", "heat", "wave_distorted", "sod", "ensemble", "adjoint"],
+                   help="wave (default) is the headline; the others measure the remaining workloads on one GPU")
     return p.parse_args()
 
 
@@ -153,6 +158,8 @@ def run_reference(args, rank):
     from oracle import oracle as O
     from cfdarcov2_b200.workloads import wave_config
     n = args.n
+    if args.tsteps is None:
+        args.tsteps = 500
     cfg = wave_config(n=n)
     m = O.Mesh(n, n, n, cfg["dx"], cfg["dx"], cfg["dx"], dtype=np.float32)
     per_step = 2  # time steps in one bounded sample
@@ -176,6 +183,8 @@ def run_reference(args, rank):
 
 # ---------------------------------------------------------------------------
 def run_native(args, rank, world, local_rank):
+    if args.tsteps is None:
+        args.tsteps = 500
     import numpy as np
     import torch
     import torch.distributed as dist
@@ -198,7 +207,7 @@ def run_native(args, rank, world, local_rank):
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
     def solve():
-        return ctx.wave_run(mesh, a, b, cfg["dt"], T, c_const=cfg["c"], path=cfdb.FUSED, use_graph=True)
+        return ctx.wave_run(mesh, a, b, cfg["dt"], T, c_const=cfg["c"], path=cfdb.FUSED, use_graph=not args.eager)
 
     def barrier():
         if world > 1:
@@ -335,13 +344,205 @@ def extras(ctx, cfdb, mesh, cfg, q0, a, b, flush, dev, n, T, peak, world):
     return out
 
 
+# ---------------------------------------------------------------------------
+# secondary workloads (one GPU): heat, distorted wave, Sod, ensemble, adjoint
+# ---------------------------------------------------------------------------
+def _timed(fn, steps, warmup, flush, prep=None):
+    """Device ms of `steps` calls of fn, each after an L2 flush and prep()."""
+    import torch
+    for _ in range(warmup):
+        if prep:
+            prep()
+        fn()
+    torch.cuda.synchronize()
+    total = 0.0
+    for _ in range(steps):
+        flush.zero_()
+        if prep:
+            prep()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        fn()
+        e.record()
+        torch.cuda.synchronize()
+        total += s.elapsed_time(e)
+    return total
+
+
+def _line(args, workload, value, ms_per_step, cfg, alg_bytes_per_update, updates_per_launch, launches_per_step,
+          extra, dtype="f32"):
+    peak, kind = measured_peak_hbm()
+    launch_ms = ms_per_step / launches_per_step
+    ach = alg_bytes_per_update * updates_per_launch / (launch_ms * 1e-3) / 1e9
+    line = {"metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded)", "config": dict(cfg, workload=workload),
+            "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                         "traffic": None, "peak_source": f"{kind} hbm_gbs",
+                         "algorithmic_bytes_per_cell_update": alg_bytes_per_update},
+            "gpu_launches": args.steps * launches_per_step}
+    line.update(extra)
+    print(json.dumps(line), flush=True)
+
+
+def run_secondary(args):
+    import numpy as np
+    import torch
+
+    import cfdarcov2_b200 as cfdb
+    from cfdarcov2_b200 import workloads as W
+
+    dev = torch.device("cuda", 0)
+    ctx = cfdb.Context(0)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    K, Wm = args.steps, args.warmup
+
+    def l2(a, b):
+        a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b)), float(np.abs(a - b).max() / np.abs(b).max())
+
+    if args.workload == "heat":
+        cfg = W.heat_config(steps=args.tsteps or 200)
+        n, T = cfg["n"], cfg["steps"]
+        m = cfdb.Mesh.structured(ctx, n, n, n, cfg["dx"], cfg["dx"], cfg["dx"])
+        res = {}
+        for name, dt_, path in (("fp32_fused", torch.float32, cfdb.FUSED), ("fp64_plain", torch.float64, cfdb.PLAIN))[: 1 if args.no_extras else 2]:
+            T0 = torch.tensor(cfg["T0"], dtype=dt_, device=dev)
+            a, b = torch.empty_like(T0), torch.empty_like(T0)
+            out = {}
+            ms = _timed(lambda: out.__setitem__("f", ctx.heat_run(m, a, b, cfg["k"], cfg["dt"], T, path=path, use_graph=not args.eager)),
+                        K, Wm, flush, prep=lambda: a.copy_(T0))
+            res[name] = (n ** 3 * T * K / (ms * 1e-3), ms / K, out["f"].double().cpu().numpy())
+        if args.no_extras:
+            res["fp64_plain"] = res["fp32_fused"]
+        err = l2(res["fp32_fused"][2], res["fp64_plain"][2])
+        _line(args, "heat3d_64^3_x200_steps", res["fp32_fused"][0], res["fp32_fused"][1],
+              {"mesh": [n] * 3, "k": cfg["k"], "dt": cfg["dt"], "time_steps_per_bench_step": T}, 8, n ** 3, T,
+              {"fp64_plain": {"value": res["fp64_plain"][0], "unit": "cell-updates/s"},
+               "speedup_fused_fp32_vs_plain_fp64": res["fp32_fused"][0] / res["fp64_plain"][0],
+               "accuracy_vs_fp64": {"l2_rel": err[0], "linf_rel": err[1]}})
+    elif args.workload == "wave_distorted":
+        cfg = W.wave_config(n=args.n, steps=args.tsteps or 500)
+        n, T = cfg["n"], cfg["steps"]
+        V = W.jittered_vertices(n, seed=2)
+        m = cfdb.Mesh.from_vertices(ctx, n, n, n, cfg["dx"], cfg["dx"], cfg["dx"], V)
+        dt = m.wave_dt(0.4)
+        res = {}
+        for name, dt_, path in (("fp32_fused", torch.float32, cfdb.FUSED), ("fp64_plain", torch.float64, cfdb.PLAIN))[: 1 if args.no_extras else 2]:
+            q0 = torch.tensor(cfg["q0"], dtype=dt_, device=dev)
+            a, b = torch.empty_like(q0), torch.empty_like(q0)
+            out = {}
+            ms = _timed(lambda: out.__setitem__("f", ctx.wave_run(m, a, b, dt, T, path=path, use_graph=not args.eager)), K, Wm, flush,
+                        prep=lambda: a.copy_(q0))
+            res[name] = (n ** 3 * T * K / (ms * 1e-3), ms / K, out["f"].double().cpu().numpy())
+        if args.no_extras:
+            res["fp64_plain"] = res["fp32_fused"]
+        err = l2(res["fp32_fused"][2], res["fp64_plain"][2])
+        _line(args, f"wave3d_rusanov_{n}^3_x{T}_steps_jittered_0.2dx", res["fp32_fused"][0], res["fp32_fused"][1],
+              {"mesh": [n] * 3, "jitter": "U(-0.2,0.2) dx, seed 2", "path": "compact area-vector gather"}, 72, n ** 3,
+              T, {"fp64_plain": {"value": res["fp64_plain"][0], "unit": "cell-updates/s"},
+                  "speedup_fused_fp32_vs_plain_fp64": res["fp32_fused"][0] / res["fp64_plain"][0],
+                  "accuracy_vs_fp64": {"l2_rel": err[0], "linf_rel": err[1]}})
+    elif args.workload == "sod":
+        from oracle import riemann
+        cfg = W.sod_config()
+        nx, ny, nz = cfg["nx"], cfg["ny"], cfg["nz"]
+        m = cfdb.Mesh.structured(ctx, nx, ny, nz, cfg["dx"], cfg["dy"], cfg["dz"])
+        res = {}
+        for name, dt_, dty, path in (("fp32_fused", torch.float32, cfdb.F32, cfdb.FUSED),
+                                     ("fp64_plain", torch.float64, cfdb.F64, cfdb.PLAIN))[: 1 if args.no_extras else 2]:
+            e = cfdb.Euler(ctx, m, dtype=dty, path=path, gamma=cfg["gamma"], cfl=cfg["cfl"], t_end=cfg["t_end"],
+                           max_steps=args.tsteps or 20000)
+            U0 = torch.tensor(cfg["U0"], dtype=dt_, device=dev)
+            a, b = torch.empty_like(U0), torch.empty_like(U0)
+            out = {}
+
+            def solve():
+                e.begin(a)
+                out["r"] = e.run(a, b, 256)
+            ms = _timed(solve, K, Wm, flush, prep=lambda: a.copy_(U0))
+            steps, in_b = out["r"]
+            fin = (b if in_b else a).double().cpu().numpy()
+            res[name] = (nx * ny * nz * steps * K / (ms * 1e-3), ms / K, fin, steps, e.totals())
+        if args.no_extras:
+            res["fp64_plain"] = res["fp32_fused"]
+        err = l2(res["fp32_fused"][2], res["fp64_plain"][2])
+        N = nx * ny * nz
+        rho = res["fp32_fused"][2][:N].reshape(nx, ny * nz)[:, 0]
+        xc = (np.arange(nx) + 0.5) * cfg["dx"]
+        ex = riemann.sample(xc, 0.2, 0.5, (1.0, 0.0, 1.0), (0.125, 0.0, 0.1))
+        tot = res["fp32_fused"][4]
+        steps = res["fp32_fused"][3]
+        _line(args, "sod_512x64x64_rusanov_to_t0.2", res["fp32_fused"][0], res["fp32_fused"][1],
+              {"mesh": [nx, ny, nz], "gamma": 1.4, "cfl": 0.4, "t_end": 0.2, "time_steps": steps}, 40, N, steps,
+              {"fp64_plain": {"value": res["fp64_plain"][0], "unit": "cell-updates/s", "time_steps": res["fp64_plain"][3]},
+               "speedup_fused_fp32_vs_plain_fp64": res["fp32_fused"][0] / res["fp64_plain"][0],
+               "accuracy_vs_fp64": {"l2_rel": err[0], "linf_rel": err[1]},
+               "fp64_totals_drift": {"mass": float(np.abs(tot[:, 0] - tot[0, 0]).max() / tot[0, 0]),
+                                     "energy": float(np.abs(tot[:, 1] - tot[0, 1]).max() / tot[0, 1])},
+               "l1_rho_vs_exact_riemann": float(np.mean(np.abs(rho - ex[0])))})
+    elif args.workload == "ensemble":
+        probs = W.ensemble_problems()
+        b = cfdb.Batch(ctx, probs)
+        pool0 = torch.tensor(W.ensemble_initial(probs, b.offsets, b.pool_elems), device=dev)
+        a, c = pool0.clone(), torch.empty_like(pool0)
+        b.tune(a, c, os.path.join(ROOT, "_work", "ensemble_tune.json") if os.path.isdir(os.path.join(ROOT, "_work")) else None)
+        T = args.tsteps or 300
+        cells = sum(p["n"] ** 3 for p in probs)
+        alg = sum(p["n"] ** 3 * (8 if p["kind"] == 0 else 32) for p in probs)
+        ms = _timed(lambda: b.run(a, c, T, use_graph=not args.eager), K, Wm, flush, prep=lambda: a.copy_(pool0))
+        _line(args, "ensemble_512_cubes_n16-96_x300_steps", cells * T * K / (ms * 1e-3), ms / K,
+              {"problems": len(probs), "cells": cells, "time_steps_per_bench_step": T,
+               "heat": sum(1 for p in probs if p["kind"] == 0), "wave": sum(1 for p in probs if p["kind"] == 1),
+               "tuned_config": list(b.get_config())}, alg / cells, cells, T,
+              {"launches_per_step": b.launch_count() // T})
+    elif args.workload == "adjoint":
+        cfg = W.adjoint_config(n=args.n, steps=args.tsteps or 400)
+        n, T, dt = cfg["n"], cfg["steps"], cfg["dt"]
+        m = cfdb.Mesh.structured(ctx, n, n, n, 1 / n, 1 / n, 1 / n)
+        q0 = torch.tensor(cfg["q0"], dtype=torch.float32, device=dev)
+        c = torch.tensor(cfg["c"], dtype=torch.float32, device=dev)
+        a, bb = q0.clone(), torch.empty_like(q0)
+        fin = ctx.wave_run(m, a, bb, dt, T, c=torch.tensor(cfg["c_true"], dtype=torch.float32, device=dev), speed_mode=1)
+        tgt = fin[: m.n].clone()
+        g_c, g_p = torch.empty(m.n, device=dev), torch.empty(m.n, device=dev)
+        out = {}
+        ms_grad = _timed(lambda: out.__setitem__("g", ctx.wave_gradient(m, q0, c, tgt, T, dt, T, g_c, g_p)), K, Wm, flush)
+        ms_fwd = _timed(lambda: ctx.wave_run(m, a, bb, dt, T, c=c, speed_mode=1), K, Wm, flush, prep=lambda: a.copy_(q0))
+        J, st = out["g"]
+        if args.no_extras:
+            print(json.dumps({"workload": "adjoint", "gradient_ms": ms_grad / K, "forward_solve_ms": ms_fwd / K}))
+            return
+        d = W.gaussian_random_field(n, corr=0.1, seed=9)
+        d = torch.tensor(d / np.abs(d).max(), dtype=torch.float64, device=dev)
+        q64, c64, t64 = q0.double(), c.double(), tgt.double()
+        eps = 1e-3
+        fd = (ctx.wave_objective(m, q64, c64 + eps * d, t64, T, dt, path=cfdb.PLAIN)
+              - ctx.wave_objective(m, q64, c64 - eps * d, t64, T, dt, path=cfdb.PLAIN)) / (2 * eps)
+        adj = float(torch.dot(g_c.double(), d))
+        _line(args, f"wave_adjoint_{n}^3_x{T}_steps", 2 * n ** 3 * T * K / (ms_grad * 1e-3), ms_grad / K,
+              {"mesh": [n] * 3, "time_steps": T, "snapshots": T, "c": "exp(0.2 g), g Gaussian random field, seed 5"},
+              60, n ** 3, T,
+              {"adjoint_over_forward_time": (ms_grad / K) / (ms_fwd / K),
+               "reverse_over_forward_sweep": st.reverse_ms / st.forward_ms,
+               "forward_solve_ms": ms_fwd / K, "gradient_ms": ms_grad / K,
+               "grad_rel_err_vs_fd": abs(adj - fd) / abs(fd), "fd_eps": eps, "J": J,
+               "note": "value counts forward + adjoint cell-updates; roofline uses the adjoint sweep's 60 B/cell"})
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
+        if args.workload != "wave":
+            raise SystemExit("--impl reference times the headline wave workload only")
         run_reference(args, rank)
+        return
+    if args.workload != "wave":
+        if rank == 0:
+            run_secondary(args)
         return
     if world > 1:
         import datetime

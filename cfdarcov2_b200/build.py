@@ -63,6 +63,31 @@ def _compile_cmd(src: str, obj: str):
             "-I", os.path.join(CUDA_HOME, "include"), *common_inc, "-c", src, "-o", obj]
 
 
+FACADE_LIB = os.path.join(LIBDIR, "libcfdb_fvm.so")
+EXAMPLE_BIN = os.path.join(LIBDIR, "fvm_example")
+
+
+def build_facade(verbose: bool = False) -> str:
+    """The drop-in C++ facade (include/cfdb/) over the C ABI, and its example."""
+    srcs = sorted(glob.glob(os.path.join(CSRC, "facade", "*.cpp")))
+    hdrs = glob.glob(os.path.join(INCLUDE, "cfdb", "*.hpp")) + [os.path.join(INCLUDE, "cfdb.h")]
+    cxx = host_cxx()
+    if _newer(srcs + hdrs + [LIB], FACADE_LIB):
+        cmd = [cxx, "-O2", "-std=c++17", "-fPIC", "-shared", "-Wall", "-I", INCLUDE, *srcs, "-o", FACADE_LIB,
+               "-L", LIBDIR, "-lcfdb", "-Wl,-rpath,$ORIGIN"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    ex = os.path.join(PKG, "examples", "fvm_example.cpp")
+    if _newer([ex, FACADE_LIB] + hdrs, EXAMPLE_BIN):
+        cmd = [cxx, "-O2", "-std=c++17", "-Wall", "-I", INCLUDE, ex, "-o", EXAMPLE_BIN, "-L", LIBDIR, "-lcfdb_fvm",
+               "-lcfdb", "-Wl,-rpath,$ORIGIN"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return FACADE_LIB
+
+
 def build(verbose: bool = False, jobs: int | None = None) -> str:
     os.makedirs(OBJ, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
@@ -94,6 +119,7 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed\n{r.stdout}\n{r.stderr}")
+    build_facade(verbose)
     return LIB
 
 

@@ -34,57 +34,55 @@ struct AdjPhys {
 #pragma unroll
     for (int f = 0; f < FT; ++f) g[f] = p[f];
   }
+  // Per face with outward normal s e_d, area A and neighbour N (dl = lam_N -
+  // lam_P, dq = q_N - q_P, all 4 fields; h = A (c_P + c_N) / 4):
+  //   ap   += h dl_p + s A/2 dl_d
+  //   au_e += h dl_e,   au_d += s A/2 (c_N^2 lam_N,p - c_P^2 lam_P,p)
+  //   gg   -= s A c_P (2 q_P,d + dq_d) lam_P,p + A/4 sum_f dq_f dl_f
+  // and at a wall: ap -= s A lam_P,d, au_d -= c_P A lam_P,d,
+  // gg -= A q_P,d lam_P,d.  Every term is linear in lam / V with one uniform
+  // V, so 1/V multiplies the sums once at the end.
   __device__ static void cell(const stencil::CellIn<FT>& in, const Params& a, float o[NF]) {
-    const float cP = in.P[8];
-    float lP[4], qP[4];
-#pragma unroll
-    for (int f = 0; f < 4; ++f) {
-      lP[f] = in.P[f] * a.iV;
-      qP[f] = in.P[4 + f];
-    }
-    float ap = 0.f, au[3] = {0.f, 0.f, 0.f}, gg = 0.f;
+    const float g0 = a.gc[in.idx];  // issued first: its latency hides behind the face sums
+    const float* P = in.P;
+    const float cP = P[8];
+    const float c2P = cP * cP;
+    float ap = 0.f, au0 = 0.f, au1 = 0.f, au2 = 0.f, gg = 0.f;
+    float* au[3] = {&au0, &au1, &au2};
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       const float Ad = a.A[d];
+      const float hA = 0.5f * Ad;
 #pragma unroll
       for (int side = 0; side < 2; ++side) {
         const int k = 2 * d + side;
-        const float s = side ? 1.f : -1.f;
+        const float sA = side ? Ad : -Ad;
         if ((in.walls >> k) & 1) {
-          ap -= s * Ad * lP[1 + d];
-          au[d] -= cP * Ad * lP[1 + d];
-          gg -= Ad * qP[1 + d] * lP[1 + d];
+          ap -= sA * P[1 + d];
+          *au[d] -= cP * Ad * P[1 + d];
+          gg -= Ad * P[5 + d] * P[1 + d];
         } else {
           const float* N = in.nb[k];
-          const float cN = N[8];
-          float lN[4], qN[4];
-#pragma unroll
-          for (int f = 0; f < 4; ++f) {
-            lN[f] = N[f] * a.iV;
-            qN[f] = N[4 + f];
-          }
-          const float h = 0.25f * (cP + cN) * Ad;
-          ap += h * (lN[0] - lP[0]) + 0.5f * s * Ad * (lN[1 + d] - lP[1 + d]);
-          const float sp = 0.5f * (cN * cN * lN[0] - cP * cP * lP[0]);
-#pragma unroll
-          for (int e = 0; e < 3; ++e) au[e] += h * (lN[1 + e] - lP[1 + e]);
-          au[d] += sp * s * Ad;
-          gg -= cP * s * Ad * (qP[1 + d] + qN[1 + d]) * lP[0];
-          const float jp = qN[0] - qP[0];
-          float ju_self = 0.f, ju_nb = 0.f;
-#pragma unroll
-          for (int e = 0; e < 3; ++e) {
-            ju_self += (qN[1 + e] - qP[1 + e]) * lP[1 + e];
-            ju_nb += (qP[1 + e] - qN[1 + e]) * lN[1 + e];
-          }
-          gg += 0.25f * Ad * ((jp * lP[0] + ju_self) + (ju_nb - jp * lN[0]));
+          const float h = 0.25f * Ad * (cP + N[8]);
+          const float dl0 = N[0] - P[0], dl1 = N[1] - P[1], dl2 = N[2] - P[2], dl3 = N[3] - P[3];
+          const float dq0 = N[4] - P[4], dq1 = N[5] - P[5], dq2 = N[6] - P[6], dq3 = N[7] - P[7];
+          const float dld = d == 0 ? dl1 : (d == 1 ? dl2 : dl3);
+          const float dqd = d == 0 ? dq1 : (d == 1 ? dq2 : dq3);
+          ap += h * dl0 + 0.5f * sA * dld;
+          au0 += h * dl1;
+          au1 += h * dl2;
+          au2 += h * dl3;
+          *au[d] += (side ? hA : -hA) * (N[8] * N[8] * N[0] - c2P * P[0]);
+          gg -= sA * cP * (2.0f * P[5 + d] + dqd) * P[0] + 0.25f * Ad * ((dq0 * dl0 + dq1 * dl1) + (dq2 * dl2 + dq3 * dl3));
         }
       }
     }
-    o[0] = in.P[0] + a.dt * ap;
-#pragma unroll
-    for (int e = 0; e < 3; ++e) o[1 + e] = in.P[1 + e] + a.dt * au[e];
-    a.gc[in.idx] += a.dt * gg;
+    const float s = a.dt * a.iV;
+    o[0] = P[0] + s * ap;
+    o[1] = P[1] + s * au0;
+    o[2] = P[2] + s * au1;
+    o[3] = P[3] + s * au2;
+    a.gc[in.idx] = g0 + s * gg;
   }
   __device__ static void acc_init(Acc&) {}
   __device__ static void acc_cell(Acc&, const float*, const Params&) {}

@@ -52,8 +52,8 @@ struct PlainGeomDev {
 // faces on the -x/-y/-z walls.
 struct CompactGeomDev {
   bool ready = false;
-  float* S = nullptr;      // 9n: [Sx.x|Sx.y|Sx.z|Sy.x|...|Sz.z]
-  float* inv_vol = nullptr;
+  float* S = nullptr;      // 10n: [Sx.x|Sx.y|Sx.z|Sy.x|...|Sz.z|1/V]
+  float* inv_vol = nullptr;  // = S + 9n
   float* wall_x = nullptr; // 3 * ny*nz  (cells x = 0, index y*nz+z)
   float* wall_y = nullptr; // 3 * nx*nz  (cells y = 0, index x*nz+z)
   float* wall_z = nullptr; // 3 * nx*ny  (cells z = 0, index x*ny+y)

@@ -6,7 +6,7 @@
 // src/mesh3d.cpp:69-105), boundary -faces come from three wall tables.
 // Warps cover consecutive z cells, so every neighbour gather is a coalesced
 // row segment.
-#include "cfdb_internal.hpp"
+#include "tma_host.hpp"
 
 namespace {
 
@@ -90,6 +90,88 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// Sweep form (uniform-lattice topology, any vertex positions): the state
+// (p,u,v,w) is swept, the compact geometry [Sx|Sy|Sz|1/V] (10 fields) is
+// staged as auxiliary data with the same halos, so the -face area vector of a
+// cell is its staged neighbour's +face vector.  -wall faces read the wall
+// tables.  Same flux as compact_wave_k.
+struct DistPhys {
+  static constexpr int NF = 4;
+  static constexpr int NA = 10;
+  static constexpr bool HAS_C = false;
+  static constexpr int FT = 14;
+  static constexpr int MIN_BLOCKS = 2;
+  struct Params {
+    float dt, c;
+    int mode;
+    int X, Y, Z;
+    const float* wx;
+    const float* wy;
+    const float* wz;
+  };
+  struct Acc {};
+  __device__ static bool begin(Params&) { return true; }
+  __device__ static void ghost(float g[FT], const float p[FT], int) {
+#pragma unroll
+    for (int f = 0; f < FT; ++f) g[f] = p[f];
+  }
+  __device__ static void cell(const stencil::CellIn<FT>& in, const Params& a, float o[NF]) {
+    const float* P = in.P;
+    const float pP = P[0], uP = P[1], vP = P[2], wP = P[3];
+    const float cP = a.c, c2 = cP * cP;
+    float ap = 0.f, au = 0.f, av = 0.f, aw = 0.f;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+#pragma unroll
+      for (int side = 0; side < 2; ++side) {
+        const int k = 2 * d + side;
+        const bool wall = (in.walls >> k) & 1;
+        float Sx, Sy, Sz;
+        if (side) {
+          Sx = P[4 + 3 * d]; Sy = P[5 + 3 * d]; Sz = P[6 + 3 * d];
+        } else if (!wall) {
+          const float* N = in.nb[k];
+          Sx = -N[4 + 3 * d]; Sy = -N[5 + 3 * d]; Sz = -N[6 + 3 * d];
+        } else {
+          const long long yz = (long long)a.Y * a.Z;
+          const int x = int(in.idx / yz);
+          const int r = int(in.idx - (long long)x * yz);
+          const int y = r / a.Z, z = r - (r / a.Z) * a.Z;
+          const float* w = d == 0 ? a.wx : (d == 1 ? a.wy : a.wz);
+          const long long cnt = d == 0 ? yz : (d == 1 ? (long long)a.X * a.Z : (long long)a.X * a.Y);
+          const long long kk = d == 0 ? (long long)y * a.Z + z : (d == 1 ? (long long)x * a.Z + z : (long long)x * a.Y + y);
+          Sx = w[kk]; Sy = w[cnt + kk]; Sz = w[2 * cnt + kk];
+        }
+        const float A = sqrtf(Sx * Sx + Sy * Sy + Sz * Sz);
+        const float unPA = uP * Sx + vP * Sy + wP * Sz;
+        float pN, uN, vN, wN;
+        if (!wall) {
+          const float* N = in.nb[k];
+          pN = N[0]; uN = N[1]; vN = N[2]; wN = N[3];
+        } else {
+          const float k2 = 2.f * unPA / (A * A);
+          pN = pP; uN = uP - k2 * Sx; vN = vP - k2 * Sy; wN = wP - k2 * Sz;
+        }
+        const float unNA = uN * Sx + vN * Sy + wN * Sz;
+        const float hA = 0.5f * cP * A;
+        const float pm = 0.5f * (pP + pN);
+        ap += c2 * 0.5f * (unPA + unNA) - hA * (pN - pP);
+        au += pm * Sx - hA * (uN - uP);
+        av += pm * Sy - hA * (vN - vP);
+        aw += pm * Sz - hA * (wN - wP);
+      }
+    }
+    const float s = -a.dt * P[13];
+    o[0] = pP + s * ap;
+    o[1] = uP + s * au;
+    o[2] = vP + s * av;
+    o[3] = wP + s * aw;
+  }
+  __device__ static void acc_init(Acc&) {}
+  __device__ static void acc_cell(Acc&, const float*, const Params&) {}
+  __device__ static void finish(Acc&, const Params&, bool) {}
+};
+
 }  // namespace
 
 int compact_wave_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* q, void* qn, const void* c, double cconst,
@@ -98,6 +180,10 @@ int compact_wave_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* q, voi
     return cfdb_fail(ctx, CFDB_EUNSUPPORTED, "the fused vertex-mesh wave step computes in float32 only");
   if (int rc = cfdb_mesh_need_compact(m)) return rc;
   const CompactGeomDev& cg = m->compact;
+  if (!c && m->nz % 4 == 0 && !(reinterpret_cast<uintptr_t>(q) & 15u) && !(reinterpret_cast<uintptr_t>(qn) & 15u)) {
+    DistPhys::Params p{float(dt), float(cconst), mode, int(m->nx), int(m->ny), int(m->nz), cg.wall_x, cg.wall_y, cg.wall_z};
+    return stencil::launch_sweep<DistPhys, 32, 8, 3, 1>(ctx, m, q, cg.S, nullptr, qn, p, 0);
+  }
   CompactArgs a{cg.S, cg.inv_vol, cg.wall_x, cg.wall_y, cg.wall_z, int(m->nx), int(m->ny), int(m->nz), (long long)m->n};
   compact_wave_k<<<grid_for(ctx, m->n, kThreads, 8), kThreads, 0, ctx->stream>>>(
       a, static_cast<const float*>(q), static_cast<float*>(qn), static_cast<const float*>(c), float(cconst), mode,

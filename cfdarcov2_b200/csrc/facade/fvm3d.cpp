@@ -1,0 +1,436 @@
+// Implementation of the drop-in C++ facade (include/cfdb/*.hpp).  It only
+// uses libcfdb's C ABI: every field lives in library device buffers and every
+// expression node evaluates through a cfdb_op_* kernel into a buffer it
+// allocates once.
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <utility>
+
+#include "cfdb/fvm3d.hpp"
+
+namespace cfdb {
+
+void check(int status, const char* what) {
+  if (status != CFDB_OK) {
+    std::string msg = std::string(what) + ": " + cfdb_last_error(CFDArcoGlobalInit::ctx());
+    throw std::runtime_error(msg);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// global context
+// ---------------------------------------------------------------------------
+namespace {
+cfdb_ctx* g_ctx = nullptr;
+}
+
+bool CFDArcoGlobalInit::skip_history = true;
+bool CFDArcoGlobalInit::cuda_enabled = false;
+
+void CFDArcoGlobalInit::initialize(int, char**, bool skip_hist) { skip_history = skip_hist; }
+
+void CFDArcoGlobalInit::enable_cuda(int device) {
+  if (g_ctx) return;
+  cfdb_ctx* c = nullptr;
+  if (cfdb_ctx_create(device, &c) != CFDB_OK)
+    throw std::runtime_error(std::string("cfdb_ctx_create: ") + cfdb_last_error(nullptr));
+  g_ctx = c;
+  cuda_enabled = true;
+}
+
+void CFDArcoGlobalInit::finalize() {
+  if (g_ctx) cfdb_ctx_destroy(g_ctx);
+  g_ctx = nullptr;
+  cuda_enabled = false;
+}
+
+cfdb_ctx* CFDArcoGlobalInit::ctx() {
+  if (!g_ctx) enable_cuda(0);
+  return g_ctx;
+}
+
+namespace {
+float* device_alloc(size_t n) {
+  void* p = nullptr;
+  check(cfdb_alloc(CFDArcoGlobalInit::ctx(), int64_t(n * sizeof(float)), &p), "cfdb_alloc");
+  return static_cast<float*>(p);
+}
+void device_free(float* p) {
+  if (p && CFDArcoGlobalInit::cuda_enabled) cfdb_free(CFDArcoGlobalInit::ctx(), p);
+}
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Mesh3D
+// ---------------------------------------------------------------------------
+Mesh3D::Mesh3D(size_t x, size_t y, size_t z, float dx, float dy, float dz)
+    : _num_nodes(x * y * z), _x(x), _y(y), _z(z), _lx(dx * float(x)), _ly(dy * float(y)), _lz(dz * float(z)),
+      _dx(dx), _dy(dy), _dz(dz) {}
+
+Mesh3D::~Mesh3D() {
+  if (mesh_ && CFDArcoGlobalInit::cuda_enabled) cfdb_mesh_destroy(mesh_);
+}
+
+void Mesh3D::init_basic_internals() {}
+
+void Mesh3D::compute() { handle(); }
+
+cfdb_mesh* Mesh3D::handle() {
+  if (!mesh_)
+    check(cfdb_mesh_create_structured(CFDArcoGlobalInit::ctx(), int64_t(_x), int64_t(_y), int64_t(_z), _dx, _dy,
+                                      _dz, &mesh_),
+          "cfdb_mesh_create_structured");
+  return mesh_;
+}
+
+float Mesh3D::x(size_t id) const { return (float(id / (_y * _z)) + 0.5f) * _dx; }
+float Mesh3D::y(size_t id) const { return (float((id / _z) % _y) + 0.5f) * _dy; }
+float Mesh3D::z(size_t id) const { return (float(id % _z) + 0.5f) * _dz; }
+bool Mesh3D::is_boundary(size_t id) const {
+  const size_t xi = id / (_y * _z), yi = (id / _z) % _y, zi = id % _z;
+  return xi == 0 || yi == 0 || zi == 0 || xi + 1 == _x || yi + 1 == _y || zi + 1 == _z;
+}
+
+// ---------------------------------------------------------------------------
+// expression nodes
+// ---------------------------------------------------------------------------
+struct Node {
+  enum Kind { kField, kConst, kBinary, kNeg, kGrad, kLapl, kStab, kDt } kind = kConst;
+  int op = 0;
+  int mask = 7;
+  float value = 0.f;
+  std::shared_ptr<Node> a, b;
+  Variable* field = nullptr;
+  const DT* dt = nullptr;
+  Mesh3D* mesh = nullptr;
+  float* buf = nullptr;
+  bool filled = false;
+  ~Node() { device_free(buf); }
+};
+
+namespace {
+
+std::shared_ptr<Node> make(Node::Kind k, Mesh3D* mesh) {
+  auto n = std::make_shared<Node>();
+  n->kind = k;
+  n->mesh = mesh;
+  return n;
+}
+
+Mesh3D* mesh_of(const Variable& a, const Variable& b) { return a.mesh ? a.mesh : b.mesh; }
+
+Variable wrap(std::shared_ptr<Node> n) {
+  Variable v;
+  v.mesh = n->mesh;
+  v.node = std::move(n);
+  return v;
+}
+
+Variable binary(const Variable& l, const Variable& r, int op) {
+  auto n = make(Node::kBinary, mesh_of(l, r));
+  n->op = op;
+  n->a = l.node;
+  n->b = r.node;
+  return wrap(n);
+}
+
+Variable mesh_op(const Variable& v, Node::Kind k, int mask) {
+  auto n = make(k, v.mesh);
+  n->mask = mask;
+  n->a = v.node;
+  return wrap(n);
+}
+
+const float* eval_node(Node* n) {
+  cfdb_ctx* ctx = CFDArcoGlobalInit::ctx();
+  const int64_t N = int64_t(n->mesh->_num_nodes);
+  if (n->kind == Node::kField) return n->field->current_cu;
+  if (!n->buf) n->buf = device_alloc(size_t(N));
+  switch (n->kind) {
+    case Node::kConst:
+      if (!n->filled) {
+        check(cfdb_op_fill(ctx, CFDB_F32, n->buf, n->value, N), "cfdb_op_fill");
+        n->filled = true;
+      }
+      break;
+    case Node::kDt:
+      check(cfdb_op_fill(ctx, CFDB_F32, n->buf, n->dt->_dt, N), "cfdb_op_fill");
+      break;
+    case Node::kBinary: {
+      // a constant operand becomes a scalar operation (no second stream)
+      if (n->b->kind == Node::kConst || n->b->kind == Node::kDt) {
+        const float s = n->b->kind == Node::kConst ? n->b->value : n->b->dt->_dt;
+        check(cfdb_op_scalar(ctx, CFDB_F32, n->op, eval_node(n->a.get()), s, n->buf, N), "cfdb_op_scalar");
+      } else if (n->a->kind == Node::kConst || n->a->kind == Node::kDt) {
+        const float s = n->a->kind == Node::kConst ? n->a->value : n->a->dt->_dt;
+        const int op = n->op == CFDB_OP_SUB ? CFDB_OP_RSUB : (n->op == CFDB_OP_DIV ? CFDB_OP_RDIV : n->op);
+        check(cfdb_op_scalar(ctx, CFDB_F32, op, eval_node(n->b.get()), s, n->buf, N), "cfdb_op_scalar");
+      } else {
+        const float* a = eval_node(n->a.get());
+        const float* b = eval_node(n->b.get());
+        check(cfdb_op_binary(ctx, CFDB_F32, n->op, a, b, n->buf, N), "cfdb_op_binary");
+      }
+      break;
+    }
+    case Node::kNeg:
+      check(cfdb_op_neg(ctx, CFDB_F32, eval_node(n->a.get()), n->buf, N), "cfdb_op_neg");
+      break;
+    case Node::kGrad:
+      check(cfdb_op_grad(ctx, n->mesh->handle(), CFDB_F32, eval_node(n->a.get()), n->buf, n->mask), "cfdb_op_grad");
+      break;
+    case Node::kLapl:
+      check(cfdb_op_lapl(ctx, n->mesh->handle(), CFDB_F32, eval_node(n->a.get()), n->buf, n->mask), "cfdb_op_lapl");
+      break;
+    case Node::kStab:
+      check(cfdb_op_stab(ctx, n->mesh->handle(), CFDB_F32, eval_node(n->a.get()), n->buf, n->mask), "cfdb_op_stab");
+      break;
+    default:
+      break;
+  }
+  return n->buf;
+}
+
+// k * lapl(T) or lapl(T) * k or lapl(T) with T the updated field: the heat
+// template that runs as one fused step.
+bool match_heat(const Node* rhs, const Variable* T, float* k) {
+  auto is_lapl_T = [&](const Node* n) {
+    return n->kind == Node::kLapl && n->mask == 7 && n->a->kind == Node::kField && n->a->field == T;
+  };
+  if (is_lapl_T(rhs)) {
+    *k = 1.f;
+    return true;
+  }
+  if (rhs->kind == Node::kBinary && rhs->op == CFDB_OP_MUL) {
+    if (rhs->a->kind == Node::kConst && is_lapl_T(rhs->b.get())) {
+      *k = rhs->a->value;
+      return true;
+    }
+    if (rhs->b->kind == Node::kConst && is_lapl_T(rhs->a.get())) {
+      *k = rhs->b->value;
+      return true;
+    }
+  }
+  return false;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Variable
+// ---------------------------------------------------------------------------
+Variable::Variable() = default;
+
+Variable::Variable(Mesh3D* m, HostVec& initial, BoundaryFN bc, std::string nm)
+    : name(std::move(nm)), mesh(m), current(initial), boundary_conditions(std::move(bc)), is_field(true) {
+  if (initial.size() != m->_num_nodes) throw std::runtime_error("Variable: initial values do not match the mesh");
+  node = make(Node::kField, m);
+  node->field = this;
+  current_cu = device_alloc(m->_num_nodes);
+  next_cu = device_alloc(m->_num_nodes);
+  check(cfdb_upload(CFDArcoGlobalInit::ctx(), current_cu, initial.data(), int64_t(initial.size() * sizeof(float))),
+        "cfdb_upload");
+}
+
+Variable::Variable(Mesh3D* m, HostVec& initial, BoundaryFN bc, BoundaryFNCU bc_cu, std::string nm)
+    : Variable(m, initial, std::move(bc), std::move(nm)) {
+  boundary_conditions_cu = std::move(bc_cu);
+  has_boundary_conditions_cu = bool(boundary_conditions_cu);
+}
+
+Variable::Variable(Mesh3D* m, float value) : mesh(m) {
+  node = make(Node::kConst, m);
+  node->value = value;
+  name = "const";
+}
+
+Variable::~Variable() {
+  if (is_field && node && node->field == this) {
+    device_free(current_cu);
+    device_free(next_cu);
+    device_free(prev_cu);
+    node->field = nullptr;
+  }
+}
+
+const HostVec& Variable::host() {
+  if (is_field) {
+    current.resize(mesh->_num_nodes);
+    check(cfdb_download(CFDArcoGlobalInit::ctx(), current.data(), current_cu, int64_t(current.size() * sizeof(float))),
+          "cfdb_download");
+  }
+  return current;
+}
+
+void Variable::set_current(const HostVec& values) {
+  current = values;
+  check(cfdb_upload(CFDArcoGlobalInit::ctx(), current_cu, values.data(), int64_t(values.size() * sizeof(float))),
+        "cfdb_upload");
+}
+
+Variable Variable::operator+(const Variable& r) const { return binary(*this, r, CFDB_OP_ADD); }
+Variable Variable::operator-(const Variable& r) const { return binary(*this, r, CFDB_OP_SUB); }
+Variable Variable::operator*(const Variable& r) const { return binary(*this, r, CFDB_OP_MUL); }
+Variable Variable::operator/(const Variable& r) const { return binary(*this, r, CFDB_OP_DIV); }
+Variable Variable::operator-() const {
+  auto n = make(Node::kNeg, mesh);
+  n->a = node;
+  return wrap(n);
+}
+
+Variable operator+(float l, const Variable& r) { return Variable(r.mesh, l) + r; }
+Variable operator-(float l, const Variable& r) { return Variable(r.mesh, l) - r; }
+Variable operator*(float l, const Variable& r) { return Variable(r.mesh, l) * r; }
+Variable operator/(float l, const Variable& r) { return Variable(r.mesh, l) / r; }
+Variable operator+(const Variable& l, float r) { return l + Variable(l.mesh, r); }
+Variable operator-(const Variable& l, float r) { return l - Variable(l.mesh, r); }
+Variable operator*(const Variable& l, float r) { return l * Variable(l.mesh, r); }
+Variable operator/(const Variable& l, float r) { return l / Variable(l.mesh, r); }
+
+namespace {
+std::vector<std::unique_ptr<Variable>>& lhs_registry() {
+  static std::vector<std::unique_ptr<Variable>> r;
+  return r;
+}
+}  // namespace
+
+DtVar* d1t(Variable& v) {
+  auto* d = new DtVar(&v);
+  d->name = "d1t(" + v.name + ")";
+  lhs_registry().emplace_back(d);
+  return d;
+}
+
+D2tVar* d2t(Variable& v) {
+  auto* d = new D2tVar(&v);
+  d->name = "d2t(" + v.name + ")";
+  lhs_registry().emplace_back(d);
+  return d;
+}
+
+Variable d1dx(const Variable& v) { return mesh_op(v, Node::kGrad, 1); }
+Variable d1dy(const Variable& v) { return mesh_op(v, Node::kGrad, 2); }
+Variable d1dz(const Variable& v) { return mesh_op(v, Node::kGrad, 4); }
+Variable d2dx(const Variable& v) { return mesh_op(v, Node::kLapl, 1); }
+Variable d2dy(const Variable& v) { return mesh_op(v, Node::kLapl, 2); }
+Variable d2dz(const Variable& v) { return mesh_op(v, Node::kLapl, 4); }
+Variable lapl(const Variable& v) { return mesh_op(v, Node::kLapl, 7); }
+Variable stab_tot(const Variable& v) { return mesh_op(v, Node::kStab, 7); }
+Variable stabx(const Variable& v) { return mesh_op(v, Node::kStab, 1); }
+Variable staby(const Variable& v) { return mesh_op(v, Node::kStab, 2); }
+Variable stabz(const Variable& v) { return mesh_op(v, Node::kStab, 4); }
+
+HostVec boundary_none(Mesh3D*, HostVec& arr, const DT*) { return arr; }
+
+BoundaryFNCU boundary_copy_cu(Mesh3D* mesh, const HostVec& values) {
+  auto buf = std::shared_ptr<float>(device_alloc(values.size()), [](float* p) { device_free(p); });
+  check(cfdb_upload(CFDArcoGlobalInit::ctx(), buf.get(), values.data(), int64_t(values.size() * sizeof(float))),
+        "cfdb_upload");
+  return [buf](Mesh3D* m, float* field, const DT*) {
+    check(cfdb_op_boundary_copy(CFDArcoGlobalInit::ctx(), m->handle(), CFDB_F32, field, buf.get(), field),
+          "cfdb_op_boundary_copy");
+  };
+}
+
+// ---------------------------------------------------------------------------
+// DT and the update policies
+// ---------------------------------------------------------------------------
+DT::DT(Mesh3D* m, UpdateFn fn, float cfl, std::vector<Variable*> vars)
+    : update_fn(std::move(fn)), CFL(cfl), space_vars(std::move(vars)) {
+  mesh = m;
+  name = "dt";
+  node = make(Node::kDt, m);
+  node->dt = this;
+}
+
+void DT::update() {
+  _dt = update_fn(CFL, space_vars, mesh);
+  ++_current_time_step_int;
+  _current_time_dbl += _dt;
+}
+
+float UpdatePolicies::CourantFriedrichsLewy3D(float CFL, std::vector<Variable*>& v, Mesh3D* mesh) {
+  double dt = 0;
+  check(cfdb_cfl_dt(CFDArcoGlobalInit::ctx(), mesh->handle(), CFDB_F32, CFL, 5.0 / 3.0, v.at(3)->current_cu,
+                    v.at(4)->current_cu, v.at(0)->current_cu, v.at(1)->current_cu, v.at(2)->current_cu, &dt),
+        "cfdb_cfl_dt");
+  return float(dt);
+}
+
+float UpdatePolicies::CourantFriedrichsLewy1D(float CFL, std::vector<Variable*>& v, Mesh3D* mesh) {
+  double dt = 0;
+  check(cfdb_cfl_dt(CFDArcoGlobalInit::ctx(), mesh->handle(), CFDB_F32, CFL, 5.0 / 3.0, v.at(1)->current_cu,
+                    v.at(2)->current_cu, v.at(0)->current_cu, nullptr, nullptr, &dt),
+        "cfdb_cfl_dt");
+  return float(dt);
+}
+
+// ---------------------------------------------------------------------------
+// Equation
+// ---------------------------------------------------------------------------
+Equation::Equation(size_t t) : timesteps(t) {}
+
+void Equation::evaluate(std::vector<Variable*>& all_vars, EquationTemplate& eqs, DT* dt, bool visualize,
+                        std::vector<Variable*> store_vars) const {
+  cfdb_ctx* ctx = CFDArcoGlobalInit::ctx();
+  fused_equations = 0;
+  for (size_t t = 0; t < timesteps; ++t) {
+    dt->update();
+    const float dtv = dt->_dt;
+    for (auto& eq : eqs) {
+      Variable* lhs = std::get<0>(eq);
+      Variable& rhs = std::get<2>(eq);
+      if (auto* d = dynamic_cast<DtVar*>(lhs)) {
+        Variable* T = d->var;
+        const int64_t N = int64_t(T->mesh->_num_nodes);
+        float k = 0.f;
+        if (match_heat(rhs.node.get(), T, &k) &&
+            cfdb_heat_step(ctx, T->mesh->handle(), CFDB_F32, CFDB_PATH_FUSED, T->current_cu, T->next_cu, k, dtv) ==
+                CFDB_OK) {
+          if (t == 0) ++fused_equations;
+        } else {
+          const float* R = eval_node(rhs.node.get());
+          check(cfdb_op_d1t(ctx, CFDB_F32, R, T->current_cu, dtv, T->next_cu, N), "cfdb_op_d1t");
+        }
+        std::swap(T->current_cu, T->next_cu);
+      } else if (auto* d2 = dynamic_cast<D2tVar*>(lhs)) {
+        Variable* U = d2->var;
+        const int64_t N = int64_t(U->mesh->_num_nodes);
+        if (!U->prev_cu) U->prev_cu = device_alloc(U->mesh->_num_nodes);
+        const float* R = eval_node(rhs.node.get());
+        check(cfdb_op_d2t(ctx, CFDB_F32, R, U->current_cu, U->prev_cu, dtv, U->has_prev ? 1 : 0, U->next_cu, N),
+              "cfdb_op_d2t");
+        std::swap(U->prev_cu, U->current_cu);  // prev <- current
+        std::swap(U->current_cu, U->next_cu);  // current <- next
+        U->has_prev = true;
+      } else if (lhs->is_field) {
+        const float* R = eval_node(rhs.node.get());
+        check(cfdb_op_scalar(ctx, CFDB_F32, CFDB_OP_MUL, R, 1.0, lhs->next_cu, int64_t(lhs->mesh->_num_nodes)),
+              "cfdb_op_scalar");
+        std::swap(lhs->current_cu, lhs->next_cu);
+      } else {
+        throw std::runtime_error("Equation: left-hand side must be a field, d1t(field) or d2t(field)");
+      }
+    }
+    for (Variable* v : all_vars) {
+      if (v->has_boundary_conditions_cu) {
+        v->boundary_conditions_cu(v->mesh, v->current_cu, dt);
+      } else if (v->boundary_conditions) {
+        using Plain = HostVec (*)(Mesh3D*, HostVec&, const DT*);
+        auto* f = v->boundary_conditions.target<Plain>();
+        if (!(f && *f == &boundary_none)) {
+          HostVec cur = v->host();
+          v->set_current(v->boundary_conditions(v->mesh, cur, dt));
+        }
+      }
+      bool store = !CFDArcoGlobalInit::skip_history;
+      for (Variable* s : store_vars) store = store || (s == v && !CFDArcoGlobalInit::skip_history);
+      if (store) v->history.push_back(v->host());
+    }
+    if (visualize) std::printf("\rstep %zu / %zu", t + 1, timesteps);
+  }
+  check(cfdb_sync(ctx), "cfdb_sync");
+  if (visualize) std::printf("\n");
+}
+
+}  // namespace cfdb

@@ -277,7 +277,7 @@ extern "C" int cfdb_mesh_destroy(cfdb_mesh* m) {
     free_plain(m->ctx, m->plain[1]);
     cfdb_dev_free(m->ctx, m->d_ids);
     CompactGeomDev& c = m->compact;
-    float** ptrs[] = {&c.S, &c.inv_vol, &c.wall_x, &c.wall_y, &c.wall_z};
+    float** ptrs[] = {&c.S, &c.wall_x, &c.wall_y, &c.wall_z};  // inv_vol lives inside S's allocation
     for (float** q : ptrs) cfdb_dev_free(m->ctx, *q);
   }
   delete m;
@@ -423,8 +423,10 @@ int cfdb_mesh_need_compact(cfdb_mesh* m) {
       for (int c3 = 0; c3 < 3; ++c3) wz[c3 * nx * ny + (x * ny + y)] = g.normal_alt[c3 * 6 * n + k6] * g.area[k6];
     }
   cfdb_ctx* ctx = m->ctx;
+  // one allocation [S (9n) | 1/V (n)]: the fused sweep stages it as 10 fields
+  S.insert(S.end(), iv.begin(), iv.end());
   int rc = upload_as<float>(ctx, S.data(), int64_t(S.size()), reinterpret_cast<void**>(&c.S));
-  if (!rc) rc = upload_as<float>(ctx, iv.data(), int64_t(iv.size()), reinterpret_cast<void**>(&c.inv_vol));
+  if (!rc) c.inv_vol = c.S + 9 * n;
   if (!rc) rc = upload_as<float>(ctx, wx.data(), int64_t(wx.size()), reinterpret_cast<void**>(&c.wall_x));
   if (!rc) rc = upload_as<float>(ctx, wy.data(), int64_t(wy.size()), reinterpret_cast<void**>(&c.wall_y));
   if (!rc) rc = upload_as<float>(ctx, wz.data(), int64_t(wz.size()), reinterpret_cast<void**>(&c.wall_z));
