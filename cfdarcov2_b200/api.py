@@ -58,6 +58,11 @@ class Context:
         call("cfdb_ctx_allocated_bytes", self.h, C.byref(v), ctx=self.h)
         return v.value
 
+    def trim(self) -> None:
+        """Returns the workspace cached by earlier calls (checkpoint slots and
+        the like) to the device."""
+        call("cfdb_ctx_trim", self.h, ctx=self.h)
+
     def adopt(self, child) -> None:
         self._children.add(child)
 

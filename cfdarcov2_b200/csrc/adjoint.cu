@@ -23,65 +23,71 @@ struct AdjPhys {
   static constexpr int FT = 9;
   static constexpr int MIN_BLOCKS = 2;
   struct Params {
-    float A[3];  // face areas normal to x, y, z
-    float iV;    // 1 / cell volume
+    float A[3];   // face areas normal to x, y, z
+    float A2[3];  // A / 2
+    float A4[3];  // A / 4
+    float iV;     // 1 / cell volume
     float dt;
     float* gc;
   };
   struct Acc {};
   __device__ static bool begin(Params&) { return true; }
-  __device__ static void ghost(float g[FT], const float p[FT], int) {
+  // Reflective wall, as in the forward step: the ghost mirrors the
+  // wall-normal component of lam and of q and copies c.  With it the
+  // interior face terms below reproduce the wall terms of the transposed
+  // forward step exactly (ap -= s A lam_d, au_d -= c_P A lam_d,
+  // gg -= A q_d lam_d), so no face needs a branch.
+  __device__ static void ghost(float g[FT], const float p[FT], int dir) {
 #pragma unroll
     for (int f = 0; f < FT; ++f) g[f] = p[f];
+    g[1 + dir] = -p[1 + dir];
+    g[5 + dir] = -p[5 + dir];
   }
   // Per face with outward normal s e_d, area A and neighbour N (dl = lam_N -
   // lam_P, dq = q_N - q_P, all 4 fields; h = A (c_P + c_N) / 4):
   //   ap   += h dl_p + s A/2 dl_d
   //   au_e += h dl_e,   au_d += s A/2 (c_N^2 lam_N,p - c_P^2 lam_P,p)
   //   gg   -= s A c_P (2 q_P,d + dq_d) lam_P,p + A/4 sum_f dq_f dl_f
-  // and at a wall: ap -= s A lam_P,d, au_d -= c_P A lam_P,d,
-  // gg -= A q_P,d lam_P,d.  Every term is linear in lam / V with one uniform
-  // V, so 1/V multiplies the sums once at the end.
+  // The s-odd terms of the two faces of one direction (neighbours M at -d,
+  // N at +d) collapse into central differences:
+  //   ap   += A/2 (lam_N,d - lam_M,d)
+  //   au_d += A/2 (c_N^2 lam_N,p - c_M^2 lam_M,p)
+  //   gg   -= c_P lam_P,p A (q_N,d - q_M,d)
+  // leaving the h and dq.dl terms per face.  Every term is linear in lam / V
+  // with one uniform V, so 1/V multiplies the sums once at the end.
   __device__ static void cell(const stencil::CellIn<FT>& in, const Params& a, float o[NF]) {
     const float g0 = a.gc[in.idx];  // issued first: its latency hides behind the face sums
     const float* P = in.P;
     const float cP = P[8];
-    const float c2P = cP * cP;
-    float ap = 0.f, au0 = 0.f, au1 = 0.f, au2 = 0.f, gg = 0.f;
-    float* au[3] = {&au0, &au1, &au2};
+    float ap = 0.f, au[3] = {0.f, 0.f, 0.f}, gq = 0.f, gw = 0.f;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      const float Ad = a.A[d];
-      const float hA = 0.5f * Ad;
+      const float* M = in.nb[2 * d];
+      const float* N = in.nb[2 * d + 1];
+      float w = 0.f;
 #pragma unroll
       for (int side = 0; side < 2; ++side) {
-        const int k = 2 * d + side;
-        const float sA = side ? Ad : -Ad;
-        if ((in.walls >> k) & 1) {
-          ap -= sA * P[1 + d];
-          *au[d] -= cP * Ad * P[1 + d];
-          gg -= Ad * P[5 + d] * P[1 + d];
-        } else {
-          const float* N = in.nb[k];
-          const float h = 0.25f * Ad * (cP + N[8]);
-          const float dl0 = N[0] - P[0], dl1 = N[1] - P[1], dl2 = N[2] - P[2], dl3 = N[3] - P[3];
-          const float dq0 = N[4] - P[4], dq1 = N[5] - P[5], dq2 = N[6] - P[6], dq3 = N[7] - P[7];
-          const float dld = d == 0 ? dl1 : (d == 1 ? dl2 : dl3);
-          const float dqd = d == 0 ? dq1 : (d == 1 ? dq2 : dq3);
-          ap += h * dl0 + 0.5f * sA * dld;
-          au0 += h * dl1;
-          au1 += h * dl2;
-          au2 += h * dl3;
-          *au[d] += (side ? hA : -hA) * (N[8] * N[8] * N[0] - c2P * P[0]);
-          gg -= sA * cP * (2.0f * P[5 + d] + dqd) * P[0] + 0.25f * Ad * ((dq0 * dl0 + dq1 * dl1) + (dq2 * dl2 + dq3 * dl3));
-        }
+        const float* X = side ? N : M;
+        const float h = a.A4[d] * (cP + X[8]);
+        const float dl0 = X[0] - P[0], dl1 = X[1] - P[1], dl2 = X[2] - P[2], dl3 = X[3] - P[3];
+        const float dq0 = X[4] - P[4], dq1 = X[5] - P[5], dq2 = X[6] - P[6], dq3 = X[7] - P[7];
+        ap += h * dl0;
+        au[0] += h * dl1;
+        au[1] += h * dl2;
+        au[2] += h * dl3;
+        w += (dq0 * dl0 + dq1 * dl1) + (dq2 * dl2 + dq3 * dl3);
       }
+      ap += a.A2[d] * (N[1 + d] - M[1 + d]);
+      au[d] += a.A2[d] * (N[8] * N[8] * N[0] - M[8] * M[8] * M[0]);
+      gq += a.A[d] * (N[5 + d] - M[5 + d]);
+      gw += a.A4[d] * w;
     }
+    const float gg = -(cP * P[0]) * gq - gw;
     const float s = a.dt * a.iV;
     o[0] = P[0] + s * ap;
-    o[1] = P[1] + s * au0;
-    o[2] = P[2] + s * au1;
-    o[3] = P[3] + s * au2;
+    o[1] = P[1] + s * au[0];
+    o[2] = P[2] + s * au[1];
+    o[3] = P[3] + s * au[2];
     a.gc[in.idx] = g0 + s * gg;
   }
   __device__ static void acc_init(Acc&) {}
@@ -171,6 +177,10 @@ int fused_wave_adjoint(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* q, co
   if (stencil::check_sweep(ctx, m, {q, lam1, lam0, c}) == CFDB_OK) {
     AdjPhys::Params p;
     p.A[0] = float(m->dy * m->dz); p.A[1] = float(m->dx * m->dz); p.A[2] = float(m->dx * m->dy);
+    for (int d = 0; d < 3; ++d) {
+      p.A2[d] = 0.5f * p.A[d];
+      p.A4[d] = 0.25f * p.A[d];
+    }
     p.iV = float(1.0 / (m->dx * m->dy * m->dz));
     p.dt = float(dt);
     p.gc = static_cast<float*>(gc);

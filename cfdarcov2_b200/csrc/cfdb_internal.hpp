@@ -67,6 +67,11 @@ struct cfdb_ctx {
   int64_t budget = 0;
   int64_t allocated = 0;
   std::unordered_map<void*, int64_t> allocs;
+  // Stream-ordered pool for per-call workspaces (checkpoint slots, adjoint
+  // buffers, reduction scratch): freed blocks stay in the pool, so a repeated
+  // call of the same size neither allocates nor frees device memory.
+  cudaMemPool_t pool = nullptr;
+  std::unordered_map<void*, int64_t> ws;
   int* d_error = nullptr;  // device error word written by bounded waits
   cudaStream_t capture_stream = nullptr;  // private stream used to record CUDA graphs
   // Objects created on this context (meshes, Euler solvers, batches) with a
@@ -118,6 +123,11 @@ int cfdb_cuda_fail(cfdb_ctx* ctx, cudaError_t e, const char* what);
 // ---- memory ---------------------------------------------------------------
 int cfdb_dev_alloc(cfdb_ctx* ctx, int64_t bytes, void** out);
 void cfdb_dev_free(cfdb_ctx* ctx, void* p);
+// Workspace from the context's pool, ordered on ctx->stream (usable by work
+// enqueued after the call; freed after the work enqueued before the free).
+// Counts toward the allocation budget while live.
+int cfdb_ws_alloc(cfdb_ctx* ctx, int64_t bytes, void** out);
+void cfdb_ws_free(cfdb_ctx* ctx, void* p);
 
 // ---- geometry helpers ------------------------------------------------------
 int cfdb_mesh_need_host_geom(cfdb_mesh* m);

@@ -103,14 +103,16 @@ int check_args(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, int path, const void* q0,
   return CFDB_OK;
 }
 
+// Workspaces of one call, taken from the context's pool and returned to it
+// (stream-ordered) when the call ends.
 struct Bufs {
   cfdb_ctx* ctx;
   std::vector<void*> v;
   ~Bufs() {
-    for (void* p : v) cfdb_dev_free(ctx, p);
+    for (void* p : v) cfdb_ws_free(ctx, p);
   }
   int get(int64_t bytes, void** out) {
-    int rc = cfdb_dev_alloc(ctx, bytes, out);
+    int rc = cfdb_ws_alloc(ctx, bytes, out);
     if (!rc) v.push_back(*out);
     return rc;
   }

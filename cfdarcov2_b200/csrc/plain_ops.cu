@@ -530,7 +530,7 @@ extern "C" int cfdb_cfl_dt(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, double cfl, d
   if ((v == nullptr) != (w == nullptr)) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_cfl_dt: give both v and w or neither");
   CFDB_CUDA(ctx, cudaSetDevice(ctx->device));
   void* res = nullptr;
-  if (int rc = cfdb_dev_alloc(ctx, 8, &res)) return rc;
+  if (int rc = cfdb_ws_alloc(ctx, 8, &res)) return rc;
   int rc = CFDB_OK;
   double host = 0;
   DISPATCH(dtype, R, {
@@ -545,7 +545,7 @@ extern "C" int cfdb_cfl_dt(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, double cfl, d
     if (e != cudaSuccess) rc = cfdb_cuda_fail(ctx, e, "cfdb_cfl_dt");
     host = double(R(cfl) * mn);
   });
-  cfdb_dev_free(ctx, res);
+  cfdb_ws_free(ctx, res);
   if (rc) return rc;
   if (!std::isfinite(host) || !(host > 0)) return cfdb_fail(ctx, CFDB_ENUMERIC, "cfdb_cfl_dt: non-finite or non-positive dt %g", host);
   *dt_out = host;
@@ -565,14 +565,14 @@ extern "C" int cfdb_total_fp64(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const voi
   const double vconst = m->dx * m->dy * m->dz;
   const int grid = grid_for(ctx, m->n, kThreads, 2);
   void* scratch = nullptr;
-  if (int rc = cfdb_dev_alloc(ctx, int64_t(sizeof(Comp)) * grid + 16, &scratch)) return rc;
+  if (int rc = cfdb_ws_alloc(ctx, int64_t(sizeof(Comp)) * grid + 16, &scratch)) return rc;
   Comp* part = static_cast<Comp*>(scratch);
   double* res = reinterpret_cast<double*>(part + grid);
   DISPATCH(dtype, R, total_k<R><<<grid, kThreads, 0, ctx->stream>>>((const R*)field, (const R*)vol, vconst, m->n, part));
   total_final_k<<<1, 32, 0, ctx->stream>>>(part, grid, res);
   cudaError_t e = cudaMemcpyAsync(out, res, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-  cfdb_dev_free(ctx, scratch);
+  cfdb_ws_free(ctx, scratch);
   if (e != cudaSuccess) return cfdb_cuda_fail(ctx, e, "cfdb_total_fp64");
   return CFDB_OK;
 }

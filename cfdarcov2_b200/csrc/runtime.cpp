@@ -62,6 +62,55 @@ void cfdb_dev_free(cfdb_ctx* ctx, void* p) {
   cudaFree(p);
 }
 
+int cfdb_ws_alloc(cfdb_ctx* ctx, int64_t bytes, void** out) {
+  *out = nullptr;
+  if (bytes <= 0) bytes = 16;
+  if (ctx->budget > 0 && ctx->allocated + bytes > ctx->budget)
+    return cfdb_fail(ctx, CFDB_ENOMEM, "workspace of %lld bytes exceeds the context budget (%lld of %lld used)",
+                     (long long)bytes, (long long)ctx->allocated, (long long)ctx->budget);
+  if (!ctx->pool) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = ctx->device;
+    CFDB_CUDA(ctx, cudaMemPoolCreate(&ctx->pool, &props));
+    uint64_t keep = UINT64_MAX;  // never hand freed blocks back on synchronisation
+    CFDB_CUDA(ctx, cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  }
+  void* p = nullptr;
+  cudaError_t e = cudaMallocFromPoolAsync(&p, size_t(bytes), ctx->pool, ctx->stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    // blocks cached for other sizes may be what is missing: return them and retry once
+    cudaStreamSynchronize(ctx->stream);
+    cudaMemPoolTrimTo(ctx->pool, 0);
+    e = cudaMallocFromPoolAsync(&p, size_t(bytes), ctx->pool, ctx->stream);
+    if (e != cudaSuccess) return cfdb_cuda_fail(ctx, e, "cudaMallocFromPoolAsync");
+  }
+  ctx->ws[p] = bytes;
+  ctx->allocated += bytes;
+  *out = p;
+  return CFDB_OK;
+}
+
+void cfdb_ws_free(cfdb_ctx* ctx, void* p) {
+  if (!p || !ctx) return;
+  auto it = ctx->ws.find(p);
+  if (it == ctx->ws.end()) return;
+  ctx->allocated -= it->second;
+  ctx->ws.erase(it);
+  cudaFreeAsync(p, ctx->stream);
+}
+
+extern "C" int cfdb_ctx_trim(cfdb_ctx* ctx) {
+  if (!ctx) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_ctx_trim: ctx is NULL");
+  if (!ctx->pool) return CFDB_OK;
+  CFDB_CUDA(ctx, cudaSetDevice(ctx->device));
+  CFDB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  CFDB_CUDA(ctx, cudaMemPoolTrimTo(ctx->pool, 0));
+  return CFDB_OK;
+}
+
 extern "C" int cfdb_abi_version(void) { return CFDB_ABI_VERSION; }
 
 extern "C" int cfdb_ctx_create(int device, cfdb_ctx** out) {
@@ -103,6 +152,11 @@ extern "C" int cfdb_ctx_destroy(cfdb_ctx* ctx) {
   for (auto& kv : children) kv.second();
   for (auto& kv : ctx->allocs) cudaFree(kv.first);
   ctx->allocs.clear();
+  if (ctx->pool) {
+    for (auto& kv : ctx->ws) cudaFreeAsync(kv.first, ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+    cudaMemPoolDestroy(ctx->pool);
+  }
   delete ctx;
   return CFDB_OK;
 }

@@ -117,9 +117,20 @@ int launch_sweep(cfdb_ctx* ctx, const cfdb_mesh* m, const void* q, const void* a
   }
   const SweepShape sh = sweep_shape(ctx, m, TZ, TY, ctas_per_sm > 0 ? std::min(ctas_per_sm, resident) : resident);
   Geometry g{int(m->nx), int(m->ny), int(m->nz), sh.chunks, (long long)m->n};
-  dim3 grid(sh.tiles, sh.chunks);
-  kern<<<grid, L::THREADS, L::SMEM_BYTES, ctx->stream>>>(tq, ta, tc, g, static_cast<float*>(out), prm, ctx->d_error);
-  CFDB_LAUNCHED(ctx);
+  // Programmatic stream serialisation: the CTAs of this step may become
+  // resident while the previous kernel drains; the kernel waits for it
+  // (griddepcontrol.wait) before touching global memory.
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(sh.tiles, sh.chunks);
+  cfg.blockDim = dim3(L::THREADS);
+  cfg.dynamicSmemBytes = L::SMEM_BYTES;
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  CFDB_CUDA(ctx, cudaLaunchKernelEx(&cfg, kern, tq, ta, tc, g, static_cast<float*>(out), prm, ctx->d_error));
   if (launched_grid) *launched_grid = sh.tiles * sh.chunks;
   return CFDB_OK;
 }

@@ -62,6 +62,16 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
       : "memory");
 }
 
+// Programmatic dependent launch: the sweep is launched with programmatic
+// stream serialisation, so its CTAs may become resident while the previous
+// kernel of the stream drains.  grid_dep_wait() blocks until that kernel has
+// completed and its writes are visible; it precedes every global-memory access
+// of the sweep (reads AND writes: the next step writes the buffer the previous
+// one reads).  grid_dep_launch() lets the next kernel start its own prologue.
+// Both are no-ops when the launch carries no programmatic dependency.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // Bounded wait: gives up after ~2 s of SM clocks so a lost transaction can
 // never hang the GPU; the caller records the failure in the error word.
 constexpr long long kWaitCycles = 4000000000LL;
@@ -163,6 +173,8 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
   const int x0 = int((long long)blockIdx.y * g.X / g.chunks);
   const int x1 = int((long long)(blockIdx.y + 1) * g.X / g.chunks);
   if (x0 >= x1) return;
+  grid_dep_wait();
+  grid_dep_launch();
   if (smem_u32(smem) & 127u) {
     if (threadIdx.x == 0) atomicExch(err, kErrSmemAlign);
     return;

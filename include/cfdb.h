@@ -100,6 +100,15 @@ int cfdb_sync(cfdb_ctx* ctx);
 int cfdb_ctx_set_alloc_budget(cfdb_ctx* ctx, int64_t bytes);
 int cfdb_ctx_allocated_bytes(const cfdb_ctx* ctx, int64_t* out);
 
+/* Per-call workspaces (cfdb_wave_gradient's checkpoint slots, adjoint and
+ * objective buffers) come from a stream-ordered pool owned by the context;
+ * freed workspace stays cached there, so repeated calls of one size do not
+ * allocate.  Returns the cached, unused blocks to the device (synchronises
+ * the context's stream).  No reference counterpart: the reference's RMM pool
+ * (src/pool_allocator.cpp:20, sized at src/cfdarcho_main_3d.cpp:335-341) is
+ * never trimmed. */
+int cfdb_ctx_trim(cfdb_ctx* ctx);
+
 /* CudaDataMatrix<T> allocation and from_eigen / to_eigen
  * (include/cuda_data_matrix.hpp:60-188).  upload/download are synchronous
  * with respect to the host buffer. */

@@ -50,17 +50,21 @@ def test_adjoint_step_plain_fp64_bitwise(cfdb, oracle, ctx, vert):
     assert np.array_equal(gc.cpu().numpy(), ref_gc)
 
 
-def test_adjoint_step_fused_fp32_vs_oracle(cfdb, oracle, ctx):
-    n = 12
-    m = cfdb.Mesh.structured(ctx, n, n, n, 1 / n, 1 / n, 1 / n)
-    o = oracle.Mesh(n, n, n, 1 / n, 1 / n, 1 / n)
+@pytest.mark.parametrize("shape", [(12, 12, 12), (20, 9, 16), (5, 17, 68), (7, 6, 10)])
+def test_adjoint_step_fused_fp32_vs_oracle(cfdb, oracle, ctx, shape):
+    """Sweep kernel (nz % 4 == 0; 32- and 64-wide z tiles, partial tiles,
+    walls on every side) and the gather fallback (nz = 10)."""
+    X, Y, Z = shape
+    m = cfdb.Mesh.structured(ctx, X, Y, Z, 1 / X, 1 / Y, 1 / Z)
+    o = oracle.Mesh(X, Y, Z, 1 / X, 1 / Y, 1 / Z)
     rng = np.random.default_rng(6)
     c = np.exp(0.2 * rng.standard_normal(m.n))
     q, lam1 = rng.standard_normal((2, 4 * m.n))
+    gc0 = rng.standard_normal(m.n) * 1e-3
     dt = o.wave_dt(0.4, c=c)
-    ref_lam0, ref_gc = o.wave_adjoint_step(q, lam1, c, np.zeros(m.n), dt)
+    ref_lam0, ref_gc = o.wave_adjoint_step(q, lam1, c, gc0, dt)
     lam0 = torch.empty(4 * m.n, dtype=torch.float32, device=DEV)
-    gc = torch.zeros(m.n, dtype=torch.float32, device=DEV)
+    gc = dev(gc0, torch.float32)
     ctx.wave_adjoint_step(m, dev(q, torch.float32), dev(lam1, torch.float32), lam0, dev(c, torch.float32), gc, dt,
                           path=cfdb.FUSED)
     assert rel_l2(lam0.cpu().numpy(), ref_lam0) <= 1e-6
@@ -119,6 +123,28 @@ def test_revolve_gradient_equals_store_all(cfdb, ctx, snaps):
     assert torch.equal(outs[snaps][1], outs[steps][1]) and torch.equal(outs[snaps][2], outs[steps][2])
     _, fwd = cfdb.revolve_plan(steps, snaps)
     assert outs[snaps][3] == fwd + 1 and outs[steps][3] == steps
+
+
+def test_gradient_workspace_is_pooled(cfdb, ctx):
+    """The checkpoint slots of a gradient come from the context's pool: after
+    the call nothing stays counted as allocated, a second call reuses the
+    cached blocks and gives the same result, and cfdb_ctx_trim releases them."""
+    n, steps = 16, 9
+    m = cfdb.Mesh.structured(ctx, n, n, n, 1 / n, 1 / n, 1 / n)
+    c, q0, target = setup(n)
+    dt = m.wave_dt(0.4, c=c * 1.1)
+    args = [dev(q0, torch.float32), dev(c, torch.float32), dev(target, torch.float32)]
+    before = ctx.allocated_bytes()
+    res = []
+    for _ in range(2):
+        g_c, g_p = torch.empty(m.n, device=DEV), torch.empty(m.n, device=DEV)
+        J, _ = ctx.wave_gradient(m, *args, steps, dt, steps, g_c, g_p, path=cfdb.FUSED)
+        res.append((J, g_c.cpu(), g_p.cpu()))
+        assert ctx.allocated_bytes() == before
+    assert res[0][0] == res[1][0] and torch.equal(res[0][1], res[1][1]) and torch.equal(res[0][2], res[1][2])
+    ctx.trim()
+    J, _ = ctx.wave_gradient(m, *args, steps, dt, steps, g_c, g_p, path=cfdb.FUSED)
+    assert J == res[0][0]
 
 
 def test_gradient_fp32_vs_finite_differences_full_size(cfdb, ctx):
