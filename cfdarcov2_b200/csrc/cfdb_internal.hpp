@@ -110,6 +110,9 @@ struct cfdb_mesh {
 // ---- error plumbing --------------------------------------------------------
 int cfdb_fail(cfdb_ctx* ctx, int code, const char* fmt, ...);
 int cfdb_cuda_fail(cfdb_ctx* ctx, cudaError_t e, const char* what);
+// Reads and clears the device error word (bounded waits, sweep launch
+// checks); synchronises ctx->stream.  CFDB_ETIMEOUT for a wait that gave up.
+int cfdb_check_device_error(cfdb_ctx* ctx);
 
 #define CFDB_CUDA(ctx, call)                                       \
   do {                                                             \

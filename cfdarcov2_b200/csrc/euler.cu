@@ -23,11 +23,12 @@ struct EulerPhys {
   static constexpr int NF = 5;
   static constexpr int NA = 0;
   static constexpr bool HAS_C = false;
-  static constexpr int MIN_BLOCKS = 1;
+  static constexpr int MIN_BLOCKS = 2;  // 64x8 tile, 2 cells per thread: 256 threads at <= 128 registers
   struct Params {
     float ih[3];
     float gamma;
-    float dt;  // filled per launch by begin()
+    float dt;     // filled per launch by begin()
+    float kd[3];  // dt / h_d, filled per launch by begin()
     double dx, dy, dz, cfl, t_end, vconst;
     EulerClock* clock;
     double* totals;
@@ -64,6 +65,7 @@ struct EulerPhys {
                            bits_to_double(ck->lam[ls][2])};
     bool last;
     p.dt = float(euler_dt(lam, p.dx, p.dy, p.dz, p.cfl, ck->t[ts], p.t_end, &last));
+    for (int d = 0; d < 3; ++d) p.kd[d] = p.dt * p.ih[d];
     return true;
   }
 
@@ -74,42 +76,55 @@ struct EulerPhys {
     if (dir != 0) g[1 + dir] = -q[1 + dir];
   }
 
-  __device__ static void prim(const float q[NF], float gm1, float gamma, float& ir, float u[3], float& p, float& a) {
-    ir = 1.0f / q[0];
-    u[0] = q[1] * ir; u[1] = q[2] * ir; u[2] = q[3] * ir;
-    p = gm1 * (q[4] - 0.5f * (q[1] * u[0] + q[2] * u[1] + q[3] * u[2]));
-    a = sqrtf(gamma * p * ir);
+  // 1/rho and the sound speed with the approximate reciprocal and square
+  // root of the SFU (relative error ~1e-7, far inside the FP32 solver's
+  // 1e-5 error bar against FP64; the FP64 path keeps IEEE division).
+  __device__ static float fast_rcp(float x) { return __fdividef(1.0f, x); }
+  __device__ static float fast_sqrt(float x) {
+    float r;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
   }
 
-  __device__ static void cell(const stencil::CellIn<NF>& in, const Params& a, float o[NF]) {
-    const float* P = in.P;
-    const float gm1 = a.gamma - 1.0f;
-    float irP, uP[3], pP, aP;
-    prim(P, gm1, a.gamma, irP, uP, pP, aP);
-    float acc[NF] = {0.f, 0.f, 0.f, 0.f, 0.f};
+  __device__ static void prim(const float q[NF], float gm1, float gamma, float& ir, float u[3], float& p, float& a) {
+    ir = fast_rcp(q[0]);
+    u[0] = q[1] * ir; u[1] = q[2] * ir; u[2] = q[3] * ir;
+    p = gm1 * (q[4] - 0.5f * (q[1] * u[0] + q[2] * u[1] + q[3] * u[2]));
+    a = fast_sqrt(gamma * p * ir);
+  }
+
+  // Derived per cell, computed once per cell and plane by the sweep:
+  // d = (1/rho, p, a).  A reflective or zero-gradient ghost has the same
+  // values as its cell, but the sweep derives ghosts itself anyway.
+  static constexpr int ND = 3;
+  __device__ static void derive(const float q[NF], float d[ND], const Params& a) {
+    float u[3];
+    prim(q, a.gamma - 1.0f, a.gamma, d[0], u, d[1], d[2]);
+  }
+
+  // Rusanov flux through a face with normal +e_d, L on its minus side:
+  //   F = (F_L + F_R)/2 . e_d - lambda/2 (U_R - U_L),  lambda = max(|u_d| + a)
+  // regrouped per conserved component U as U_L (u_L/2 + l) + U_R (u_R/2 - l)
+  // with l = lambda/2 (two instructions per component), the pressure terms
+  // added to the momentum and energy components.  Each face is evaluated
+  // once by the sweep (FACE_FLUX) and enters the two cells it separates with
+  // opposite signs.
+  static constexpr bool FACE_FLUX = true;
+  __device__ static void flux(const float L[NF], const float Ld[ND], const float R[NF], const float Rd[ND], int d,
+                              const Params&, float F[NF]) {
+    const float uL = L[1 + d] * Ld[0], uR = R[1 + d] * Rd[0];
+    const float pL = Ld[1], pR = Rd[1];
+    const float l = 0.5f * fmaxf(fabsf(uL) + Ld[2], fabsf(uR) + Rd[2]);
+    const float wL = 0.5f * uL + l, wR = 0.5f * uR - l;
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
+    for (int c = 0; c < NF; ++c) F[c] = L[c] * wL + R[c] * wR;
+    F[1 + d] += 0.5f * (pL + pR);
+    F[4] += 0.5f * (pL * uL + pR * uR);
+  }
+  __device__ static void update(const float P[NF], const float[ND], const float dF[3][NF], long long,
+                                const Params& a, float o[NF]) {
 #pragma unroll
-      for (int side = 0; side < 2; ++side) {
-        const float* N = in.nb[2 * d + side];
-        const float sg = side ? 1.0f : -1.0f;
-        float irN, uN[3], pN, aN;
-        prim(N, gm1, a.gamma, irN, uN, pN, aN);
-        const float unP = sg * uP[d], unN = sg * uN[d];
-        const float hl = 0.5f * fmaxf(fabsf(uP[d]) + aP, fabsf(uN[d]) + aN);
-        float f[NF];
-        f[0] = 0.5f * (P[0] * unP + N[0] * unN) - hl * (N[0] - P[0]);
-#pragma unroll
-        for (int e = 0; e < 3; ++e) f[1 + e] = 0.5f * (P[1 + e] * unP + N[1 + e] * unN) - hl * (N[1 + e] - P[1 + e]);
-        f[1 + d] += 0.5f * sg * (pP + pN);
-        f[4] = 0.5f * ((P[4] + pP) * unP + (N[4] + pN) * unN) - hl * (N[4] - P[4]);
-        const float ih = a.ih[d];
-#pragma unroll
-        for (int c = 0; c < NF; ++c) acc[c] += f[c] * ih;
-      }
-    }
-#pragma unroll
-    for (int c = 0; c < NF; ++c) o[c] = P[c] - a.dt * acc[c];
+    for (int c = 0; c < NF; ++c) o[c] = P[c] - (a.kd[0] * dF[0][c] + (a.kd[1] * dF[1][c] + a.kd[2] * dF[2][c]));
   }
 
   __device__ static void acc_init(Acc& s) {
@@ -117,20 +132,26 @@ struct EulerPhys {
     s.s0 = s.c0 = s.s1 = s.c1 = 0.0;
   }
 
+  // A thread's own cells (VZ columns of one x chunk) are summed in plain
+  // double: with 24-bit inputs the error stays near 1e-13 relative even for
+  // thousands of cells; compensation starts at the thread level, where the
+  // partial sums of millions of cells meet.  The uniform volume multiplies once.
   __device__ static void acc_cell(Acc& s, const float o[NF], const Params& a) {
     float ir, u[3], p, c;
     prim(o, a.gamma - 1.0f, a.gamma, ir, u, p, c);
     s.l[0] = fmaxf(s.l[0], fabsf(u[0]) + c);
     s.l[1] = fmaxf(s.l[1], fabsf(u[1]) + c);
     s.l[2] = fmaxf(s.l[2], fabsf(u[2]) + c);
-    comp_add(s.s0, s.c0, double(o[0]) * a.vconst);
-    comp_add(s.s1, s.c1, double(o[4]) * a.vconst);
+    s.s0 += double(o[0]);
+    s.s1 += double(o[4]);
   }
 
   __device__ static void finish(Acc& s, const Params& a, bool) {
     __shared__ double sh[32][4];
     __shared__ float shl[32][3];
     __shared__ bool is_last;
+    s.s0 *= a.vconst;
+    s.s1 *= a.vconst;
     for (int o = 16; o > 0; o >>= 1) {
       s.l[0] = fmaxf(s.l[0], __shfl_xor_sync(0xffffffffu, s.l[0], o));
       s.l[1] = fmaxf(s.l[1], __shfl_xor_sync(0xffffffffu, s.l[1], o));
@@ -193,7 +214,7 @@ struct EulerPhys {
 };
 
 constexpr int kEulerCtasPerSm = 2;
-constexpr int kEulerVZ = 4;
+constexpr int kEulerVZ = 2;
 
 template <int TZ>
 int launch_euler(cfdb_euler* e, const void* U, void* Un, int64_t s) {
@@ -210,7 +231,7 @@ int launch_euler(cfdb_euler* e, const void* U, void* Un, int64_t s) {
   return stencil::launch_sweep<EulerPhys, TZ, 8, 4, kEulerVZ>(e->ctx, m, U, nullptr, nullptr, Un, p, kEulerCtasPerSm);
 }
 
-int tz_for(const cfdb_mesh* m) { return m->nz >= 128 ? 128 : (m->nz >= 64 ? 64 : 32); }
+int tz_for(const cfdb_mesh* m) { return m->nz >= 64 ? 64 : 32; }
 
 }  // namespace
 
@@ -224,7 +245,6 @@ int euler_fused_grid(const cfdb_euler* e) {
 
 int euler_fused_step(cfdb_euler* e, const void* U, void* Un, int64_t s) {
   switch (tz_for(e->mesh)) {
-    case 128: return launch_euler<128>(e, U, Un, s);
     case 64: return launch_euler<64>(e, U, Un, s);
     default: return launch_euler<32>(e, U, Un, s);
   }
@@ -307,12 +327,7 @@ extern "C" int cfdb_euler_status(cfdb_euler* e, double* t, int64_t* steps_done, 
   EulerClock ck;
   CFDB_CUDA(e->ctx, cudaMemcpyAsync(&ck, e->clock, sizeof(ck), cudaMemcpyDeviceToHost, e->ctx->stream));
   CFDB_CUDA(e->ctx, cudaStreamSynchronize(e->ctx->stream));
-  int err = 0;
-  CFDB_CUDA(e->ctx, cudaMemcpy(&err, e->ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost));
-  if (err) {
-    cudaMemset(e->ctx->d_error, 0, sizeof(int));
-    return cfdb_fail(e->ctx, CFDB_ETIMEOUT, "a bounded device wait gave up (error word %d)", err);
-  }
+  if (int rc = cfdb_check_device_error(e->ctx)) return rc;
   const int sl = euler_slot(e->launches);
   if (t) *t = ck.t[sl];
   if (steps_done) *steps_done = ck.steps[sl];

@@ -171,10 +171,24 @@ extern "C" int cfdb_ctx_set_stream(cfdb_ctx* ctx, void* stream) {
   return CFDB_OK;
 }
 
+int cfdb_check_device_error(cfdb_ctx* ctx) {
+  int err = 0;
+  CFDB_CUDA(ctx, cudaMemcpyAsync(&err, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CFDB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (!err) return CFDB_OK;
+  CFDB_CUDA(ctx, cudaMemsetAsync(ctx->d_error, 0, sizeof(int), ctx->stream));
+  switch (err) {
+    case 1: return cfdb_fail(ctx, CFDB_ETIMEOUT, "a bounded device wait gave up (a staged copy never completed)");
+    case 2: return cfdb_fail(ctx, CFDB_ECUDA, "a sweep kernel found its shared memory misaligned for TMA");
+    case 3: return cfdb_fail(ctx, CFDB_ECUDA, "a sweep kernel was launched with less shared memory than its layout");
+    default: return cfdb_fail(ctx, CFDB_ECUDA, "device error word %d", err);
+  }
+}
+
 extern "C" int cfdb_sync(cfdb_ctx* ctx) {
   if (!ctx) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_sync: ctx is NULL");
   CFDB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  return CFDB_OK;
+  return cfdb_check_device_error(ctx);
 }
 
 extern "C" int cfdb_ctx_set_alloc_budget(cfdb_ctx* ctx, int64_t bytes) {

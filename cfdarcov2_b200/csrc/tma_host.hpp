@@ -96,7 +96,7 @@ inline SweepShape sweep_shape(const cfdb_ctx* ctx, const cfdb_mesh* m, int tz, i
 template <class Phys, int TZ, int TY, int S, int VZ = 4>
 int launch_sweep(cfdb_ctx* ctx, const cfdb_mesh* m, const void* q, const void* aux, const void* c, void* out,
                  const typename Phys::Params& prm, int ctas_per_sm, int* launched_grid = nullptr) {
-  using L = Layout<TZ, TY, S, Phys::NF, Phys::NA, Phys::HAS_C, VZ>;
+  using L = Layout<TZ, TY, S, Phys::NF, Phys::NA, Phys::HAS_C, VZ, derived_count<Phys>::value>;
   static_assert(TZ % VZ == 0 && (VZ == 1 || VZ == 2 || VZ == 4), "bad vector width");
   CUtensorMap tq, ta, tc;
   if (int rc = encode_state(ctx, &tq, q, m, Phys::NF, TZ, TY)) return rc;

@@ -118,7 +118,10 @@ class Mesh:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
-            getattr(lib(), f"fvo_mesh_destroy_{self.suf}")(h)
+            try:
+                getattr(lib(), f"fvo_mesh_destroy_{self.suf}")(h)
+            except TypeError:  # interpreter shutdown: module globals already cleared
+                pass
             self._h = None
 
     def _fn(self, name):

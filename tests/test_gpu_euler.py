@@ -73,6 +73,40 @@ def test_fused_fp32_vs_fp64_oracle(cfdb, oracle, ctx):
     assert np.abs(tot[:, 1] - tot[0, 1]).max() <= 1e-6 * tot[0, 1]
 
 
+def blast(X, Y, Z, seed=7):
+    """A 3-D state with structure along every axis: an off-centre pressure
+    and density bump plus a seeded smooth velocity field."""
+    rng = np.random.default_rng(seed)
+    x = (np.arange(X) + 0.5) / X
+    y = (np.arange(Y) + 0.5) / Y
+    z = (np.arange(Z) + 0.5) / Z
+    gx, gy, gz = np.meshgrid(x, y, z, indexing="ij")
+    r2 = (gx - 0.4) ** 2 + (gy - 0.55) ** 2 + (gz - 0.45) ** 2
+    bump = np.exp(-r2 / 0.02)
+    rho = 1.0 + 0.3 * bump
+    p = 1.0 + 2.0 * bump
+    k = rng.uniform(1, 3, size=(3, 3))
+    ph = rng.uniform(0, 2 * np.pi, size=3)
+    u = [0.2 * np.sin(2 * np.pi * (k[d, 0] * gx + k[d, 1] * gy + k[d, 2] * gz) + ph[d]) for d in range(3)]
+    E = p / 0.4 + 0.5 * rho * (u[0] ** 2 + u[1] ** 2 + u[2] ** 2)
+    return np.concatenate([rho.ravel(), (rho * u[0]).ravel(), (rho * u[1]).ravel(), (rho * u[2]).ravel(), E.ravel()])
+
+
+@pytest.mark.parametrize("shape", [(24, 20, 36), (16, 9, 68), (12, 33, 8)])
+def test_fused_fp32_3d_vs_fp64_oracle(cfdb, oracle, ctx, shape):
+    """Structure along x, y and z: exercises the face fluxes of every
+    direction, the z faces between a thread's cells and across threads and
+    tiles (32- and 64-wide z tiles, partial tiles), and every wall."""
+    X, Y, Z = shape
+    U0 = blast(X, Y, Z)
+    m = cfdb.Mesh.structured(ctx, X, Y, Z, 1 / X, 1 / Y, 1 / Z)
+    o = oracle.Mesh(X, Y, Z, 1 / X, 1 / Y, 1 / Z)
+    got, steps, t, fin, tot = run_gpu(cfdb, ctx, m, U0, cfdb.F32, cfdb.FUSED, 0.05)
+    ref, rsteps, rt, rtot = o.euler_solve(U0, 1.4, 0.4, 0.05)
+    assert fin and abs(steps - rsteps) <= 1
+    assert rel_l2(got, ref) <= 1e-5
+
+
 def test_fused_full_size_sod_matches_exact_riemann(cfdb, ctx):
     """The Sod workload at full size (512 x 64 x 64 on [0,1] x [0,0.125]^2 to
     t = 0.2): the density profile is uniform across y/z (walls are reflective
