@@ -297,8 +297,9 @@ typedef struct {
  * F32) one state pool must hold. */
 int cfdb_batch_create(cfdb_ctx* ctx, cfdb_problem* probs, int32_t count, int64_t* pool_elems, cfdb_batch** out);
 int cfdb_batch_destroy(cfdb_batch* b);
-/* cells_per_item: cells one CTA work item covers; threads: CTA size;
- * ctas_per_sm: persistent grid = SMs x ctas_per_sm. */
+/* cells_per_item: cells one CTA work item covers (threads (y, z) columns x
+ * cells_per_item / threads x planes); threads: CTA size; ctas_per_sm:
+ * persistent grid = SMs x ctas_per_sm. */
 int cfdb_batch_set_config(cfdb_batch* b, int32_t cells_per_item, int32_t threads, int32_t ctas_per_sm);
 int cfdb_batch_get_config(const cfdb_batch* b, int32_t* cells_per_item, int32_t* threads, int32_t* ctas_per_sm);
 /* Autotuner: times candidate configurations on the given pools (contents are

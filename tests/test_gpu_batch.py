@@ -21,7 +21,10 @@ def problems():
     return ensemble_problems(count=10, nmin=5, nmax=18, seed=11)
 
 
-def test_ensemble_matches_oracle_per_problem(cfdb, oracle, ctx):
+@pytest.mark.parametrize("cfg", [(256, 128, 4), (32, 32, 2), (8192, 64, 8)])
+def test_ensemble_matches_oracle_per_problem(cfdb, oracle, ctx, cfg):
+    """Work items of one plane, a few planes, and whole problems (more
+    planes than n); column runs shorter and longer than n^2."""
     from cfdarcov2_b200.workloads import ensemble_initial
     probs = problems()
     b = cfdb.Batch(ctx, probs)
@@ -34,7 +37,7 @@ def test_ensemble_matches_oracle_per_problem(cfdb, oracle, ctx):
     a = torch.tensor(pool0, device=DEV)
     c = torch.empty_like(a)
     steps = 13
-    b.set_config(256, 128, 4)
+    b.set_config(*cfg)
     b.run(a, c, steps, use_graph=True)
     got = (c if steps % 2 else a).cpu().numpy()
     assert b.launch_count() == steps
