@@ -225,6 +225,7 @@ def run_native(args, rank, world, local_rank):
     torch.cuda.synchronize()
     sampler.start()
     wall0 = time.perf_counter()
+    launches0 = ctx.launch_count()
     for k in range(args.steps):
         flush.zero_()
         a.copy_(q0)
@@ -234,6 +235,7 @@ def run_native(args, rank, world, local_rank):
     torch.cuda.synchronize()
     barrier()
     wall = time.perf_counter() - wall0
+    launches = ctx.launch_count() - launches0
     clocks = sampler.stop()
     dev_ms = sum(s.elapsed_time(e) for s, e in ev)
     t_max = torch.tensor([dev_ms], dtype=torch.float64, device=dev)
@@ -277,7 +279,7 @@ def run_native(args, rank, world, local_rank):
                      "algorithmic_bytes_per_cell_update": ALG_BYTES},
         "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": int(q0_host.numel() * 4),
                 "d2h_bytes_per_step": int(out_host.numel() * 4)},
-        "gpu_launches": args.steps * T,
+        "gpu_launches": launches,  # counted by the library (cfdb_ctx_launch_count), graph replays included
         "clocks": clocks,
         "wall_s": wall,
     }
@@ -347,8 +349,12 @@ def extras(ctx, cfdb, mesh, cfg, q0, a, b, flush, dev, n, T, peak, world):
 # ---------------------------------------------------------------------------
 # secondary workloads (one GPU): heat, distorted wave, Sod, ensemble, adjoint
 # ---------------------------------------------------------------------------
-def _timed(fn, steps, warmup, flush, prep=None):
-    """Device ms of `steps` calls of fn, each after an L2 flush and prep()."""
+LAUNCHES = {"last": None}  # kernels the library launched in the last _timed region
+
+
+def _timed(fn, steps, warmup, flush, prep=None, ctx=None):
+    """Device ms of `steps` calls of fn, each after an L2 flush and prep();
+    with ctx, LAUNCHES["last"] = the library's kernel launches in those calls."""
     import torch
     for _ in range(warmup):
         if prep:
@@ -356,21 +362,29 @@ def _timed(fn, steps, warmup, flush, prep=None):
         fn()
     torch.cuda.synchronize()
     total = 0.0
+    launches = 0
     for _ in range(steps):
         flush.zero_()
         if prep:
             prep()
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0 = ctx.launch_count() if ctx is not None else 0
         s.record()
         fn()
         e.record()
         torch.cuda.synchronize()
+        if ctx is not None:
+            launches += ctx.launch_count() - c0
         total += s.elapsed_time(e)
+    LAUNCHES["last"] = launches if ctx is not None else None
     return total
 
 
 def _line(args, workload, value, ms_per_step, cfg, alg_bytes_per_update, updates_per_launch, launches_per_step,
-          extra, dtype="f32"):
+          extra, dtype="f32", launches=None):
+    """One JSON line.  launches_per_step: time steps per bench step (the
+    roofline's per-step time); launches: kernels counted by the library in
+    the timed region (gpu_launches)."""
     peak, kind = measured_peak_hbm()
     launch_ms = ms_per_step / launches_per_step
     ach = alg_bytes_per_update * updates_per_launch / (launch_ms * 1e-3) / 1e9
@@ -380,7 +394,7 @@ def _line(args, workload, value, ms_per_step, cfg, alg_bytes_per_update, updates
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                          "traffic": None, "peak_source": f"{kind} hbm_gbs",
                          "algorithmic_bytes_per_cell_update": alg_bytes_per_update},
-            "gpu_launches": args.steps * launches_per_step}
+            "gpu_launches": launches if launches is not None else args.steps * launches_per_step}
     line.update(extra)
     print(json.dumps(line), flush=True)
 
@@ -411,8 +425,8 @@ def run_secondary(args):
             a, b = torch.empty_like(T0), torch.empty_like(T0)
             out = {}
             ms = _timed(lambda: out.__setitem__("f", ctx.heat_run(m, a, b, cfg["k"], cfg["dt"], T, path=path, use_graph=not args.eager)),
-                        K, Wm, flush, prep=lambda: a.copy_(T0))
-            res[name] = (n ** 3 * T * K / (ms * 1e-3), ms / K, out["f"].double().cpu().numpy())
+                        K, Wm, flush, prep=lambda: a.copy_(T0), ctx=ctx)
+            res[name] = (n ** 3 * T * K / (ms * 1e-3), ms / K, out["f"].double().cpu().numpy(), LAUNCHES["last"])
         if args.no_extras:
             res["fp64_plain"] = res["fp32_fused"]
         err = l2(res["fp32_fused"][2], res["fp64_plain"][2])
@@ -420,7 +434,9 @@ def run_secondary(args):
               {"mesh": [n] * 3, "k": cfg["k"], "dt": cfg["dt"], "time_steps_per_bench_step": T}, 8, n ** 3, T,
               {"fp64_plain": {"value": res["fp64_plain"][0], "unit": "cell-updates/s"},
                "speedup_fused_fp32_vs_plain_fp64": res["fp32_fused"][0] / res["fp64_plain"][0],
-               "accuracy_vs_fp64": {"l2_rel": err[0], "linf_rel": err[1]}})
+               "accuracy_vs_fp64": {"l2_rel": err[0], "linf_rel": err[1]},
+               "path": "cluster-resident (one launch per solve)" if res["fp32_fused"][3] == K else "per-step sweep"},
+              launches=res["fp32_fused"][3])
     elif args.workload == "wave_distorted":
         cfg = W.wave_config(n=args.n, steps=args.tsteps or 500)
         n, T = cfg["n"], cfg["steps"]
@@ -433,8 +449,8 @@ def run_secondary(args):
             a, b = torch.empty_like(q0), torch.empty_like(q0)
             out = {}
             ms = _timed(lambda: out.__setitem__("f", ctx.wave_run(m, a, b, dt, T, path=path, use_graph=not args.eager)), K, Wm, flush,
-                        prep=lambda: a.copy_(q0))
-            res[name] = (n ** 3 * T * K / (ms * 1e-3), ms / K, out["f"].double().cpu().numpy())
+                        prep=lambda: a.copy_(q0), ctx=ctx)
+            res[name] = (n ** 3 * T * K / (ms * 1e-3), ms / K, out["f"].double().cpu().numpy(), LAUNCHES["last"])
         if args.no_extras:
             res["fp64_plain"] = res["fp32_fused"]
         err = l2(res["fp32_fused"][2], res["fp64_plain"][2])
@@ -442,7 +458,8 @@ def run_secondary(args):
               {"mesh": [n] * 3, "jitter": "U(-0.2,0.2) dx, seed 2", "path": "compact area-vector gather"}, 72, n ** 3,
               T, {"fp64_plain": {"value": res["fp64_plain"][0], "unit": "cell-updates/s"},
                   "speedup_fused_fp32_vs_plain_fp64": res["fp32_fused"][0] / res["fp64_plain"][0],
-                  "accuracy_vs_fp64": {"l2_rel": err[0], "linf_rel": err[1]}})
+                  "accuracy_vs_fp64": {"l2_rel": err[0], "linf_rel": err[1]}},
+              launches=res["fp32_fused"][3])
     elif args.workload == "sod":
         from oracle import riemann
         cfg = W.sod_config()
@@ -460,10 +477,10 @@ def run_secondary(args):
             def solve():
                 e.begin(a)
                 out["r"] = e.run(a, b, 256)
-            ms = _timed(solve, K, Wm, flush, prep=lambda: a.copy_(U0))
+            ms = _timed(solve, K, Wm, flush, prep=lambda: a.copy_(U0), ctx=ctx)
             steps, in_b = out["r"]
             fin = (b if in_b else a).double().cpu().numpy()
-            res[name] = (nx * ny * nz * steps * K / (ms * 1e-3), ms / K, fin, steps, e.totals())
+            res[name] = (nx * ny * nz * steps * K / (ms * 1e-3), ms / K, fin, steps, e.totals(), LAUNCHES["last"])
         if args.no_extras:
             res["fp64_plain"] = res["fp32_fused"]
         err = l2(res["fp32_fused"][2], res["fp64_plain"][2])
@@ -480,7 +497,8 @@ def run_secondary(args):
                "accuracy_vs_fp64": {"l2_rel": err[0], "linf_rel": err[1]},
                "fp64_totals_drift": {"mass": float(np.abs(tot[:, 0] - tot[0, 0]).max() / tot[0, 0]),
                                      "energy": float(np.abs(tot[:, 1] - tot[0, 1]).max() / tot[0, 1])},
-               "l1_rho_vs_exact_riemann": float(np.mean(np.abs(rho - ex[0])))})
+               "l1_rho_vs_exact_riemann": float(np.mean(np.abs(rho - ex[0])))},
+              launches=res["fp32_fused"][5])
     elif args.workload == "ensemble":
         probs = W.ensemble_problems()
         b = cfdb.Batch(ctx, probs)
@@ -490,12 +508,14 @@ def run_secondary(args):
         T = args.tsteps or 300
         cells = sum(p["n"] ** 3 for p in probs)
         alg = sum(p["n"] ** 3 * (8 if p["kind"] == 0 else 32) for p in probs)
-        ms = _timed(lambda: b.run(a, c, T, use_graph=not args.eager), K, Wm, flush, prep=lambda: a.copy_(pool0))
+        ms = _timed(lambda: b.run(a, c, T, use_graph=not args.eager), K, Wm, flush, prep=lambda: a.copy_(pool0),
+                    ctx=ctx)
+        ens_launches = LAUNCHES["last"]
         _line(args, "ensemble_512_cubes_n16-96_x300_steps", cells * T * K / (ms * 1e-3), ms / K,
               {"problems": len(probs), "cells": cells, "time_steps_per_bench_step": T,
                "heat": sum(1 for p in probs if p["kind"] == 0), "wave": sum(1 for p in probs if p["kind"] == 1),
                "tuned_config": list(b.get_config())}, alg / cells, cells, T,
-              {"launches_per_step": b.launch_count() // T})
+              {"launches_per_step": b.launch_count() // T}, launches=ens_launches)
     elif args.workload == "adjoint":
         cfg = W.adjoint_config(n=args.n, steps=args.tsteps or 400)
         n, T, dt = cfg["n"], cfg["steps"], cfg["dt"]
@@ -507,7 +527,9 @@ def run_secondary(args):
         tgt = fin[: m.n].clone()
         g_c, g_p = torch.empty(m.n, device=dev), torch.empty(m.n, device=dev)
         out = {}
-        ms_grad = _timed(lambda: out.__setitem__("g", ctx.wave_gradient(m, q0, c, tgt, T, dt, T, g_c, g_p)), K, Wm, flush)
+        ms_grad = _timed(lambda: out.__setitem__("g", ctx.wave_gradient(m, q0, c, tgt, T, dt, T, g_c, g_p)), K, Wm, flush,
+                         ctx=ctx)
+        grad_launches = LAUNCHES["last"]
         ms_fwd = _timed(lambda: ctx.wave_run(m, a, bb, dt, T, c=c, speed_mode=1), K, Wm, flush, prep=lambda: a.copy_(q0))
         J, st = out["g"]
         if args.no_extras:
@@ -527,7 +549,8 @@ def run_secondary(args):
                "reverse_over_forward_sweep": st.reverse_ms / st.forward_ms,
                "forward_solve_ms": ms_fwd / K, "gradient_ms": ms_grad / K,
                "grad_rel_err_vs_fd": abs(adj - fd) / abs(fd), "fd_eps": eps, "J": J,
-               "note": "value counts forward + adjoint cell-updates; roofline uses the adjoint sweep's 60 B/cell"})
+               "note": "value counts forward + adjoint cell-updates; roofline uses the adjoint sweep's 60 B/cell"},
+              launches=grad_launches)
 
 
 def main():

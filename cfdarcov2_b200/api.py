@@ -58,6 +58,12 @@ class Context:
         call("cfdb_ctx_allocated_bytes", self.h, C.byref(v), ctx=self.h)
         return v.value
 
+    def launch_count(self) -> int:
+        """Kernels launched on this context so far (graph replays included)."""
+        v = C.c_int64()
+        call("cfdb_ctx_launch_count", self.h, C.byref(v), ctx=self.h)
+        return v.value
+
     def trim(self) -> None:
         """Returns the workspace cached by earlier calls (checkpoint slots and
         the like) to the device."""

@@ -58,6 +58,7 @@ PROTOTYPES = {
     "cfdb_ctx_set_alloc_budget": (_I, [_P, _I64]),
     "cfdb_ctx_allocated_bytes": (_I, [_P, _PI64]),
     "cfdb_ctx_trim": (_I, [_P]),
+    "cfdb_ctx_launch_count": (_I, [_P, _PI64]),
     "cfdb_alloc": (_I, [_P, _I64, _PP]),
     "cfdb_free": (_I, [_P, _P]),
     "cfdb_upload": (_I, [_P, _P, _P, _I64]),

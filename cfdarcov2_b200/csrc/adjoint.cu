@@ -32,6 +32,9 @@ struct AdjPhys {
   };
   struct Acc {};
   __device__ static bool begin(Params&) { return true; }
+  // dJ/dc of the cell so far: loaded by the sweep one plane ahead (in.pre)
+  static constexpr bool HAS_PRE = true;
+  __device__ static float* pre_ptr(const Params& a) { return a.gc; }
   // Reflective wall, as in the forward step: the ghost mirrors the
   // wall-normal component of lam and of q and copies c.  With it the
   // interior face terms below reproduce the wall terms of the transposed
@@ -56,7 +59,7 @@ struct AdjPhys {
   // leaving the h and dq.dl terms per face.  Every term is linear in lam / V
   // with one uniform V, so 1/V multiplies the sums once at the end.
   __device__ static void cell(const stencil::CellIn<FT>& in, const Params& a, float o[NF]) {
-    const float g0 = a.gc[in.idx];  // issued first: its latency hides behind the face sums
+    const float g0 = in.pre;
     const float* P = in.P;
     const float cP = P[8];
     float ap = 0.f, au[3] = {0.f, 0.f, 0.f}, gq = 0.f, gw = 0.f;
@@ -174,7 +177,7 @@ __global__ void __launch_bounds__(kThreads)
 int fused_wave_adjoint(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* q, const void* lam1, void* lam0,
                        const void* c, void* gc, double dt) {
   (void)dtype;
-  if (stencil::check_sweep(ctx, m, {q, lam1, lam0, c}) == CFDB_OK) {
+  if (stencil::check_sweep(ctx, m, {q, lam1, lam0, c, gc}) == CFDB_OK) {
     AdjPhys::Params p;
     p.A[0] = float(m->dy * m->dz); p.A[1] = float(m->dx * m->dz); p.A[2] = float(m->dx * m->dy);
     for (int d = 0; d < 3; ++d) {

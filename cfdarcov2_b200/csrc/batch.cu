@@ -374,6 +374,7 @@ extern "C" int cfdb_batch_run(cfdb_batch* b, void* a, void* out, int32_t steps, 
     ctx->stream = ctx->capture_stream;
     cudaGraph_t g = nullptr;
     int rc = CFDB_OK;
+    const int64_t before = ctx->launches;  // recorded launches run only when replayed
     cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
       rc = launch(b, a, out);
@@ -383,6 +384,7 @@ extern "C" int cfdb_batch_run(cfdb_batch* b, void* a, void* out, int32_t steps, 
     } else {
       rc = cfdb_cuda_fail(ctx, e, "cudaStreamBeginCapture");
     }
+    ctx->launches = before;
     ctx->stream = user;
     if (rc) {
       if (g) cudaGraphDestroy(g);
@@ -401,6 +403,7 @@ extern "C" int cfdb_batch_run(cfdb_batch* b, void* a, void* out, int32_t steps, 
   for (int32_t k = 0; k + 1 < steps; k += 2) {
     CFDB_CUDA(b->ctx, cudaGraphLaunch(b->graph, b->ctx->stream));
     b->last_launches += 2;
+    b->ctx->launches += 2;
   }
   if (steps & 1) {
     if (int rc = launch(b, a, out)) return rc;

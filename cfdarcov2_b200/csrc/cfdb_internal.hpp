@@ -7,6 +7,7 @@
 #include <cstdarg>
 #include <cstdint>
 #include <functional>
+#include <initializer_list>
 #include <memory>
 #include <string>
 #include <unordered_map>
@@ -74,6 +75,20 @@ struct cfdb_ctx {
   std::unordered_map<void*, int64_t> ws;
   int* d_error = nullptr;  // device error word written by bounded waits
   cudaStream_t capture_stream = nullptr;  // private stream used to record CUDA graphs
+  // Kernels launched on this context so far (graph replays count every
+  // kernel node they run).
+  int64_t launches = 0;
+  // Instantiated step graphs of cfdb_run_steps, keyed by everything the
+  // recorded launches depend on; least recently used beyond kGraphCache.
+  struct GraphEntry {
+    std::string key;
+    cudaGraphExec_t exec = nullptr;
+    int32_t chunk = 0;        // steps per replay
+    int64_t per_replay = 0;   // kernels per replay
+    uint64_t last_use = 0;
+  };
+  std::vector<GraphEntry> graphs;
+  uint64_t graph_clock = 0;
   // Objects created on this context (meshes, Euler solvers, batches) with a
   // callback that detaches them when the context is destroyed first: their
   // device memory goes with the context, their own destroy then frees only
@@ -89,13 +104,22 @@ inline void cfdb_release(cfdb_ctx* ctx, void* child) {
 }
 
 // Runs `steps` calls of step(src, dst) alternating a -> b -> a ..., eagerly or
-// replayed from a captured CUDA graph (graphs.cpp).
+// replayed from a captured CUDA graph (graphs.cpp).  `key` names everything
+// the recorded launches depend on (kernel, mesh uid, buffers, parameters); a
+// graph recorded under the same key by an earlier call is replayed without
+// recording again.  An empty key records a fresh graph every call.
 #include <functional>
 int cfdb_run_steps(cfdb_ctx* ctx, void* a, void* b, int32_t steps, int use_graph,
-                   const std::function<int(const void*, void*)>& step, int64_t* launches = nullptr);
+                   const std::function<int(const void*, void*)>& step, const std::string& key = std::string());
+void cfdb_graphs_clear(cfdb_ctx* ctx);
+// Key of a cached step graph: the step kind, the mesh (by uid), dtype, path,
+// the three buffers and the scalar parameters, bit for bit.
+std::string graph_key(const char* kind, const struct cfdb_mesh* m, int dtype, int path, const void* a, const void* b,
+                      const void* c, std::initializer_list<double> params);
 
 struct cfdb_mesh {
   cfdb_ctx* ctx = nullptr;
+  uint64_t uid = 0;  // process-unique, never reused (keys of cached step graphs)
   int64_t nx = 0, ny = 0, nz = 0, n = 0;
   double dx = 0, dy = 0, dz = 0;
   bool uniform = true;
@@ -121,7 +145,11 @@ int cfdb_check_device_error(cfdb_ctx* ctx);
   } while (0)
 
 // Checks for a launch error right after a kernel launch.
-#define CFDB_LAUNCHED(ctx) CFDB_CUDA(ctx, cudaGetLastError())
+#define CFDB_LAUNCHED(ctx)                   \
+  do {                                       \
+    ++(ctx)->launches;                       \
+    CFDB_CUDA(ctx, cudaGetLastError());      \
+  } while (0)
 
 // ---- memory ---------------------------------------------------------------
 int cfdb_dev_alloc(cfdb_ctx* ctx, int64_t bytes, void** out);
@@ -154,6 +182,11 @@ int plain_wave_adjoint(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* q, co
                        const void* c, void* gc, double dt);
 // fused_tma.cu
 int fused_heat_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* T, void* Tn, double k, double dt);
+// All `steps` FP32 heat steps in one thread-block-cluster launch with the
+// field resident in distributed shared memory (resident.cu); CFDB_EUNSUPPORTED
+// when the mesh does not fit (nothing launched).
+int heat_resident_run(cfdb_ctx* ctx, cfdb_mesh* m, const void* Ta, void* Tb, double k, double dt, int32_t steps,
+                      int* launched);
 int fused_wave_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* q, void* qn, const void* c,
                     double cconst, int mode, double dt);
 // distorted.cu

@@ -7,6 +7,7 @@
 #include <cstdlib>
 #include <string>
 
+#include "heat_cell.cuh"
 #include "tma_host.hpp"
 
 namespace {
@@ -24,11 +25,8 @@ struct HeatPhys {
   __device__ static bool begin(Params&) { return true; }
   __device__ static void ghost(float g[NF], const float p[NF], int) { g[0] = p[0]; }
   __device__ static void cell(const stencil::CellIn<1>& in, const Params& a, float o[NF]) {
-    const float t = in.P[0];
-    const float lx = (in.nb[1][0] - t) + (in.nb[0][0] - t);
-    const float ly = (in.nb[3][0] - t) + (in.nb[2][0] - t);
-    const float lz = (in.nb[5][0] - t) + (in.nb[4][0] - t);
-    o[0] = t + (a.cx * lx + (a.cy * ly + a.cz * lz));
+    o[0] = heat_update(in.P[0], in.nb[0][0], in.nb[1][0], in.nb[2][0], in.nb[3][0], in.nb[4][0], in.nb[5][0], a.cx,
+                       a.cy, a.cz);
   }
   __device__ static void acc_init(Acc&) {}
   __device__ static void acc_cell(Acc&, const float*, const Params&) {}

@@ -131,7 +131,9 @@ extern "C" int cfdb_wave_objective(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, int p
   if (int rc = B.get(int64_t(4 * R.esz) * R.n, &b)) return rc;
   if (int rc = B.get(int64_t(8) * (grid_for(ctx, R.n, kThreads, 2) + 2), &scratch)) return rc;
   if (int rc = R.copy(a, q0)) return rc;
-  if (int rc = cfdb_run_steps(ctx, a, b, steps, 1, [&](const void* s, void* d) { return R.step(s, d); })) return rc;
+  if (int rc = cfdb_run_steps(ctx, a, b, steps, 1, [&](const void* s, void* d) { return R.step(s, d); },
+                              graph_key("wave", m, dtype, path, a, b, c, {0.0, 1.0, dt})))
+    return rc;
   return R.misfit((steps & 1) ? b : a, target, nullptr, J_out, scratch);
 }
 

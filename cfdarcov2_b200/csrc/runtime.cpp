@@ -5,6 +5,7 @@
 // (include/mesh3d.hpp:209-236) with library-owned buffers, status codes and
 // no per-step allocation.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -102,6 +103,12 @@ void cfdb_ws_free(cfdb_ctx* ctx, void* p) {
   cudaFreeAsync(p, ctx->stream);
 }
 
+extern "C" int cfdb_ctx_launch_count(const cfdb_ctx* ctx, int64_t* out) {
+  if (!ctx || !out) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_ctx_launch_count: bad arguments");
+  *out = ctx->launches;
+  return CFDB_OK;
+}
+
 extern "C" int cfdb_ctx_trim(cfdb_ctx* ctx) {
   if (!ctx) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_ctx_trim: ctx is NULL");
   if (!ctx->pool) return CFDB_OK;
@@ -147,6 +154,7 @@ extern "C" int cfdb_ctx_destroy(cfdb_ctx* ctx) {
   if (!ctx) return CFDB_OK;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
+  cfdb_graphs_clear(ctx);
   if (ctx->capture_stream) cudaStreamDestroy(ctx->capture_stream);
   auto children = std::move(ctx->children);
   for (auto& kv : children) kv.second();
@@ -247,6 +255,11 @@ int check_dims(cfdb_ctx* ctx, int64_t nx, int64_t ny, int64_t nz, double dx, dou
 }
 }  // namespace
 
+static uint64_t next_mesh_uid() {
+  static std::atomic<uint64_t> uid{0};
+  return ++uid;
+}
+
 extern "C" int cfdb_mesh_create_structured(cfdb_ctx* ctx, int64_t nx, int64_t ny, int64_t nz, double dx,
                                            double dy, double dz, cfdb_mesh** out) {
   if (!out) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_mesh_create_structured: out is NULL");
@@ -255,6 +268,7 @@ extern "C" int cfdb_mesh_create_structured(cfdb_ctx* ctx, int64_t nx, int64_t ny
   auto* m = new (std::nothrow) cfdb_mesh();
   if (!m) return cfdb_fail(ctx, CFDB_ENOMEM, "host allocation failed");
   m->ctx = ctx;
+  m->uid = next_mesh_uid();
   m->nx = nx; m->ny = ny; m->nz = nz; m->n = nx * ny * nz;
   m->dx = dx; m->dy = dy; m->dz = dz;
   m->uniform = true;
@@ -276,6 +290,7 @@ extern "C" int cfdb_mesh_create_from_vertices(cfdb_ctx* ctx, int64_t nx, int64_t
   auto* m = new (std::nothrow) cfdb_mesh();
   if (!m) return cfdb_fail(ctx, CFDB_ENOMEM, "host allocation failed");
   m->ctx = ctx;
+  m->uid = next_mesh_uid();
   m->nx = nx; m->ny = ny; m->nz = nz; m->n = nx * ny * nz;
   m->dx = dx; m->dy = dy; m->dz = dz;
   m->uniform = false;

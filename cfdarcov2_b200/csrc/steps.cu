@@ -56,9 +56,19 @@ extern "C" int cfdb_heat_run(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, int path, v
                              int32_t steps, int use_graph, int* final_in_b) {
   if (int rc = check_step(ctx, m, dtype, path, "cfdb_heat_run")) return rc;
   if (!Ta || !Tb || Ta == Tb) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_heat_run: need distinct T_a and T_b");
-  int rc = cfdb_run_steps(ctx, Ta, Tb, steps, use_graph, [&](const void* src, void* dst) {
-    return cfdb_heat_step(ctx, m, dtype, path, src, dst, k, dt);
-  });
+  if (path == CFDB_PATH_FUSED && dtype == CFDB_F32 && std::isfinite(k) && std::isfinite(dt)) {
+    int launched = 0;
+    const int r = heat_resident_run(ctx, m, Ta, Tb, k, dt, steps, &launched);
+    if (r == CFDB_OK) {
+      if (final_in_b) *final_in_b = steps & 1;
+      return CFDB_OK;
+    }
+    if (r != CFDB_EUNSUPPORTED) return r;
+  }
+  int rc = cfdb_run_steps(
+      ctx, Ta, Tb, steps, use_graph,
+      [&](const void* src, void* dst) { return cfdb_heat_step(ctx, m, dtype, path, src, dst, k, dt); },
+      graph_key("heat", m, dtype, path, Ta, Tb, nullptr, {k, dt}));
   if (!rc && final_in_b) *final_in_b = steps & 1;
   return rc;
 }
@@ -67,9 +77,10 @@ extern "C" int cfdb_wave_run(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, int path, v
                              double cconst, int mode, double dt, int32_t steps, int use_graph, int* final_in_b) {
   if (int rc = check_step(ctx, m, dtype, path, "cfdb_wave_run")) return rc;
   if (!qa || !qb || qa == qb) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_wave_run: need distinct q_a and q_b");
-  int rc = cfdb_run_steps(ctx, qa, qb, steps, use_graph, [&](const void* src, void* dst) {
-    return cfdb_wave_step(ctx, m, dtype, path, src, dst, c, cconst, mode, dt);
-  });
+  int rc = cfdb_run_steps(
+      ctx, qa, qb, steps, use_graph,
+      [&](const void* src, void* dst) { return cfdb_wave_step(ctx, m, dtype, path, src, dst, c, cconst, mode, dt); },
+      graph_key("wave", m, dtype, path, qa, qb, c, {cconst, double(mode), dt}));
   if (!rc && final_in_b) *final_in_b = steps & 1;
   return rc;
 }

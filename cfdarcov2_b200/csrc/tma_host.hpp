@@ -131,6 +131,7 @@ int launch_sweep(cfdb_ctx* ctx, const cfdb_mesh* m, const void* q, const void* a
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   CFDB_CUDA(ctx, cudaLaunchKernelEx(&cfg, kern, tq, ta, tc, g, static_cast<float*>(out), prm, ctx->d_error));
+  ++ctx->launches;
   if (launched_grid) *launched_grid = sh.tiles * sh.chunks;
   return CFDB_OK;
 }

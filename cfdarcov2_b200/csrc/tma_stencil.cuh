@@ -109,7 +109,15 @@ template <int FT, int ND = 0> struct CellIn {
   float nbd[6][ND > 0 ? ND : 1];
   int walls;
   long long idx;  // cell id
+  float pre;      // Phys::pre_ptr(params)[idx], loaded one plane ahead (physics with HAS_PRE)
 };
+
+// Physics that read one per-cell value from global memory besides the staged
+// fields (Phys::HAS_PRE, pointer Phys::pre_ptr(params)): the sweep loads the
+// next plane's values while the current plane is computed, so the load
+// latency hides behind a plane of work.
+template <class P, class = void> struct has_pre { static constexpr bool value = false; };
+template <class P> struct has_pre<P, decltype(void(P::HAS_PRE))> { static constexpr bool value = P::HAS_PRE; };
 
 // Number of derived values a physics declares (Phys::ND), 0 when it has none.
 template <class P, class = void> struct derived_count { static constexpr int value = 0; };
@@ -187,6 +195,7 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
   constexpr int ND = derived_count<Phys>::value;
   constexpr int NDA = ND > 0 ? ND : 1;  // array extent
   constexpr bool FF = is_face_flux<Phys>::value;
+  constexpr bool PRE = has_pre<Phys>::value;
   using L = Layout<TZ, TY, S, NF, NA, Phys::HAS_C, VZ, ND>;
   constexpr int FT = L::FT;
   // Indexing the extern array directly keeps the accesses in the shared
@@ -360,9 +369,18 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
   Phys::acc_init(acc);
   const long long plane = (long long)g.Y * g.Z;
   const int wy = (y == 0 ? 4 : 0) | (y == g.Y - 1 ? 8 : 0);
+  // HAS_PRE: the per-cell global value of the current plane (preC) and the next one (preN)
+  float preC[VZ], preN[VZ];
+  const long long col = (long long)y * g.Z + zb;
+  if constexpr (PRE) {
+    if (active) ldv<VZ>(Phys::pre_ptr(P) + ((long long)x0 * plane + col), preC);
+  }
 
   for (int x = x0; x < x1; ++x) {
     const int k = x - x0 + 1;
+    if constexpr (PRE) {
+      if (active && x + 1 < x1) ldv<VZ>(Phys::pre_ptr(P) + ((long long)(x + 1) * plane + col), preN);
+    }
     if (x + 1 < g.X) {
       wait_plane(k + 1);
       load_center(k + 1, nxt);
@@ -517,6 +535,7 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
         }
         in.walls = w;
         in.idx = (long long)x * plane + (long long)y * g.Z + zb + j;
+        if constexpr (PRE) in.pre = preC[j];
         float o[NF];
         Phys::cell(in, P, o);
         Phys::acc_cell(acc, o, P);
@@ -548,6 +567,10 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
           if constexpr (!FF) prvD[e][j] = curD[e][j];
           curD[e][j] = nxtD[e][j];
         }
+    }
+    if constexpr (PRE) {
+#pragma unroll
+      for (int j = 0; j < VZ; ++j) preC[j] = preN[j];
     }
   }
   if (bad) atomicExch(err, kErrWaitTimeout);

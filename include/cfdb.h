@@ -109,6 +109,11 @@ int cfdb_ctx_allocated_bytes(const cfdb_ctx* ctx, int64_t* out);
  * never trimmed. */
 int cfdb_ctx_trim(cfdb_ctx* ctx);
 
+/* Kernels this context has launched so far, those run by CUDA-graph replays
+ * included (each replay adds the kernels it runs).  No reference
+ * counterpart; benchmarks read it around a timed region. */
+int cfdb_ctx_launch_count(const cfdb_ctx* ctx, int64_t* out);
+
 /* CudaDataMatrix<T> allocation and from_eigen / to_eigen
  * (include/cuda_data_matrix.hpp:60-188).  upload/download are synchronous
  * with respect to the host buffer. */
@@ -246,7 +251,11 @@ int cfdb_wave_step(cfdb_ctx* ctx, cfdb_mesh* mesh, int dtype, int path, const vo
  * equation: `steps` steps alternating a -> b -> a ...; *final_in_b = 1 when
  * the last state is in b.  use_graph captures the step launches into a CUDA
  * graph (after two eager steps that perform any one-time setup) and replays
- * it, so host launch latency never gaps the device.  Asynchronous. */
+ * it, so host launch latency never gaps the device.  Asynchronous.
+ * cfdb_heat_run, fused FP32: a uniform mesh whose field fits twice into the
+ * shared memory of one thread-block cluster (e.g. 64^3) runs all steps in one
+ * cluster launch instead, field resident on chip; same arithmetic, same
+ * result.  Only the buffer *final_in_b names is defined afterwards. */
 int cfdb_heat_run(cfdb_ctx* ctx, cfdb_mesh* mesh, int dtype, int path, void* T_a, void* T_b, double k, double dt,
                   int32_t steps, int use_graph, int* final_in_b);
 int cfdb_wave_run(cfdb_ctx* ctx, cfdb_mesh* mesh, int dtype, int path, void* q_a, void* q_b, const void* c_field,

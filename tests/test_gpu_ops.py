@@ -280,3 +280,35 @@ def test_graph_run_equals_eager_steps(cfdb, ctx, path):
 def host_t(t):
     torch.cuda.synchronize()
     return t.detach().cpu()
+
+
+@pytest.mark.parametrize("path", ["plain", "fused"])
+def test_launch_count_and_cached_graph_replay(cfdb, ctx, path):
+    """cfdb_ctx_launch_count counts every kernel, graph replays included; a
+    repeated run with the same mesh, buffers and parameters replays the
+    cached graph (no second recording) and gives the same bits as the first
+    run and as step-by-step launches."""
+    P = cfdb.FUSED if path == "fused" else cfdb.PLAIN
+    n = 32
+    m = cfdb.Mesh.structured(ctx, n, n, n, 1 / n, 1 / n, 1 / n)
+    q0 = dev(np.random.default_rng(21).standard_normal(4 * m.n), torch.float32)
+    dt = m.wave_dt(0.4)
+    a, b = q0.clone(), torch.empty_like(q0)
+    ctx.wave_step(m, a, b, dt, path=P)  # one-time setup (plain geometry upload) outside the counts
+    per_step = 1 if path == "fused" else None
+    c0 = ctx.launch_count()
+    ctx.wave_step(m, a, b, dt, path=P)
+    one = ctx.launch_count() - c0
+    if per_step is not None:
+        assert one == per_step
+    steps = 100
+    outs = []
+    for _ in range(2):
+        a.copy_(q0)
+        c0 = ctx.launch_count()
+        outs.append(host_t(ctx.wave_run(m, a, b, dt, steps, path=P, use_graph=True)).clone())
+        assert ctx.launch_count() - c0 == steps * one
+    assert torch.equal(outs[0], outs[1])
+    x, y = q0.clone(), torch.empty_like(q0)
+    ref = run_steps(lambda s, d: ctx.wave_step(m, s, d, dt, path=P), x, y, steps)
+    assert torch.equal(outs[0], host_t(ref))

@@ -1,0 +1,77 @@
+"""Cluster-resident heat solver: cfdb_heat_run (fused FP32) on meshes whose
+field fits into one thread-block cluster's shared memory runs all steps in
+one launch.  It must give exactly the per-step TMA sweep's result (the same
+cell update, heat_update(), on the same operands) and match the FP64
+oracle to the fused path's 1e-5 bar.  Which path ran is visible from the
+buffer that does not hold the result: the resident solver leaves it
+untouched, the per-step ping-pong overwrites it."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda:0"
+
+
+def field(X, Y, Z, seed=1):
+    rng = np.random.default_rng(seed)
+    x = (np.arange(X) + 0.5) / X
+    y = (np.arange(Y) + 0.5) / Y
+    z = (np.arange(Z) + 0.5) / Z
+    gx, gy, gz = np.meshgrid(x, y, z, indexing="ij")
+    T = np.exp(-((gx - 0.45) ** 2 + (gy - 0.55) ** 2 + (gz - 0.5) ** 2) / 0.02)
+    return (T + rng.uniform(-1e-3, 1e-3, T.shape)).ravel()
+
+
+@pytest.mark.parametrize("shape,steps", [((64, 64, 64), 200), ((64, 64, 64), 37), ((40, 36, 32), 12),
+                                         ((17, 24, 20), 9)])
+def test_resident_equals_per_step_sweep(cfdb, ctx, shape, steps):
+    X, Y, Z = shape
+    m = cfdb.Mesh.structured(ctx, X, Y, Z, 1 / X, 1 / Y, 1 / Z)
+    T0 = torch.tensor(field(X, Y, Z), dtype=torch.float32, device=DEV)
+    k = 0.01
+    dt = 0.1 * min(1 / X, 1 / Y, 1 / Z) ** 2 / k
+    # resident: one call; the buffer not named final keeps its contents
+    # (b: NaN; a: the initial field), where the per-step ping-pong would
+    # have overwritten it with the state one step before the last
+    a, b = T0.clone(), torch.full_like(T0, float("nan"))
+    final = ctx.heat_run(m, a, b, k, dt, steps)
+    torch.cuda.synchronize()
+    if final is a:
+        assert torch.isnan(b).all(), "the cluster-resident path did not run"
+    else:
+        assert torch.equal(a, T0), "the cluster-resident path did not run"
+    # per step: one fused sweep launch per step
+    p, q = T0.clone(), torch.empty_like(T0)
+    for s in range(steps):
+        ctx.heat_step(m, p, q, k, dt)
+        p, q = q, p
+    torch.cuda.synchronize()
+    assert torch.equal(final, p)
+
+
+def test_resident_matches_fp64_oracle(cfdb, oracle, ctx):
+    from cfdarcov2_b200.workloads import heat_config
+    cfg = heat_config()
+    n = cfg["n"]
+    m = cfdb.Mesh.structured(ctx, n, n, n, cfg["dx"], cfg["dx"], cfg["dx"])
+    o = oracle.Mesh(n, n, n, cfg["dx"], cfg["dx"], cfg["dx"])
+    ref = o.heat_solve(cfg["T0"], cfg["k"], cfg["dt"], cfg["steps"])
+    a = torch.tensor(cfg["T0"], dtype=torch.float32, device=DEV)
+    b = torch.empty_like(a)
+    got = ctx.heat_run(m, a, b, cfg["k"], cfg["dt"], cfg["steps"]).double().cpu().numpy()
+    assert rel_l2(got, ref) <= 1e-5
+
+
+def test_too_large_mesh_takes_the_per_step_path(cfdb, ctx):
+    X = Y = Z = 128  # 8 MB field: does not fit one cluster
+    m = cfdb.Mesh.structured(ctx, X, Y, Z, 1 / X, 1 / Y, 1 / Z)
+    a = torch.rand(X * Y * Z, device=DEV)
+    b = torch.full_like(a, float("nan"))
+    final = ctx.heat_run(m, a, b, 0.01, 1e-6, 4)
+    torch.cuda.synchronize()
+    assert final is a and not torch.isnan(b).any()
