@@ -10,4 +10,4 @@ from .capi import F32, F64, FUSED, PLAIN, CfdbError, lib  # noqa: F401
 
 lib()  # fail loudly at import time when the CUDA library is missing
 
-from .api import Batch, Context, Euler, Mesh, revolve_plan  # noqa: E402,F401
+from .api import Batch, Context, Euler, Mesh, revolve_plan, write_mesh_json, write_vti  # noqa: E402,F401

@@ -6,13 +6,14 @@ provider here); every computation runs in libcfdb's own kernels.
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
 from . import capi
 from .capi import F32, F64, FUSED, PLAIN, call, lib
 
-__all__ = ["Context", "Mesh", "Euler", "Batch", "F32", "F64", "PLAIN", "FUSED"]
+__all__ = ["Context", "Mesh", "Euler", "Batch", "F32", "F64", "PLAIN", "FUSED", "write_vti", "write_mesh_json"]
 
 
 def _ptr(t):
@@ -367,3 +368,25 @@ def revolve_plan(steps: int, snapshots: int):
     call("cfdb_revolve_plan", int(steps), int(snapshots), a.ctypes.data_as(C.c_void_p), g.ctypes.data_as(C.c_void_p),
          s.ctypes.data_as(C.c_void_p), n, C.byref(count), C.byref(fwd))
     return list(zip(a.tolist(), g.tolist(), s.tolist())), fwd.value
+
+
+def write_vti(path, name, values, nx, ny, nz):
+    """VTK image (.vti) of a field given in cell order (z fastest), as the
+    reference's store_history writes it; `values` is host data (numpy or a
+    CPU tensor), converted to float32."""
+    v = np.ascontiguousarray(np.asarray(values, dtype=np.float32).reshape(-1))
+    if v.size != nx * ny * nz:
+        raise ValueError("values do not match the mesh size")
+    call("cfdb_write_vti", os.fsencode(path), str(name).encode(), int(nx), int(ny), int(nz),
+         v.ctypes.data_as(C.c_void_p))
+
+
+def write_mesh_json(path, nx, ny, nz, dx, dy, dz, vertices=None):
+    """mesh.json as the reference's store_mesh writes it."""
+    ptr = None
+    if vertices is not None:
+        vertices = np.ascontiguousarray(np.asarray(vertices, dtype=np.float64).reshape(-1))
+        if vertices.size != 3 * (nx + 1) * (ny + 1) * (nz + 1):
+            raise ValueError("vertices do not match the mesh size")
+        ptr = vertices.ctypes.data_as(C.c_void_p)
+    call("cfdb_write_mesh_json", os.fsencode(path), int(nx), int(ny), int(nz), float(dx), float(dy), float(dz), ptr)

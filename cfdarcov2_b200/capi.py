@@ -15,7 +15,7 @@ _PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_PKG, "_lib", "libcfdb.so")
 HEADER_PATH = os.path.join(os.path.dirname(_PKG), "include", "cfdb.h")
 
-OK, EINVAL, ENOMEM, ECUDA, ETIMEOUT, ENUMERIC, EUNSUPPORTED = range(7)
+OK, EINVAL, ENOMEM, ECUDA, ETIMEOUT, ENUMERIC, EUNSUPPORTED, EIO = range(8)
 F32, F64 = 0, 1
 PLAIN, FUSED = 0, 1
 OP_ADD, OP_SUB, OP_MUL, OP_DIV, OP_RSUB, OP_RDIV = range(6)
@@ -59,6 +59,8 @@ PROTOTYPES = {
     "cfdb_ctx_allocated_bytes": (_I, [_P, _PI64]),
     "cfdb_ctx_trim": (_I, [_P]),
     "cfdb_ctx_launch_count": (_I, [_P, _PI64]),
+    "cfdb_write_vti": (_I, [C.c_char_p, C.c_char_p, _I64, _I64, _I64, _P]),
+    "cfdb_write_mesh_json": (_I, [C.c_char_p, _I64, _I64, _I64, _D, _D, _D, _P]),
     "cfdb_alloc": (_I, [_P, _I64, _PP]),
     "cfdb_free": (_I, [_P, _P]),
     "cfdb_upload": (_I, [_P, _P, _P, _I64]),

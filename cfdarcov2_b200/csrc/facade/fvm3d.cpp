@@ -4,6 +4,8 @@
 // allocates once.
 #include <cstdio>
 #include <cstring>
+#include <ctime>
+#include <filesystem>
 #include <stdexcept>
 #include <utility>
 
@@ -27,8 +29,18 @@ cfdb_ctx* g_ctx = nullptr;
 
 bool CFDArcoGlobalInit::skip_history = true;
 bool CFDArcoGlobalInit::cuda_enabled = false;
+bool CFDArcoGlobalInit::store_stepping = false;
+std::string CFDArcoGlobalInit::store_dir;
 
-void CFDArcoGlobalInit::initialize(int, char**, bool skip_hist) { skip_history = skip_hist; }
+void CFDArcoGlobalInit::initialize(int, char**, bool skip_hist, const std::string& store_path) {
+  skip_history = skip_hist;
+  const std::time_t t = std::time(nullptr);
+  const std::tm* now = std::localtime(&t);
+  char stamp[96];
+  std::snprintf(stamp, sizeof(stamp), "run_%d_%d_%d_%d_%d_%d", now->tm_year + 1900, now->tm_mon + 1, now->tm_mday,
+                now->tm_hour, now->tm_min, now->tm_sec);
+  store_dir = (std::filesystem::path(store_path) / stamp).string();
+}
 
 void CFDArcoGlobalInit::enable_cuda(int device) {
   if (g_ctx) return;
@@ -431,6 +443,76 @@ void Equation::evaluate(std::vector<Variable*>& all_vars, EquationTemplate& eqs,
   }
   check(cfdb_sync(ctx), "cfdb_sync");
   if (visualize) std::printf("\n");
+}
+
+// ---------------------------------------------------------------------------
+// output files (include/io_operators_tmpl.hpp)
+// ---------------------------------------------------------------------------
+namespace {
+namespace fs = std::filesystem;
+
+std::string var_dir(const Variable* v) {
+  fs::path d = fs::path(CFDArcoGlobalInit::store_dir) / (v->name.empty() ? std::string("var") : v->name);
+  fs::create_directories(d);
+  return d.string();
+}
+
+void link_latest(const fs::path& latest) {
+  std::error_code ec;
+  fs::remove_all(latest, ec);
+  fs::create_directory_symlink(fs::absolute(CFDArcoGlobalInit::store_dir), latest, ec);
+  if (ec) throw std::runtime_error("run_latest link: " + ec.message());
+}
+}  // namespace
+
+void store_history(const std::vector<Variable*>& vars_to_store, const Mesh3D* mesh) {
+  if (CFDArcoGlobalInit::store_dir.empty()) throw std::runtime_error("store_history: call CFDArcoGlobalInit::initialize first");
+  fs::create_directories(CFDArcoGlobalInit::store_dir);
+  for (const Variable* v : vars_to_store) {
+    const std::string dir = var_dir(v);
+    // every stored entry but the last, as the reference (io_operators_tmpl.hpp:53)
+    for (size_t i = 0; i + 1 < v->history.size(); ++i) {
+      const std::string path = (fs::path(dir) / ("res_" + std::to_string(i) + ".vti")).string();
+      check(cfdb_write_vti(path.c_str(), v->name.c_str(), int64_t(mesh->_x), int64_t(mesh->_y), int64_t(mesh->_z),
+                           v->history[i].data()),
+            "cfdb_write_vti");
+    }
+  }
+  link_latest(fs::absolute(fs::path(CFDArcoGlobalInit::store_dir) / ".." / "run_latest"));
+}
+
+void init_store_history_stepping(const std::vector<Variable*>& vars_to_store, const Mesh3D* mesh,
+                                 const std::string&) {
+  if (CFDArcoGlobalInit::store_dir.empty())
+    throw std::runtime_error("init_store_history_stepping: call CFDArcoGlobalInit::initialize first");
+  CFDArcoGlobalInit::store_stepping = true;
+  fs::create_directories(CFDArcoGlobalInit::store_dir);
+  for (const Variable* v : vars_to_store) var_dir(v);
+  store_mesh(mesh, CFDArcoGlobalInit::store_dir);
+}
+
+void store_history_stepping(const std::vector<Variable*>& vars_to_store, const Mesh3D*, int i) {
+  for (Variable* v : vars_to_store) {
+    const HostVec cur = v->host();
+    const std::string path = (fs::path(var_dir(v)) / (std::to_string(i) + ".bin")).string();
+    FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) throw std::runtime_error("store_history_stepping: cannot open " + path);
+    const size_t w = std::fwrite(cur.data(), sizeof(float), cur.size(), f);
+    const bool ok = std::fclose(f) == 0 && w == cur.size();
+    if (!ok) throw std::runtime_error("store_history_stepping: writing " + path + " failed");
+  }
+}
+
+void finalize_history_stepping(const std::string& store_path) {
+  link_latest(fs::absolute(fs::path(store_path) / "run_latest"));
+}
+
+void store_mesh(const Mesh3D* mesh, const std::string& store_path) {
+  fs::create_directories(store_path);
+  const std::string path = (fs::path(store_path) / "mesh.json").string();
+  check(cfdb_write_mesh_json(path.c_str(), int64_t(mesh->_x), int64_t(mesh->_y), int64_t(mesh->_z), mesh->_dx,
+                             mesh->_dy, mesh->_dz, nullptr),
+        "cfdb_write_mesh_json");
 }
 
 }  // namespace cfdb

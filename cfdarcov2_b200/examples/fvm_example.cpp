@@ -8,6 +8,10 @@
 //   fvm_example wave_d2t out.bin nx ny nz steps   d2t(u) = c^2 (d2dx(u) + d2dy(u)) (operator tree)
 //   fvm_example advect   out.bin nx ny nz steps   q = q - dt (u d1dx(q) + v d1dy(q)) + 0.01 stab_tot(q),
 //                                                 then d1t(r) = -d1dz(q) - r (operator tree)
+//   fvm_example heat_store out.bin nx ny nz steps dir
+//                                                 heat with history kept, then the reference's output
+//                                                 calls: store_history (.vti per step), mesh.json and
+//                                                 one stepping .bin of the final state under dir
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -39,7 +43,12 @@ int main(int argc, char** argv) {
                nz = std::strtoul(argv[5], nullptr, 10);
   const size_t steps = std::strtoul(argv[6], nullptr, 10);
   try {
-    CFDArcoGlobalInit::initialize(argc, argv, true);
+    const bool storing = mode == "heat_store";
+    if (storing && argc < 8) {
+      std::fprintf(stderr, "heat_store needs a store directory\n");
+      return 2;
+    }
+    CFDArcoGlobalInit::initialize(argc, argv, !storing, storing ? argv[7] : "./dumps");
     CFDArcoGlobalInit::enable_cuda(0);
     Mesh3D mesh(nx, ny, nz, 1.f / float(nx), 1.f / float(ny), 1.f / float(nz));
     mesh.init_basic_internals();
@@ -47,18 +56,24 @@ int main(int argc, char** argv) {
     std::vector<HostVec> result;
     int fused = 0;
     const auto t0 = std::chrono::steady_clock::now();
-    if (mode == "heat" || mode == "heat_bc") {
+    if (mode == "heat" || mode == "heat_bc" || storing) {
       HostVec T0 = gaussian(mesh, 0.5f, 0.5f, 0.5f, 0.1f);
-      Variable T = mode == "heat" ? Variable(&mesh, T0, boundary_none, "T")
-                                  : Variable(&mesh, T0, boundary_none, boundary_copy_cu(&mesh, T0), "T");
+      Variable T = mode == "heat_bc" ? Variable(&mesh, T0, boundary_none, boundary_copy_cu(&mesh, T0), "T")
+                                     : Variable(&mesh, T0, boundary_none, "T");
       std::vector<Variable*> space_vars{&T};
       const float h = 1.f / float(nx);
       DT dt(&mesh, UpdatePolicies::constant_dt, 0.1f * h * h / 0.01f, space_vars);
       EquationTemplate eqs = {{d1t(T), '=', 0.01f * lapl(T), true}};
       Equation eq(steps);
-      eq.evaluate(space_vars, eqs, &dt, false);
+      eq.evaluate(space_vars, eqs, &dt, false, {&T});
       fused = eq.fused_equations;
       result.push_back(T.host());
+      if (storing) {
+        store_history({&T}, &mesh);
+        init_store_history_stepping({&T}, &mesh, argv[7]);
+        store_history_stepping({&T}, &mesh, int(steps));
+        finalize_history_stepping(argv[7]);
+      }
     } else if (mode == "wave_d2t") {
       HostVec U0 = gaussian(mesh, 0.5f, 0.5f, 0.5f, 0.15f);
       Variable u(&mesh, U0, boundary_none, "u");

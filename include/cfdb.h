@@ -34,7 +34,8 @@ enum {
   CFDB_ECUDA = 3,        /* a CUDA runtime call failed */
   CFDB_ETIMEOUT = 4,     /* a bounded device-side wait gave up */
   CFDB_ENUMERIC = 5,     /* non-finite values detected */
-  CFDB_EUNSUPPORTED = 6  /* valid request this build or mesh kind cannot serve */
+  CFDB_EUNSUPPORTED = 6, /* valid request this build or mesh kind cannot serve */
+  CFDB_EIO = 7           /* a file could not be written */
 };
 
 /* Arithmetic type of a field (the reference computes in float only,
@@ -367,6 +368,25 @@ enum { CFDB_RV_ADVANCE = 1,  /* arg = steps to advance from the current state  *
  * forward steps the schedule performs. */
 int cfdb_revolve_plan(int32_t steps, int32_t snapshots, int32_t* actions, int32_t* args, int32_t* at_step,
                       int64_t capacity, int64_t* count, int64_t* forward_steps);
+
+/* ---- output files (host side, no GPU needed) ------------------------------
+ * store_history's .vti writer (include/io_operators_tmpl.hpp:44-100) without
+ * VTK: a VTK XML ImageData file with dimensions nx x ny x nz carrying one
+ * Float32 point array `name`, point (x, y, z) = values[Z*Y*x + Z*y + z]
+ * (host memory, reference cell order), written x-fastest as VTK orders image
+ * points, appended raw with UInt64 size headers.  Origin 0 and spacing 1 as
+ * the reference's vtkImageData (it never sets them), so its readers see the
+ * same grid.  Error messages go to cfdb_last_error(NULL). */
+int cfdb_write_vti(const char* path, const char* name, int64_t nx, int64_t ny, int64_t nz, const float* values);
+
+/* store_mesh (include/io_operators_tmpl.hpp:161-212) without nlohmann::json:
+ * mesh.json with "vertexes" [[x,y,z],...], "face" [{"vertexes_id": [4],
+ * "nodes_id": [...]}, ...], "nodes" [{"vertexes": [8], "face": [6]}, ...],
+ * "x", "y", "z", "lx", "ly", "lz", numbered as Mesh3D::init_basic_internals
+ * (src/mesh3d.cpp:323-416).  vertices: (nx+1)(ny+1)(nz+1) x 3 doubles in
+ * the vertex numbering, or NULL for the uniform lattice of spacing dx, dy, dz. */
+int cfdb_write_mesh_json(const char* path, int64_t nx, int64_t ny, int64_t nz, double dx, double dy, double dz,
+                         const double* vertices);
 
 #ifdef __cplusplus
 }

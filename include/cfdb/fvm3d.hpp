@@ -155,4 +155,19 @@ class Equation {
   mutable int fused_equations = 0;
 };
 
+// Output of the reference's include/io_operators_tmpl.hpp, written through
+// libcfdb's headless writers (no VTK, no nlohmann::json):
+//   store_history            store_dir/<name>/res_<i>.vti for each stored history entry but the
+//                            last, then store_dir/../run_latest -> store_dir (lines 44-103)
+//   init_store_history_stepping  directories + mesh.json (lines 105-120)
+//   store_history_stepping   store_dir/<name>/<i>.bin, raw float32 in cell order (lines 133-159)
+//   finalize_history_stepping    store_path/run_latest -> store_dir (lines 121-128)
+//   store_mesh               store_path/mesh.json (lines 161-212)
+void store_history(const std::vector<Variable*>& vars_to_store, const Mesh3D* mesh);
+void init_store_history_stepping(const std::vector<Variable*>& vars_to_store, const Mesh3D* mesh,
+                                 const std::string& store_path = "./dumps");
+void store_history_stepping(const std::vector<Variable*>& vars_to_store, const Mesh3D* mesh, int i);
+void finalize_history_stepping(const std::string& store_path = "./dumps");
+void store_mesh(const Mesh3D* mesh, const std::string& store_path);
+
 }  // namespace cfdb

@@ -21,12 +21,16 @@ void check(int status, const char* what);
 // owns the library context.
 class CFDArcoGlobalInit {
  public:
-  static void initialize(int argc, char** argv, bool skip_history = true);
+  // store_dir becomes store_path/run_<timestamp>, as the reference's
+  // initialize sets it (src/cfdarcho_main_3d.cpp:276-299)
+  static void initialize(int argc, char** argv, bool skip_history = true, const std::string& store_path = "./dumps");
   static void enable_cuda(int device = 0);
   static void finalize();
   static cfdb_ctx* ctx();
   static bool skip_history;
   static bool cuda_enabled;
+  static bool store_stepping;
+  static std::string store_dir;
 };
 
 class Mesh3D {

@@ -73,6 +73,41 @@ def test_d2t_leapfrog_operator_tree(oracle, tmp_path):
     assert rel_l2(U, u) <= 1e-5
 
 
+def test_store_history_files(oracle, tmp_path):
+    """The reference's output calls through the facade: store_history writes
+    <store_dir>/T/res_<i>.vti for every stored step but the last and links
+    run_latest; the stepping calls write mesh.json and a raw .bin of the
+    final state."""
+    import json
+    from test_io_cpu import read_vti
+    n, steps = 8, 5
+    store = tmp_path / "dumps"
+    out = tmp_path / "heat_store.bin"
+    r = subprocess.run([EXE, "heat_store", str(out), str(n), str(n), str(n), str(steps), str(store)],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    runs = [p for p in store.iterdir() if p.name.startswith("run_") and p.name != "run_latest"]
+    assert len(runs) == 1
+    run = runs[0]
+    assert (store / "run_latest").resolve() == run.resolve()
+    m = oracle.Mesh(n, n, n, 1 / n, 1 / n, 1 / n)
+    T = gaussian(m, (0.5, 0.5, 0.5), 0.1)
+    dt = float(np.float32(0.1 * (1 / n) ** 2 / 0.01))
+    vtis = sorted((run / "T").glob("res_*.vti"), key=lambda p: int(p.stem[4:]))
+    assert [p.name for p in vtis] == [f"res_{i}.vti" for i in range(steps - 1)]
+    x, y, z = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    for i, p in enumerate(vtis):
+        T = m.heat_solve(T, 0.01, dt, 1)
+        _, img = read_vti(p)
+        cells = np.empty(n ** 3, np.float32)
+        cells[n * n * x + n * y + z] = img[x + n * (y + n * z)]
+        assert rel_l2(cells.astype(np.float64), T) <= 1e-5, i
+    mesh = json.loads((run / "mesh.json").read_text())
+    assert len(mesh["nodes"]) == n ** 3 and mesh["x"] == n
+    final = np.fromfile(run / "T" / f"{steps}.bin", dtype=np.float32)
+    assert np.array_equal(final, np.fromfile(out, dtype=np.float32))
+
+
 def test_operator_tree_with_grad_stab_and_sequential_equations(oracle, tmp_path):
     n, steps = 12, 15
     (Q, R), _ = run_example(tmp_path, "advect", n, n, n, steps, nfields=2)
