@@ -113,7 +113,10 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
         for _ in ex.map(run, todo):
             pass
     if todo or _newer(objs, LIB):
-        cmd = [NVCC, *ARCH, "-shared", "-ccbin", host_cxx(), "-o", LIB, *objs, "-Xcompiler", "-fopenmp", "-lgomp"]
+        # NVRTC for the run-time compiled equation kernels (jit.cpp), found via rpath
+        cudalib = os.path.join(CUDA_HOME, "lib64")
+        cmd = [NVCC, *ARCH, "-shared", "-ccbin", host_cxx(), "-o", LIB, *objs, "-Xcompiler", "-fopenmp", "-lgomp",
+               "-L", cudalib, "-lnvrtc", "-Xlinker", f"-rpath,{cudalib}"]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)

@@ -59,6 +59,10 @@ PROTOTYPES = {
     "cfdb_ctx_allocated_bytes": (_I, [_P, _PI64]),
     "cfdb_ctx_trim": (_I, [_P]),
     "cfdb_ctx_launch_count": (_I, [_P, _PI64]),
+    "cfdb_kernel_build": (_I, [_P, C.c_char_p, C.c_char_p, _PP]),
+    "cfdb_kernel_launch": (_I, [_P, _I64, _I, _P]),
+    "cfdb_kernel_destroy": (_I, [_P]),
+    "cfdb_mesh_plain_geometry": (_I, [_P, _P]),
     "cfdb_write_vti": (_I, [C.c_char_p, C.c_char_p, _I64, _I64, _I64, _P]),
     "cfdb_write_mesh_json": (_I, [C.c_char_p, _I64, _I64, _I64, _D, _D, _D, _P]),
     "cfdb_alloc": (_I, [_P, _I64, _PP]),

@@ -112,6 +112,7 @@ inline void cfdb_release(cfdb_ctx* ctx, void* child) {
 int cfdb_run_steps(cfdb_ctx* ctx, void* a, void* b, int32_t steps, int use_graph,
                    const std::function<int(const void*, void*)>& step, const std::string& key = std::string());
 void cfdb_graphs_clear(cfdb_ctx* ctx);
+void cfdb_jit_release(cfdb_ctx* ctx);  // unloads the context's run-time compiled modules (jit.cpp)
 // Key of a cached step graph: the step kind, the mesh (by uid), dtype, path,
 // the three buffers and the scalar parameters, bit for bit.
 std::string graph_key(const char* kind, const struct cfdb_mesh* m, int dtype, int path, const void* a, const void* b,

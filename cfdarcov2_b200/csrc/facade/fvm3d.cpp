@@ -2,10 +2,14 @@
 // uses libcfdb's C ABI: every field lives in library device buffers and every
 // expression node evaluates through a cfdb_op_* kernel into a buffer it
 // allocates once.
+#include <algorithm>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <ctime>
 #include <filesystem>
+#include <map>
+#include <memory>
 #include <stdexcept>
 #include <utility>
 
@@ -203,6 +207,146 @@ const float* eval_node(Node* n) {
   return n->buf;
 }
 
+// ---- run-time generated equation kernels (KernelBuilder, src/fvm3d.cpp:1071-1394)
+// One device function per expression node, e<k>(i, A) = the node's value at
+// cell i; an operator node hands a lambda over its operand to the library's
+// cfdb_grad / cfdb_lapl / cfdb_stab, which evaluate the operand at the
+// neighbours themselves, so the whole right-hand side and the time update
+// become one kernel.  Operand order and constants are those of the operator
+// path (a constant operand as a scalar operation), and the library compiles
+// with --fmad=false, so the kernel's result equals the operator chain's bit
+// for bit.
+struct JitGen {
+  std::vector<Variable*> fields;
+  std::map<const Node*, int> done;
+  std::string funcs;
+  int next = 0;
+  bool ok = true;
+
+  static std::string lit(float v) {
+    uint32_t bits;
+    std::memcpy(&bits, &v, sizeof(bits));
+    char b[48];
+    std::snprintf(b, sizeof(b), "__uint_as_float(0x%08xu)", bits);
+    return b;
+  }
+  int field(Variable* v) {
+    for (size_t k = 0; k < fields.size(); ++k)
+      if (fields[k] == v) return int(k);
+    fields.push_back(v);
+    return int(fields.size() - 1);
+  }
+  std::string call(int k, const char* idx) { return "e" + std::to_string(k) + "(" + idx + ", A)"; }
+  int emit(const Node* n) {
+    auto it = done.find(n);
+    if (it != done.end()) return it->second;
+    std::string body;
+    static const char* ops[] = {" + ", " - ", " * ", " / "};
+    switch (n->kind) {
+      case Node::kField: body = "A.f[" + std::to_string(field(n->field)) + "][i]"; break;
+      case Node::kConst: body = lit(n->value); break;
+      case Node::kDt: body = "A.dt"; break;
+      case Node::kBinary: {
+        if (n->op < 0 || n->op > 3) {
+          ok = false;
+          return -1;
+        }
+        const int a = emit(n->a.get()), b = emit(n->b.get());
+        body = call(a, "i") + ops[n->op] + call(b, "i");
+        break;
+      }
+      case Node::kNeg: body = "-" + call(emit(n->a.get()), "i"); break;
+      case Node::kGrad:
+      case Node::kLapl:
+      case Node::kStab: {
+        const int a = emit(n->a.get());
+        const char* fn = n->kind == Node::kGrad ? "cfdb_grad" : (n->kind == Node::kLapl ? "cfdb_lapl" : "cfdb_stab");
+        body = std::string(fn) + "([&](long long j) { return " + call(a, "j") + "; }, i, " + std::to_string(n->mask) +
+               ", A.g)";
+        break;
+      }
+      default:
+        ok = false;
+        return -1;
+    }
+    const int k = next++;
+    funcs += "__device__ __forceinline__ float e" + std::to_string(k) + "(long long i, const CfdbArgs& A) { return " +
+             body + "; }\n";
+    done[n] = k;
+    return k;
+  }
+  std::string source(int root) const {
+    const size_t nf = std::max<size_t>(1, fields.size());
+    std::string s = "#include \"cfdb_jit.cuh\"\n";
+    s += "struct CfdbArgs { const float* f[" + std::to_string(nf) + "]; float dt; CfdbGeom g; };\n";
+    s += funcs;
+    s += "extern \"C\" __global__ void cfdb_equation(CfdbArgs A, float* __restrict__ out, const float* __restrict__ cur,\n"
+         "                                        const float* __restrict__ prev, int mode, long long n) {\n"
+         "  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;\n"
+         "  if (i >= n) return;\n"
+         "  const float R = e" + std::to_string(root) + "(i, A);\n"
+         "  if (mode == 0) out[i] = R;                                      // plain left-hand side\n"
+         "  else if (mode == 1) out[i] = A.dt * R + cur[i];                 // d1t, first d2t step\n"
+         "  else out[i] = (A.dt * A.dt * R + 2.0f * cur[i]) - prev[i];      // d2t\n"
+         "}\n";
+    return s;
+  }
+};
+
+// A built equation kernel and the fields its A.f[] names, in order.
+struct JitEquation {
+  cfdb_kernel* k = nullptr;
+  std::vector<Variable*> fields;
+  ~JitEquation() {
+    if (k) cfdb_kernel_destroy(k);
+  }
+};
+
+std::unique_ptr<JitEquation> jit_build(const Node* rhs) {
+  JitGen gen;
+  const int root = gen.emit(rhs);
+  if (!gen.ok || root < 0) return nullptr;
+  auto eq = std::make_unique<JitEquation>();
+  check(cfdb_kernel_build(CFDArcoGlobalInit::ctx(), gen.source(root).c_str(), "cfdb_equation", &eq->k),
+        "cfdb_kernel_build");
+  eq->fields = gen.fields;
+  return eq;
+}
+
+// KernelBuilder::run: one launch computes rhs and the update into `out`.
+void jit_run(const JitEquation& eq, Mesh3D* mesh, float dt, float* out, const float* cur, const float* prev, int mode) {
+  cfdb_plain_geometry g{};
+  check(cfdb_mesh_plain_geometry(mesh->handle(), &g), "cfdb_mesh_plain_geometry");
+  // CfdbArgs { const float* f[nf]; float dt; CfdbGeom g; } laid out as the device compiler does
+  const size_t nf = std::max<size_t>(1, eq.fields.size());
+  const size_t off_dt = nf * sizeof(void*);
+  const size_t off_g = (off_dt + sizeof(float) + 7) / 8 * 8;
+  struct Geom {
+    const int32_t* ids;
+    const float *normal, *normal_alt, *area, *alpha, *len, *volume;
+    long long n;
+  } geom{g.ids, g.normal, g.normal_alt, g.area, g.alpha, g.len, g.volume, (long long)g.n};
+  std::vector<unsigned char> A(off_g + sizeof(Geom), 0);
+  for (size_t k = 0; k < eq.fields.size(); ++k) {
+    const float* p = eq.fields[k]->current_cu;
+    std::memcpy(&A[k * sizeof(void*)], &p, sizeof(p));
+  }
+  std::memcpy(&A[off_dt], &dt, sizeof(dt));
+  std::memcpy(&A[off_g], &geom, sizeof(geom));
+  long long n = (long long)mesh->_num_nodes;
+  void* args[] = {A.data(), &out, &cur, &prev, &mode, &n};
+  check(cfdb_kernel_launch(eq.k, n, 256, args), "cfdb_kernel_launch");
+}
+
+// Whether the fused TMA step can serve this mesh (uniform, z rows of 16 bytes).
+bool stencil_fusable(Mesh3D* mesh) {
+  int64_t dims[3];
+  double h[3];
+  int uniform = 0;
+  check(cfdb_mesh_info(mesh->handle(), dims, h, &uniform), "cfdb_mesh_info");
+  return uniform && dims[2] % 4 == 0;
+}
+
 // k * lapl(T) or lapl(T) * k or lapl(T) with T the updated field: the heat
 // template that runs as one fused step.
 bool match_heat(const Node* rhs, const Variable* T, float* k) {
@@ -386,19 +530,37 @@ void Equation::evaluate(std::vector<Variable*>& all_vars, EquationTemplate& eqs,
                         std::vector<Variable*> store_vars) const {
   cfdb_ctx* ctx = CFDArcoGlobalInit::ctx();
   fused_equations = 0;
+  jit_equations = 0;
+  // use_jit equations (tuple element 3) that are not the fused heat
+  // template become one generated kernel each, built before the first step
+  std::vector<std::unique_ptr<JitEquation>> jit(eqs.size());
+  for (size_t e = 0; e < eqs.size(); ++e) {
+    Variable* lhs = std::get<0>(eqs[e]);
+    const Node* rhs = std::get<2>(eqs[e]).node.get();
+    if (!std::get<3>(eqs[e]) || !rhs) continue;
+    float k = 0.f;
+    auto* d = dynamic_cast<DtVar*>(lhs);
+    if (d && match_heat(rhs, d->var, &k) && d->var->mesh->handle() && stencil_fusable(d->var->mesh)) continue;
+    jit[e] = jit_build(rhs);
+    if (jit[e]) ++jit_equations;
+  }
   for (size_t t = 0; t < timesteps; ++t) {
     dt->update();
     const float dtv = dt->_dt;
-    for (auto& eq : eqs) {
+    for (size_t e = 0; e < eqs.size(); ++e) {
+      auto& eq = eqs[e];
       Variable* lhs = std::get<0>(eq);
       Variable& rhs = std::get<2>(eq);
+      const JitEquation* J = jit[e].get();
       if (auto* d = dynamic_cast<DtVar*>(lhs)) {
         Variable* T = d->var;
         const int64_t N = int64_t(T->mesh->_num_nodes);
         float k = 0.f;
-        if (match_heat(rhs.node.get(), T, &k) &&
-            cfdb_heat_step(ctx, T->mesh->handle(), CFDB_F32, CFDB_PATH_FUSED, T->current_cu, T->next_cu, k, dtv) ==
-                CFDB_OK) {
+        if (J) {
+          jit_run(*J, T->mesh, dtv, T->next_cu, T->current_cu, nullptr, 1);
+        } else if (match_heat(rhs.node.get(), T, &k) &&
+                   cfdb_heat_step(ctx, T->mesh->handle(), CFDB_F32, CFDB_PATH_FUSED, T->current_cu, T->next_cu, k,
+                                  dtv) == CFDB_OK) {
           if (t == 0) ++fused_equations;
         } else {
           const float* R = eval_node(rhs.node.get());
@@ -409,16 +571,24 @@ void Equation::evaluate(std::vector<Variable*>& all_vars, EquationTemplate& eqs,
         Variable* U = d2->var;
         const int64_t N = int64_t(U->mesh->_num_nodes);
         if (!U->prev_cu) U->prev_cu = device_alloc(U->mesh->_num_nodes);
-        const float* R = eval_node(rhs.node.get());
-        check(cfdb_op_d2t(ctx, CFDB_F32, R, U->current_cu, U->prev_cu, dtv, U->has_prev ? 1 : 0, U->next_cu, N),
-              "cfdb_op_d2t");
+        if (J) {
+          jit_run(*J, U->mesh, dtv, U->next_cu, U->current_cu, U->prev_cu, U->has_prev ? 2 : 1);
+        } else {
+          const float* R = eval_node(rhs.node.get());
+          check(cfdb_op_d2t(ctx, CFDB_F32, R, U->current_cu, U->prev_cu, dtv, U->has_prev ? 1 : 0, U->next_cu, N),
+                "cfdb_op_d2t");
+        }
         std::swap(U->prev_cu, U->current_cu);  // prev <- current
         std::swap(U->current_cu, U->next_cu);  // current <- next
         U->has_prev = true;
       } else if (lhs->is_field) {
-        const float* R = eval_node(rhs.node.get());
-        check(cfdb_op_scalar(ctx, CFDB_F32, CFDB_OP_MUL, R, 1.0, lhs->next_cu, int64_t(lhs->mesh->_num_nodes)),
-              "cfdb_op_scalar");
+        if (J) {
+          jit_run(*J, lhs->mesh, dtv, lhs->next_cu, nullptr, nullptr, 0);
+        } else {
+          const float* R = eval_node(rhs.node.get());
+          check(cfdb_op_scalar(ctx, CFDB_F32, CFDB_OP_MUL, R, 1.0, lhs->next_cu, int64_t(lhs->mesh->_num_nodes)),
+                "cfdb_op_scalar");
+        }
         std::swap(lhs->current_cu, lhs->next_cu);
       } else {
         throw std::runtime_error("Equation: left-hand side must be a field, d1t(field) or d2t(field)");

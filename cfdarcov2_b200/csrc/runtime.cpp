@@ -155,6 +155,7 @@ extern "C" int cfdb_ctx_destroy(cfdb_ctx* ctx) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   cfdb_graphs_clear(ctx);
+  cfdb_jit_release(ctx);
   if (ctx->capture_stream) cudaStreamDestroy(ctx->capture_stream);
   auto children = std::move(ctx->children);
   for (auto& kv : children) kv.second();
@@ -469,6 +470,23 @@ int cfdb_mesh_need_plain(cfdb_mesh* m, int dtype) {
     return rc;
   }
   p.ready = true;
+  return CFDB_OK;
+}
+
+extern "C" int cfdb_mesh_plain_geometry(cfdb_mesh* m, cfdb_plain_geometry* out) {
+  if (!out) return cfdb_fail(m ? m->ctx : nullptr, CFDB_EINVAL, "cfdb_mesh_plain_geometry: out is NULL");
+  if (!m || !m->ctx) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_mesh_plain_geometry: mesh is NULL or host-only");
+  CFDB_CUDA(m->ctx, cudaSetDevice(m->ctx->device));
+  if (int rc = cfdb_mesh_need_plain(m, CFDB_F32)) return rc;
+  const PlainGeomDev& p = m->plain[0];
+  out->ids = m->d_ids;
+  out->normal = static_cast<const float*>(p.normal);
+  out->normal_alt = static_cast<const float*>(p.normal_alt);
+  out->area = static_cast<const float*>(p.area);
+  out->alpha = static_cast<const float*>(p.alpha);
+  out->len = static_cast<const float*>(p.len);
+  out->volume = static_cast<const float*>(p.volume);
+  out->n = m->n;
   return CFDB_OK;
 }
 

@@ -8,6 +8,8 @@
 //   fvm_example wave_d2t out.bin nx ny nz steps   d2t(u) = c^2 (d2dx(u) + d2dy(u)) (operator tree)
 //   fvm_example advect   out.bin nx ny nz steps   q = q - dt (u d1dx(q) + v d1dy(q)) + 0.01 stab_tot(q),
 //                                                 then d1t(r) = -d1dz(q) - r (operator tree)
+//   fvm_example <mode>_nojit ...                  the same with use_jit = false: operator by operator
+//                                                 instead of one generated kernel per equation
 //   fvm_example heat_store out.bin nx ny nz steps dir
 //                                                 heat with history kept, then the reference's output
 //                                                 calls: store_history (.vti per step), mesh.json and
@@ -37,7 +39,10 @@ int main(int argc, char** argv) {
     std::fprintf(stderr, "usage: %s mode out.bin nx ny nz steps\n", argv[0]);
     return 2;
   }
-  const std::string mode = argv[1];
+  // "<mode>_nojit": the same equations with use_jit = false (operator-by-operator path)
+  std::string mode = argv[1];
+  const bool jit = mode.size() < 6 || mode.compare(mode.size() - 6, 6, "_nojit") != 0;
+  if (!jit) mode.resize(mode.size() - 6);
   const char* out = argv[2];
   const size_t nx = std::strtoul(argv[3], nullptr, 10), ny = std::strtoul(argv[4], nullptr, 10),
                nz = std::strtoul(argv[5], nullptr, 10);
@@ -54,7 +59,7 @@ int main(int argc, char** argv) {
     mesh.init_basic_internals();
     mesh.compute();
     std::vector<HostVec> result;
-    int fused = 0;
+    int fused = 0, jitted = 0;
     const auto t0 = std::chrono::steady_clock::now();
     if (mode == "heat" || mode == "heat_bc" || storing) {
       HostVec T0 = gaussian(mesh, 0.5f, 0.5f, 0.5f, 0.1f);
@@ -63,10 +68,11 @@ int main(int argc, char** argv) {
       std::vector<Variable*> space_vars{&T};
       const float h = 1.f / float(nx);
       DT dt(&mesh, UpdatePolicies::constant_dt, 0.1f * h * h / 0.01f, space_vars);
-      EquationTemplate eqs = {{d1t(T), '=', 0.01f * lapl(T), true}};
+      EquationTemplate eqs = {{d1t(T), '=', 0.01f * lapl(T), jit}};
       Equation eq(steps);
       eq.evaluate(space_vars, eqs, &dt, false, {&T});
       fused = eq.fused_equations;
+      jitted = eq.jit_equations;
       result.push_back(T.host());
       if (storing) {
         store_history({&T}, &mesh);
@@ -80,8 +86,10 @@ int main(int argc, char** argv) {
       std::vector<Variable*> vars{&u};
       const float c = 0.3f;
       DT dt(&mesh, UpdatePolicies::constant_dt, 0.01f, vars);
-      EquationTemplate eqs = {{d2t(u), '=', c * c * (d2dx(u) + d2dy(u)), true}};
-      Equation(steps).evaluate(vars, eqs, &dt, false);
+      EquationTemplate eqs = {{d2t(u), '=', c * c * (d2dx(u) + d2dy(u)), jit}};
+      Equation eq(steps);
+      eq.evaluate(vars, eqs, &dt, false);
+      jitted = eq.jit_equations;
       result.push_back(u.host());
     } else if (mode == "advect") {
       HostVec Q0 = gaussian(mesh, 0.4f, 0.5f, 0.5f, 0.15f), Uv(mesh._num_nodes, 0.3f), Vv(mesh._num_nodes, -0.2f),
@@ -91,10 +99,12 @@ int main(int argc, char** argv) {
       std::vector<Variable*> vars{&q, &u, &v, &r};
       DT dt(&mesh, UpdatePolicies::constant_dt, 0.002f, vars);
       EquationTemplate eqs = {
-          {&q, '=', q - dt * (u * d1dx(q) + v * d1dy(q)) + 0.01f * stab_tot(q), true},
-          {d1t(r), '=', -d1dz(q) - r, true},
+          {&q, '=', q - dt * (u * d1dx(q) + v * d1dy(q)) + 0.01f * stab_tot(q), jit},
+          {d1t(r), '=', -d1dz(q) - r, jit},
       };
-      Equation(steps).evaluate(vars, eqs, &dt, false);
+      Equation eq(steps);
+      eq.evaluate(vars, eqs, &dt, false);
+      jitted = eq.jit_equations;
       result.push_back(q.host());
       result.push_back(r.host());
     } else {
@@ -111,8 +121,8 @@ int main(int argc, char** argv) {
       sum += x;
       mx = x > mx ? x : mx;
     }
-    std::printf("mode=%s cells=%zu steps=%zu fused_equations=%d sum=%.9g max=%.9g seconds=%.6f\n", mode.c_str(),
-                mesh._num_nodes, steps, fused, sum, mx, secs);
+    std::printf("mode=%s cells=%zu steps=%zu fused_equations=%d jit_equations=%d sum=%.9g max=%.9g seconds=%.6f\n",
+                mode.c_str(), mesh._num_nodes, steps, fused, jitted, sum, mx, secs);
     CFDArcoGlobalInit::finalize();
   } catch (const std::exception& e) {
     std::fprintf(stderr, "error: %s\n", e.what());

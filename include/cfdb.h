@@ -369,6 +369,46 @@ enum { CFDB_RV_ADVANCE = 1,  /* arg = steps to advance from the current state  *
 int cfdb_revolve_plan(int32_t steps, int32_t snapshots, int32_t* actions, int32_t* args, int32_t* at_step,
                       int64_t capacity, int64_t* count, int64_t* forward_steps);
 
+/* ---- run-time compiled kernels (the KernelBuilder of src/fvm3d.cpp:1071-1394)
+ * The reference turns each use_jit equation into CUDA source and compiles
+ * it with OCCA (KernelBuilder::build, src/fvm3d.cpp:1219-1316); here NVRTC
+ * compiles for sm_100a and the CUDA runtime loads the cubin.  Generated
+ * sources may #include "cfdb_jit.cuh": struct CfdbGeom (the mesh's plain
+ * FP32 geometry, see cfdb_mesh_plain_geometry) and the device helpers
+ * cfdb_grad / cfdb_lapl / cfdb_stab of the operator layer's formulas.
+ * Compiled with --fmad=false and IEEE division, so a generated kernel
+ * rounds like the plain operator kernels it fuses. */
+typedef struct cfdb_kernel cfdb_kernel;
+
+/* Compiles `source` (once per context and source text: later calls return
+ * the cached module) and looks up the extern "C" __global__ `name`.  A
+ * compile error returns CFDB_EINVAL with the compiler log in
+ * cfdb_last_error. */
+int cfdb_kernel_build(cfdb_ctx* ctx, const char* source, const char* name, cfdb_kernel** out);
+/* KernelBuilder::run (src/fvm3d.cpp:1318-1394) without its two device
+ * syncs: launches ceil(n_threads / block) CTAs of `block` threads on the
+ * context's stream; args points to the kernel's argument values in order
+ * (the cudaLaunchKernel convention).  Asynchronous. */
+int cfdb_kernel_launch(cfdb_kernel* k, int64_t n_threads, int block, void** args);
+int cfdb_kernel_destroy(cfdb_kernel* k);
+
+/* The plain FP32 geometry of a mesh as device pointers (uploaded on first
+ * use, owned by the mesh): the inputs KernelBuilder wires into generated
+ * kernels (GradVar / Grad2Var::reset_input_pointers, src/fvm3d.cpp:1147-1216),
+ * N x 6 arrays column-major (entry (i, f) at f*n + i), per-dimension arrays
+ * stacked (d*6n + f*n + i), ids int32 with the cell itself on boundary faces. */
+typedef struct {
+  const int32_t* ids;
+  const float* normal;
+  const float* normal_alt;
+  const float* area;
+  const float* alpha;
+  const float* len;
+  const float* volume;
+  int64_t n;
+} cfdb_plain_geometry;
+int cfdb_mesh_plain_geometry(cfdb_mesh* mesh, cfdb_plain_geometry* out);
+
 /* ---- output files (host side, no GPU needed) ------------------------------
  * store_history's .vti writer (include/io_operators_tmpl.hpp:44-100) without
  * VTK: a VTK XML ImageData file with dimensions nx x ny x nz carrying one

@@ -151,8 +151,11 @@ class Equation {
   void evaluate(std::vector<Variable*>& all_vars, EquationTemplate& equation_system, DT* dt, bool visualize,
                 std::vector<Variable*> store_vars = {}) const;
   size_t timesteps;
-  // number of equations the last evaluate() ran as fused kernels
+  // number of equations the last evaluate() ran as hand-written fused kernels
   mutable int fused_equations = 0;
+  // number of use_jit equations the last evaluate() ran as one generated,
+  // run-time compiled kernel each (KernelBuilder, src/fvm3d.cpp:1219-1394)
+  mutable int jit_equations = 0;
 };
 
 // Output of the reference's include/io_operators_tmpl.hpp, written through

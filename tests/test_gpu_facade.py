@@ -73,6 +73,33 @@ def test_d2t_leapfrog_operator_tree(oracle, tmp_path):
     assert rel_l2(U, u) <= 1e-5
 
 
+@pytest.mark.parametrize("mode,nfields,n", [("advect", 2, 12), ("wave_d2t", 1, 16), ("advect", 2, 9)])
+def test_jit_equations_equal_operator_path_bitwise(tmp_path, mode, nfields, n):
+    """use_jit equations run as one NVRTC-compiled kernel each (KernelBuilder,
+    src/fvm3d.cpp:1219-1394): grad, lapl and the two-stage stab of
+    expressions, a plain left-hand side, d1t and d2t.  The generated kernel
+    rounds like the operator-by-operator path (--fmad=false, same operand
+    order), so both give the same bits; n = 9 has nz % 4 != 0."""
+    steps = 7
+    (J, out_j) = run_example(tmp_path, mode, n, n, n, steps, nfields)
+    (P, out_p) = run_example(tmp_path, mode + "_nojit", n, n, n, steps, nfields)
+    jit_eqs = 2 if mode == "advect" else 1
+    assert f"jit_equations={jit_eqs}" in out_j and "jit_equations=0" in out_p
+    assert np.array_equal(J, P)
+
+
+def test_jit_heat_on_a_mesh_the_sweep_cannot_take(oracle, tmp_path):
+    """The heat template on nz % 4 != 0 cannot use the fused TMA step; with
+    use_jit it runs as a generated kernel and matches the oracle."""
+    n, steps = 10, 20
+    (T,), out = run_example(tmp_path, "heat", n, n, n, steps)
+    assert "fused_equations=0" in out and "jit_equations=1" in out
+    m = oracle.Mesh(n, n, n, 1 / n, 1 / n, 1 / n)
+    T0 = gaussian(m, (0.5, 0.5, 0.5), 0.1)
+    dt = float(np.float32(0.1 * (1 / n) ** 2 / 0.01))
+    assert rel_l2(T, m.heat_solve(T0, 0.01, dt, steps)) <= 1e-5
+
+
 def test_store_history_files(oracle, tmp_path):
     """The reference's output calls through the facade: store_history writes
     <store_dir>/T/res_<i>.vti for every stored step but the last and links
