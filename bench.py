@@ -44,7 +44,7 @@ def parse():
     p.add_argument("--no-extras", action="store_true", help="skip the FP64, large-mesh and CPU side measurements")
     p.add_argument("--eager", action="store_true",
                    help="launch every step eagerly instead of replaying CUDA graphs (for profilers that skip graph nodes)")
-    p.add_argument("--workload", default="wave", choices=["wave", "heat", "wave_distorted", "sod", "ensemble", "adjoint"],
+    p.add_argument("--workload", default="wave", choices=["wave", "heat", "wave_distorted", "sod", "ensemble", "adjoint", "reference_rows"],
                    help="wave (default) is the headline; the others measure the remaining workloads on one GPU")
     return p.parse_args()
 
@@ -553,8 +553,55 @@ def run_secondary(args):
               launches=grad_launches)
 
 
+# the reference's own benchmark rows (scripts/benchmark_cfdarchov2.py: 200
+# time steps, unit cells, wall time of Equation::evaluate including the
+# kernel builds) run through the drop-in C++ facade; published = the
+# reference's A100 figure for the same binary and mesh (Mcell-updates/s,
+# scripts/v2_results/report_history_a100_cuda_full_no_data_move_even_better.csv)
+REFERENCE_ROWS = [
+    ("heat", "ref_heat", 200, 6440.3, "main_3d_heat.cpp: d1t(T) = 3 lapl(T), boundary copy, dt 0.005"),
+    ("wave", "ref_wave", 400, 7258.6, "main_3d_wave.cu: d2t(u) = c^2 (d2dx(u) + d2dy(u)), sine driver, dt 0.1"),
+    ("euler", "euler3d", 200, 264.7, "main_3d.cpp: 20-equation central + stab Euler system, CFL 0.005"),
+]
+
+
+def run_reference_rows(args):
+    """One JSON line per reference benchmark row: value = cells x 200 steps /
+    the wall time of the first Equation::evaluate (kernel builds included,
+    as the reference times it); steady = the same for a second evaluate."""
+    import subprocess
+    exe = os.path.join(ROOT, "cfdarcov2_b200", "_lib", "fvm_example")
+    if not os.path.exists(exe):
+        raise SystemExit("fvm_example is not built; run `python -m cfdarcov2_b200.build`")
+    steps = 200
+    for name, mode, n, published, what in REFERENCE_ROWS:
+        r = subprocess.run([exe, mode + "_twice", os.devnull, str(n), str(n), str(n), str(steps)],
+                           capture_output=True, text=True, timeout=900)
+        if r.returncode != 0:
+            raise SystemExit(f"{mode}: exit {r.returncode}: {r.stderr[-2000:]}")
+        kv = dict(tok.split("=", 1) for line in r.stdout.splitlines() for tok in line.split() if "=" in tok)
+        first_us, steady_us = float(kv["evaluate_us"]), float(kv["steady_us"])
+        cells = n ** 3 * steps
+        value = cells / (first_us * 1e-6) / 1e6
+        print(json.dumps({
+            "metric": "Mcell-updates/s (reference benchmark row, wall time of Equation::evaluate)",
+            "value": value, "unit": "Mcell-updates/s", "n_gpus": 1, "steps": 1, "warmup": 0,
+            "ms_per_step": first_us / 1e3 / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": value / published, "baseline_published": published, "baseline_hardware": "A100",
+            "dtype": "f32", "data": "synthetic (the reference example's initial state)",
+            "config": {"workload": f"reference_{name}_{n}^3_x{steps}_steps", "system": what,
+                       "path": "C++ facade (include/cfdb/fvm3d.hpp), use_jit equations"},
+            "steady": {"value": cells / (steady_us * 1e-6) / 1e6, "unit": "Mcell-updates/s",
+                       "note": "second evaluate on the same variables: no kernel builds"},
+            "facade_counts": {k: int(kv[k]) for k in ("jit_equations", "fused_equations") if k in kv},
+        }), flush=True)
+
+
 def main():
     args = parse()
+    if args.workload == "reference_rows":
+        run_reference_rows(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

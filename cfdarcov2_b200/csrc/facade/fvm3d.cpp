@@ -208,20 +208,68 @@ const float* eval_node(Node* n) {
 }
 
 // ---- run-time generated equation kernels (KernelBuilder, src/fvm3d.cpp:1071-1394)
-// One device function per expression node, e<k>(i, A) = the node's value at
-// cell i; an operator node hands a lambda over its operand to the library's
-// cfdb_grad / cfdb_lapl / cfdb_stab, which evaluate the operand at the
-// neighbours themselves, so the whole right-hand side and the time update
-// become one kernel.  Operand order and constants are those of the operator
-// path (a constant operand as a scalar operation), and the library compiles
-// with --fmad=false, so the kernel's result equals the operator chain's bit
-// for bit.
+// An equation becomes a short plan of generated kernels: the pointwise part
+// of the right-hand side, the operators on fields and the time update fuse
+// into the last one; an operator whose operand is an expression first
+// materialises the operand in its own pass (so no cell recomputes a
+// neighbour's expression), and a stabilisation first writes its stage-1
+// face values in a pass of their own.  Inside a kernel there is one device
+// function per expression node, e<k>(i, A) = the node's value at cell i.
+// Operand order and constants are those of the operator path (a constant
+// operand as a scalar operation), and the library compiles with
+// --fmad=false, so the plan's result equals the operator chain's bit for
+// bit.
+
+// An input of a generated kernel: a field's current buffer (looked up at
+// launch time: fields swap buffers every step) or a scratch buffer of the plan.
+struct JitInput {
+  Variable* field = nullptr;
+  int scratch = -1;
+  bool operator==(const JitInput& o) const { return field == o.field && scratch == o.scratch; }
+};
+
+struct JitPass {
+  cfdb_kernel* k = nullptr;
+  std::vector<JitInput> inputs;
+  int out_scratch = -1;  // -1: the equation's output (the last pass)
+  ~JitPass() {
+    if (k) cfdb_kernel_destroy(k);
+  }
+};
+
+struct JitPlan {
+  Mesh3D* mesh = nullptr;
+  std::vector<std::unique_ptr<JitPass>> passes;  // run order; the last computes the equation
+  std::vector<float*> scratch;
+  std::map<const Node*, int> materialised;
+  std::vector<std::pair<JitInput, int>> stab_stage1;
+  bool ok = true;
+  ~JitPlan() {
+    for (float* p : scratch) device_free(p);
+  }
+  int new_scratch(size_t floats) {
+    scratch.push_back(device_alloc(floats));
+    return int(scratch.size() - 1);
+  }
+  int materialise(const Node* n);
+  int stab1(const JitInput& in);
+  void add_pass(const std::string& src, const char* entry, std::vector<JitInput> inputs, int out) {
+    auto p = std::make_unique<JitPass>();
+    check(cfdb_kernel_build(CFDArcoGlobalInit::ctx(), src.c_str(), entry, &p->k), "cfdb_kernel_build");
+    p->inputs = std::move(inputs);
+    p->out_scratch = out;
+    passes.push_back(std::move(p));
+  }
+};
+
+// One generated kernel.
 struct JitGen {
-  std::vector<Variable*> fields;
+  JitPlan& plan;
+  std::vector<JitInput> inputs;
   std::map<const Node*, int> done;
   std::string funcs;
   int next = 0;
-  bool ok = true;
+  explicit JitGen(JitPlan& p) : plan(p) {}
 
   static std::string lit(float v) {
     uint32_t bits;
@@ -230,43 +278,65 @@ struct JitGen {
     std::snprintf(b, sizeof(b), "__uint_as_float(0x%08xu)", bits);
     return b;
   }
-  int field(Variable* v) {
-    for (size_t k = 0; k < fields.size(); ++k)
-      if (fields[k] == v) return int(k);
-    fields.push_back(v);
-    return int(fields.size() - 1);
+  int input(const JitInput& in) {
+    for (size_t k = 0; k < inputs.size(); ++k)
+      if (inputs[k] == in) return int(k);
+    inputs.push_back(in);
+    return int(inputs.size() - 1);
   }
-  std::string call(int k, const char* idx) { return "e" + std::to_string(k) + "(" + idx + ", A)"; }
+  // operand of a neighbour operator: a field as it is, an expression materialised by an earlier pass
+  JitInput operand(const Node* n) {
+    JitInput in;
+    if (n->kind == Node::kField) in.field = n->field;
+    else in.scratch = plan.materialise(n);
+    return in;
+  }
+  std::string call(int k) { return "e" + std::to_string(k) + "(i, A)"; }
   int emit(const Node* n) {
     auto it = done.find(n);
     if (it != done.end()) return it->second;
+    if (!plan.ok) return -1;
     std::string body;
     static const char* ops[] = {" + ", " - ", " * ", " / "};
     switch (n->kind) {
-      case Node::kField: body = "A.f[" + std::to_string(field(n->field)) + "][i]"; break;
+      case Node::kField: body = "A.f[" + std::to_string(input(JitInput{n->field, -1})) + "][i]"; break;
       case Node::kConst: body = lit(n->value); break;
       case Node::kDt: body = "A.dt"; break;
       case Node::kBinary: {
         if (n->op < 0 || n->op > 3) {
-          ok = false;
+          plan.ok = false;
           return -1;
         }
         const int a = emit(n->a.get()), b = emit(n->b.get());
-        body = call(a, "i") + ops[n->op] + call(b, "i");
+        if (a < 0 || b < 0) return -1;
+        body = call(a) + ops[n->op] + call(b);
         break;
       }
-      case Node::kNeg: body = "-" + call(emit(n->a.get()), "i"); break;
-      case Node::kGrad:
-      case Node::kLapl:
-      case Node::kStab: {
+      case Node::kNeg: {
         const int a = emit(n->a.get());
-        const char* fn = n->kind == Node::kGrad ? "cfdb_grad" : (n->kind == Node::kLapl ? "cfdb_lapl" : "cfdb_stab");
-        body = std::string(fn) + "([&](long long j) { return " + call(a, "j") + "; }, i, " + std::to_string(n->mask) +
+        if (a < 0) return -1;
+        body = "-" + call(a);
+        break;
+      }
+      case Node::kGrad:
+      case Node::kLapl: {
+        const JitInput src = operand(n->a.get());
+        if (!plan.ok) return -1;
+        const std::string f = "A.f[" + std::to_string(input(src)) + "]";
+        body = std::string(n->kind == Node::kGrad ? "cfdb_grad" : "cfdb_lapl") + "([&](long long j) { return " + f +
+               "[j]; }, i, " + std::to_string(n->mask) + ", A.g)";
+        break;
+      }
+      case Node::kStab: {
+        const JitInput src = operand(n->a.get());
+        if (!plan.ok) return -1;
+        const int up = plan.stab1(src);
+        body = "cfdb_stab2(A.f[" + std::to_string(input(JitInput{nullptr, up})) + "], i, " + std::to_string(n->mask) +
                ", A.g)";
         break;
       }
       default:
-        ok = false;
+        plan.ok = false;
         return -1;
     }
     const int k = next++;
@@ -275,67 +345,95 @@ struct JitGen {
     done[n] = k;
     return k;
   }
-  std::string source(int root) const {
-    const size_t nf = std::max<size_t>(1, fields.size());
-    std::string s = "#include \"cfdb_jit.cuh\"\n";
-    s += "struct CfdbArgs { const float* f[" + std::to_string(nf) + "]; float dt; CfdbGeom g; };\n";
-    s += funcs;
-    s += "extern \"C\" __global__ void cfdb_equation(CfdbArgs A, float* __restrict__ out, const float* __restrict__ cur,\n"
-         "                                        const float* __restrict__ prev, int mode, long long n) {\n"
-         "  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;\n"
-         "  if (i >= n) return;\n"
-         "  const float R = e" + std::to_string(root) + "(i, A);\n"
-         "  if (mode == 0) out[i] = R;                                      // plain left-hand side\n"
-         "  else if (mode == 1) out[i] = A.dt * R + cur[i];                 // d1t, first d2t step\n"
-         "  else out[i] = (A.dt * A.dt * R + 2.0f * cur[i]) - prev[i];      // d2t\n"
-         "}\n";
-    return s;
+  std::string prelude() const {
+    return "#include \"cfdb_jit.cuh\"\nstruct CfdbArgs { const float* f[" +
+           std::to_string(std::max<size_t>(1, inputs.size())) + "]; float dt; CfdbGeom g; };\n";
+  }
+  // every generated kernel has the signature (A, out, cur, prev, mode, n)
+  std::string equation_source(int root) const {
+    return prelude() + funcs +
+           "extern \"C\" __global__ void cfdb_equation(CfdbArgs A, float* __restrict__ out, const float* __restrict__ cur,\n"
+           "                                        const float* __restrict__ prev, int mode, long long n) {\n"
+           "  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;\n"
+           "  if (i >= n) return;\n"
+           "  const float R = e" + std::to_string(root) + "(i, A);\n"
+           "  if (mode == 0) out[i] = R;                                      // plain left-hand side, scratch\n"
+           "  else if (mode == 1) out[i] = A.dt * R + cur[i];                 // d1t, first d2t step\n"
+           "  else out[i] = (A.dt * A.dt * R + 2.0f * cur[i]) - prev[i];      // d2t\n"
+           "}\n";
   }
 };
 
-// A built equation kernel and the fields its A.f[] names, in order.
-struct JitEquation {
-  cfdb_kernel* k = nullptr;
-  std::vector<Variable*> fields;
-  ~JitEquation() {
-    if (k) cfdb_kernel_destroy(k);
+int JitPlan::materialise(const Node* n) {
+  auto it = materialised.find(n);
+  if (it != materialised.end()) return it->second;
+  JitGen g(*this);
+  const int root = g.emit(n);
+  if (!ok || root < 0) {
+    ok = false;
+    return -1;
   }
-};
-
-std::unique_ptr<JitEquation> jit_build(const Node* rhs) {
-  JitGen gen;
-  const int root = gen.emit(rhs);
-  if (!gen.ok || root < 0) return nullptr;
-  auto eq = std::make_unique<JitEquation>();
-  check(cfdb_kernel_build(CFDArcoGlobalInit::ctx(), gen.source(root).c_str(), "cfdb_equation", &eq->k),
-        "cfdb_kernel_build");
-  eq->fields = gen.fields;
-  return eq;
+  const int s = new_scratch(mesh->_num_nodes);
+  add_pass(g.equation_source(root), "cfdb_equation", g.inputs, s);
+  materialised[n] = s;
+  return s;
 }
 
-// KernelBuilder::run: one launch computes rhs and the update into `out`.
-void jit_run(const JitEquation& eq, Mesh3D* mesh, float dt, float* out, const float* cur, const float* prev, int mode) {
+int JitPlan::stab1(const JitInput& in) {
+  for (auto& kv : stab_stage1)
+    if (kv.first == in) return kv.second;
+  const int s = new_scratch(18 * mesh->_num_nodes);
+  const std::string src = "#include \"cfdb_jit.cuh\"\nstruct CfdbArgs { const float* f[1]; float dt; CfdbGeom g; };\n"
+                          "extern \"C\" __global__ void cfdb_stab_stage1(CfdbArgs A, float* __restrict__ up, const float*,\n"
+                          "                                           const float*, int, long long n) {\n"
+                          "  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;\n"
+                          "  if (i >= n) return;\n"
+                          "  cfdb_stab1([&](long long j) { return A.f[0][j]; }, i, up, A.g);\n"
+                          "}\n";
+  add_pass(src, "cfdb_stab_stage1", {in}, s);
+  stab_stage1.emplace_back(in, s);
+  return s;
+}
+
+std::unique_ptr<JitPlan> jit_build(const Node* rhs, Mesh3D* mesh) {
+  auto plan = std::make_unique<JitPlan>();
+  plan->mesh = mesh;
+  JitGen g(*plan);
+  const int root = g.emit(rhs);
+  if (!plan->ok || root < 0) return nullptr;
+  plan->add_pass(g.equation_source(root), "cfdb_equation", g.inputs, -1);
+  return plan;
+}
+
+// KernelBuilder::run: the plan's passes in order; the last one writes the
+// equation's update (mode 0: value, 1: d1t, 2: d2t) into `out`.
+void jit_run(const JitPlan& plan, float dt, float* out, const float* cur, const float* prev, int mode) {
   cfdb_plain_geometry g{};
-  check(cfdb_mesh_plain_geometry(mesh->handle(), &g), "cfdb_mesh_plain_geometry");
-  // CfdbArgs { const float* f[nf]; float dt; CfdbGeom g; } laid out as the device compiler does
-  const size_t nf = std::max<size_t>(1, eq.fields.size());
-  const size_t off_dt = nf * sizeof(void*);
-  const size_t off_g = (off_dt + sizeof(float) + 7) / 8 * 8;
+  check(cfdb_mesh_plain_geometry(plan.mesh->handle(), &g), "cfdb_mesh_plain_geometry");
   struct Geom {
     const int32_t* ids;
     const float *normal, *normal_alt, *area, *alpha, *len, *volume;
     long long n;
   } geom{g.ids, g.normal, g.normal_alt, g.area, g.alpha, g.len, g.volume, (long long)g.n};
-  std::vector<unsigned char> A(off_g + sizeof(Geom), 0);
-  for (size_t k = 0; k < eq.fields.size(); ++k) {
-    const float* p = eq.fields[k]->current_cu;
-    std::memcpy(&A[k * sizeof(void*)], &p, sizeof(p));
+  long long n = (long long)plan.mesh->_num_nodes;
+  for (const auto& p : plan.passes) {
+    // CfdbArgs { const float* f[nf]; float dt; CfdbGeom g; } laid out as the device compiler does
+    const size_t nf = std::max<size_t>(1, p->inputs.size());
+    const size_t off_dt = nf * sizeof(void*);
+    const size_t off_g = (off_dt + sizeof(float) + 7) / 8 * 8;
+    std::vector<unsigned char> A(off_g + sizeof(Geom), 0);
+    for (size_t k = 0; k < p->inputs.size(); ++k) {
+      const JitInput& in = p->inputs[k];
+      const float* ptr = in.field ? in.field->current_cu : plan.scratch[size_t(in.scratch)];
+      std::memcpy(&A[k * sizeof(void*)], &ptr, sizeof(ptr));
+    }
+    std::memcpy(&A[off_dt], &dt, sizeof(dt));
+    std::memcpy(&A[off_g], &geom, sizeof(geom));
+    float* o = p->out_scratch >= 0 ? plan.scratch[size_t(p->out_scratch)] : out;
+    int m = p->out_scratch >= 0 ? 0 : mode;
+    void* args[] = {A.data(), &o, &cur, &prev, &m, &n};
+    check(cfdb_kernel_launch(p->k, n, 256, args), "cfdb_kernel_launch");
   }
-  std::memcpy(&A[off_dt], &dt, sizeof(dt));
-  std::memcpy(&A[off_g], &geom, sizeof(geom));
-  long long n = (long long)mesh->_num_nodes;
-  void* args[] = {A.data(), &out, &cur, &prev, &mode, &n};
-  check(cfdb_kernel_launch(eq.k, n, 256, args), "cfdb_kernel_launch");
 }
 
 // Whether the fused TMA step can serve this mesh (uniform, z rows of 16 bytes).
@@ -532,16 +630,19 @@ void Equation::evaluate(std::vector<Variable*>& all_vars, EquationTemplate& eqs,
   fused_equations = 0;
   jit_equations = 0;
   // use_jit equations (tuple element 3) that are not the fused heat
-  // template become one generated kernel each, built before the first step
-  std::vector<std::unique_ptr<JitEquation>> jit(eqs.size());
+  // template become a plan of generated kernels each, built before the first step
+  std::vector<std::unique_ptr<JitPlan>> jit(eqs.size());
   for (size_t e = 0; e < eqs.size(); ++e) {
     Variable* lhs = std::get<0>(eqs[e]);
     const Node* rhs = std::get<2>(eqs[e]).node.get();
     if (!std::get<3>(eqs[e]) || !rhs) continue;
     float k = 0.f;
     auto* d = dynamic_cast<DtVar*>(lhs);
-    if (d && match_heat(rhs, d->var, &k) && d->var->mesh->handle() && stencil_fusable(d->var->mesh)) continue;
-    jit[e] = jit_build(rhs);
+    auto* d2 = dynamic_cast<D2tVar*>(lhs);
+    Mesh3D* mesh = d ? d->var->mesh : (d2 ? d2->var->mesh : lhs->mesh);
+    if (!mesh) continue;
+    if (d && match_heat(rhs, d->var, &k) && stencil_fusable(d->var->mesh)) continue;
+    jit[e] = jit_build(rhs, mesh);
     if (jit[e]) ++jit_equations;
   }
   for (size_t t = 0; t < timesteps; ++t) {
@@ -551,13 +652,13 @@ void Equation::evaluate(std::vector<Variable*>& all_vars, EquationTemplate& eqs,
       auto& eq = eqs[e];
       Variable* lhs = std::get<0>(eq);
       Variable& rhs = std::get<2>(eq);
-      const JitEquation* J = jit[e].get();
+      const JitPlan* J = jit[e].get();
       if (auto* d = dynamic_cast<DtVar*>(lhs)) {
         Variable* T = d->var;
         const int64_t N = int64_t(T->mesh->_num_nodes);
         float k = 0.f;
         if (J) {
-          jit_run(*J, T->mesh, dtv, T->next_cu, T->current_cu, nullptr, 1);
+          jit_run(*J, dtv, T->next_cu, T->current_cu, nullptr, 1);
         } else if (match_heat(rhs.node.get(), T, &k) &&
                    cfdb_heat_step(ctx, T->mesh->handle(), CFDB_F32, CFDB_PATH_FUSED, T->current_cu, T->next_cu, k,
                                   dtv) == CFDB_OK) {
@@ -572,7 +673,7 @@ void Equation::evaluate(std::vector<Variable*>& all_vars, EquationTemplate& eqs,
         const int64_t N = int64_t(U->mesh->_num_nodes);
         if (!U->prev_cu) U->prev_cu = device_alloc(U->mesh->_num_nodes);
         if (J) {
-          jit_run(*J, U->mesh, dtv, U->next_cu, U->current_cu, U->prev_cu, U->has_prev ? 2 : 1);
+          jit_run(*J, dtv, U->next_cu, U->current_cu, U->prev_cu, U->has_prev ? 2 : 1);
         } else {
           const float* R = eval_node(rhs.node.get());
           check(cfdb_op_d2t(ctx, CFDB_F32, R, U->current_cu, U->prev_cu, dtv, U->has_prev ? 1 : 0, U->next_cu, N),
@@ -583,7 +684,7 @@ void Equation::evaluate(std::vector<Variable*>& all_vars, EquationTemplate& eqs,
         U->has_prev = true;
       } else if (lhs->is_field) {
         if (J) {
-          jit_run(*J, lhs->mesh, dtv, lhs->next_cu, nullptr, nullptr, 0);
+          jit_run(*J, dtv, lhs->next_cu, nullptr, nullptr, 0);
         } else {
           const float* R = eval_node(rhs.node.get());
           check(cfdb_op_scalar(ctx, CFDB_F32, CFDB_OP_MUL, R, 1.0, lhs->next_cu, int64_t(lhs->mesh->_num_nodes)),

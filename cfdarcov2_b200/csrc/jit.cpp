@@ -5,13 +5,12 @@
 // on the context's stream.  Modules are cached per context by source text.
 //
 // Generated sources may include "cfdb_jit.cuh" (kJitHeader below): the
-// operator layer's Green-Gauss gradient, orthogonal Laplacian and two-stage
-// stabilisation as device templates over a callable that evaluates the
-// operand at any cell, so an operator of an expression fuses into one
-// kernel.  Their arithmetic and its order are those of plain_ops.cu's
-// grad_k, lapl_at and stab1_k/stab2_k; compiled with --fmad=false and IEEE
-// division as plain_ops.cu is, a fused kernel rounds exactly like the chain
-// of operator kernels it replaces.
+// operator layer's Green-Gauss gradient, orthogonal Laplacian and the two
+// stages of the stabilisation as device templates over a callable that
+// reads the operand at any cell.  Their arithmetic and its order are those
+// of plain_ops.cu's grad_k, lapl_at and stab1_k/stab2_k; compiled with
+// --fmad=false and IEEE division as plain_ops.cu is, a generated kernel
+// rounds exactly like the chain of operator kernels it replaces.
 #include <nvrtc.h>
 
 #include <cstring>
@@ -101,23 +100,36 @@ template <class F> __device__ __forceinline__ float cfdb_lapl(F phi, long long i
   return res;
 }
 
-// two-stage stabilisation (StabVar, src/fvm3d.cpp:909-942): upwind face
-// values phi_P + |x_f - x_P| g_d n_alt from both sides of every face
-template <class F> __device__ __forceinline__ float cfdb_stab(F phi, long long i, int mask, const CfdbGeom& g) {
+// two-stage stabilisation (StabVar, src/fvm3d.cpp:909-942).  Stage 1, per
+// cell: the upwind face values phi_P + |x_f - x_P| g_d n_alt of its six
+// faces in all three directions, into up (3 x 6n, entry d*6n + f*n + i).
+template <class F> __device__ __forceinline__ void cfdb_stab1(F phi, long long i, float* up, const CfdbGeom& g) {
   const long long n = g.n;
   const float crr = phi(i);
+  float gr[3];
+  for (int d = 0; d < 3; ++d) gr[d] = cfdb_grad_component(phi, i, d, g);
+  for (int d = 0; d < 3; ++d)
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+      const long long k6 = f * n + i;
+      const long long kd = d * 6 * n + k6;
+      up[kd] = crr + g.len[k6] * gr[d] * g.normal_alt[kd];
+    }
+}
+// Stage 2: half the jump of the two face values across each face, summed
+// over the faces (each cell's face f meets its neighbour's face f ^ 1).
+__device__ __forceinline__ float cfdb_stab2(const float* up, long long i, int mask, const CfdbGeom& g) {
+  const long long n = g.n;
   float res = 0.f;
   for (int d = 0; d < 3; ++d) {
     if (!(mask & (1 << d))) continue;
-    const float grP = cfdb_grad_component(phi, i, d, g);
+    const float* u = up + d * 6 * n;
     float acc = 0.f;
+#pragma unroll
     for (int f = 0; f < 6; ++f) {
       const long long k6 = f * n + i;
-      const long long N = g.ids[k6];
-      const long long kN = (f ^ 1) * n + N;
-      const float upP = crr + g.len[k6] * grP * g.normal_alt[d * 6 * n + k6];
-      const float upN = phi(N) + g.len[kN] * cfdb_grad_component(phi, N, d, g) * g.normal_alt[d * 6 * n + kN];
-      const float s = 0.5f * (upP - upN);
+      const float col = u[(f ^ 1) * n + g.ids[k6]];
+      const float s = 0.5f * (u[k6] - col);
       const float t = s * g.normal[d * 6 * n + k6];
       acc = acc + t * g.area[k6];
     }

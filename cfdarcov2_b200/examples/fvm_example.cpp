@@ -10,6 +10,10 @@
 //                                                 then d1t(r) = -d1dz(q) - r (operator tree)
 //   fvm_example <mode>_nojit ...                  the same with use_jit = false: operator by operator
 //                                                 instead of one generated kernel per equation
+//   fvm_example euler3d  out.bin nx ny nz steps   the reference's 20-equation Euler system (main_3d.cpp)
+//   fvm_example ref_heat out.bin nx ny nz steps   the reference's heat benchmark (main_3d_heat.cpp)
+//   fvm_example ref_wave out.bin nx ny nz steps   the reference's wave benchmark (main_3d_wave.cu)
+//   fvm_example <mode>_twice ...                  evaluate twice, print evaluate_us and steady_us
 //   fvm_example heat_store out.bin nx ny nz steps dir
 //                                                 heat with history kept, then the reference's output
 //                                                 calls: store_history (.vti per step), mesh.json and
@@ -25,6 +29,26 @@
 
 using namespace cfdb;
 
+// Equation(steps).evaluate timed on the wall clock around the call, as the
+// reference's examples time it (examples/main_3d.cpp: the time includes
+// building the generated kernels): evaluate_us.  With `twice` a second call
+// follows (kernels already built, the state advanced further): steady_us.
+static int timed_evaluate(size_t steps, std::vector<Variable*>& vars, EquationTemplate& eqs, DT& dt, bool twice,
+                          int* fused = nullptr) {
+  auto run = [&](int* jitted) {
+    const auto t0 = std::chrono::steady_clock::now();
+    Equation eq(steps);
+    eq.evaluate(vars, eqs, &dt, false);
+    if (jitted) *jitted = eq.jit_equations;
+    if (fused) *fused = eq.fused_equations;
+    return std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count();
+  };
+  int jitted = 0;
+  std::printf("evaluate_us=%.0f\n", run(&jitted));
+  if (twice) std::printf("steady_us=%.0f\n", run(nullptr));
+  return jitted;
+}
+
 static HostVec gaussian(Mesh3D& m, float cx, float cy, float cz, float sigma) {
   HostVec v(m._num_nodes);
   for (size_t i = 0; i < m._num_nodes; ++i) {
@@ -39,10 +63,17 @@ int main(int argc, char** argv) {
     std::fprintf(stderr, "usage: %s mode out.bin nx ny nz steps\n", argv[0]);
     return 2;
   }
+  // "<mode>_twice": evaluate twice (second timing without kernel builds);
   // "<mode>_nojit": the same equations with use_jit = false (operator-by-operator path)
   std::string mode = argv[1];
-  const bool jit = mode.size() < 6 || mode.compare(mode.size() - 6, 6, "_nojit") != 0;
-  if (!jit) mode.resize(mode.size() - 6);
+  auto suffix = [&](const char* s) {
+    const size_t k = std::strlen(s);
+    if (mode.size() <= k || mode.compare(mode.size() - k, k, s) != 0) return false;
+    mode.resize(mode.size() - k);
+    return true;
+  };
+  const bool twice = suffix("_twice");
+  const bool jit = !suffix("_nojit");
   const char* out = argv[2];
   const size_t nx = std::strtoul(argv[3], nullptr, 10), ny = std::strtoul(argv[4], nullptr, 10),
                nz = std::strtoul(argv[5], nullptr, 10);
@@ -107,6 +138,115 @@ int main(int argc, char** argv) {
       jitted = eq.jit_equations;
       result.push_back(q.host());
       result.push_back(r.host());
+    } else if (mode == "euler3d") {
+      // The reference's "euler" benchmark system (examples/main_3d.cpp): primitive
+      // and conservative variables, 15 use_jit equations (primitive recovery,
+      // a half-step predictor, conservative fluxes) and 5 operator-path
+      // updates with stab_tot dissipation; gamma 5/3, CFL time step, Dirichlet
+      // boundary layers holding the initial values.  The reference's mesh
+      // defaults: unit cells (dx = dy = dz = 1, so V = 1: the scheme adds
+      // per-volume fluxes to per-cell conservative variables), CFL 0.005
+      // (include/utils3d.hpp:35-66).
+      Mesh3D cube(nx, ny, nz, 1.f, 1.f, 1.f);
+      cube.init_basic_internals();
+      cube.compute();
+      Mesh3D& mesh = cube;  // this system runs on the unit-cell mesh
+      const size_t N = mesh._num_nodes;
+      HostVec r0(N), u0(N), v0(N), w0(N, 0.6f), p0(N, 2.5f), vol(N, mesh._dx * mesh._dy * mesh._dz);
+      for (size_t i = 0; i < N; ++i) {
+        const float x = mesh.x(i), y = mesh.y(i), z = mesh.z(i);
+        const bool jet = 0.4f * mesh._lx < x && x < 0.6f * mesh._lx && 0.4f * mesh._ly < y && y < 0.6f * mesh._ly;
+        r0[i] = jet ? 5.f : 1.f;
+        const int band = int(z / (0.1f * mesh._lz));  // alternating shear bands in z
+        u0[i] = v0[i] = (band % 2 == 0) ? -0.1f : 0.1f;
+      }
+      const float gamma = 5.f / 3.f;
+      HostVec m0(N), mu0(N), mv0(N), mw0(N), e0(N);
+      for (size_t i = 0; i < N; ++i) {
+        m0[i] = r0[i] * vol[i];
+        mu0[i] = r0[i] * u0[i] * vol[i];
+        mv0[i] = r0[i] * v0[i] * vol[i];
+        mw0[i] = r0[i] * w0[i] * vol[i];
+        e0[i] = (p0[i] / (gamma - 1) + 0.5f * r0[i] * (u0[i] * u0[i] + v0[i] * v0[i] + w0[i] * w0[i])) * vol[i];
+      }
+      auto fixed = [&](HostVec& init, const char* name) {
+        return Variable(&mesh, init, boundary_none, boundary_copy_cu(&mesh, init), name);
+      };
+      Variable rho = fixed(r0, "rho"), u = fixed(u0, "u"), v = fixed(v0, "v"), w = fixed(w0, "w"), p = fixed(p0, "p");
+      Variable mass = fixed(m0, "mass"), rho_u = fixed(mu0, "rho_u"), rho_v = fixed(mv0, "rho_v"),
+               rho_w = fixed(mw0, "rho_w"), rho_e = fixed(e0, "rho_e");
+      Variable mass_tmp(&mesh, m0, boundary_none, "mass_tmp"), rho_u_tmp(&mesh, mu0, boundary_none, "rho_u_tmp"),
+          rho_v_tmp(&mesh, mv0, boundary_none, "rho_v_tmp"), rho_w_tmp(&mesh, mw0, boundary_none, "rho_w_tmp"),
+          rho_e_tmp(&mesh, e0, boundary_none, "rho_e_tmp"), volumes(&mesh, vol, boundary_none, "volumes");
+      Variable E = p / (gamma - 1) + 0.5f * rho * ((u * u) + (v * v) + (w * w));
+      std::vector<Variable*> space_vars{&u, &v, &w, &p, &rho};
+      DT dt(&mesh, UpdatePolicies::CourantFriedrichsLewy3D, 0.005f, space_vars);
+      const float dissip = 2.f;
+      EquationTemplate eqs = {
+          {&rho, '=', mass / volumes, jit},
+          {&u, '=', rho_u / rho / volumes, jit},
+          {&v, '=', rho_v / rho / volumes, jit},
+          {&w, '=', rho_w / rho / volumes, jit},
+          {&p, '=', (rho_e / volumes - 0.5f * rho * (u * u + v * v + w * w)) * (gamma - 1), jit},
+          {&rho, '=', rho - 0.5f * dt * (u * d1dx(rho) + rho * d1dx(u) + v * d1dy(rho) + rho * d1dy(v) +
+                                         w * d1dz(rho) + rho * d1dz(w)), jit},
+          {&u, '=', u - 0.5f * dt * (u * d1dx(u) + v * d1dy(u) + w * d1dz(u) + (1.f / rho) * d1dx(p)), jit},
+          {&v, '=', v - 0.5f * dt * (u * d1dx(v) + v * d1dy(v) + w * d1dz(v) + (1.f / rho) * d1dy(p)), jit},
+          {&w, '=', w - 0.5f * dt * (u * d1dx(w) + v * d1dy(w) + w * d1dz(w) + (1.f / rho) * d1dz(p)), jit},
+          {&p, '=', p - 0.5f * dt * (gamma * p * (d1dx(u) + d1dy(v) + d1dz(w)) + u * d1dx(p) + v * d1dy(p) +
+                                     w * d1dz(p)), jit},
+          {&mass_tmp, '=', 0.f * mass_tmp - (d1dx(rho * u) + d1dy(rho * v) + d1dz(rho * w)), jit},
+          {&rho_u_tmp, '=', 0.f * rho_u_tmp - (d1dx(rho * u * u + p) + d1dy(rho * v * u) + d1dz(rho * w * u)), jit},
+          {&rho_v_tmp, '=', 0.f * rho_v_tmp - (d1dx(rho * v * u) + d1dy(rho * v * v + p) + d1dz(rho * v * w)), jit},
+          {&rho_w_tmp, '=', 0.f * rho_w_tmp - (d1dx(rho * w * u) + d1dy(rho * w * v) + d1dz(rho * w * w + p)), jit},
+          {&rho_e_tmp, '=', 0.f * rho_e_tmp - (d1dx((E + p) * u) + d1dy((E + p) * v) + d1dz((E + p) * w)), jit},
+          {d1t(mass), '=', mass_tmp - stab_tot(rho) * dissip, false},
+          {d1t(rho_u), '=', rho_u_tmp - stab_tot(rho * u) * dissip, false},
+          {d1t(rho_v), '=', rho_v_tmp - stab_tot(rho * v) * dissip, false},
+          {d1t(rho_w), '=', rho_w_tmp - stab_tot(rho * w) * dissip, false},
+          {d1t(rho_e), '=', rho_e_tmp - stab_tot(E) * dissip, false},
+      };
+      std::vector<Variable*> all_vars{&rho, &u, &v, &w, &p, &mass, &rho_u, &rho_v, &rho_w, &rho_e};
+      jitted = timed_evaluate(steps, all_vars, eqs, dt, twice);
+      for (Variable* x : {&rho, &u, &v, &w, &p}) result.push_back(x->host());
+    } else if (mode == "ref_heat") {
+      // the reference's heat benchmark (examples/main_3d_heat.cpp): unit cells, T = 100
+      // in the two lowest z layers, boundary copy, dt 0.005, d1t(T) = 3 lapl(T)
+      Mesh3D cube(nx, ny, nz, 1.f, 1.f, 1.f);
+      cube.init_basic_internals();
+      cube.compute();
+      HostVec T0(cube._num_nodes);
+      for (size_t i = 0; i < cube._num_nodes; ++i) T0[i] = cube.z(i) < 2.f * cube._dz ? 100.f : 0.f;
+      Variable T(&cube, T0, boundary_none, boundary_copy_cu(&cube, T0), "T");
+      std::vector<Variable*> vars{&T};
+      DT dt(&cube, UpdatePolicies::constant_dt, 0.005f, vars);
+      EquationTemplate eqs = {{d1t(T), '=', 3.0f * lapl(T), jit}};
+      jitted = timed_evaluate(steps, vars, eqs, dt, twice, &fused);
+      result.push_back(T.host());
+    } else if (mode == "ref_wave") {
+      // the reference's wave benchmark (examples/main_3d_wave.cu): unit cells, u = 0,
+      // sin(0.2 t) driven at the cells (0.1, 0.1, 0.1) and (0.9, 0.9, 0.9) of the box,
+      // dt 0.1, c 0.3, d2t(u) = c^2 (d2dx(u) + d2dy(u)); the driver is applied on the
+      // device (the reference's boundary_sine_cu) instead of through host memory
+      Mesh3D cube(nx, ny, nz, 1.f, 1.f, 1.f);
+      cube.init_basic_internals();
+      cube.compute();
+      HostVec U0(cube._num_nodes, 0.f);
+      const size_t n1 = cube.square_node_coord_to_idx(size_t(nx * 0.1), size_t(ny * 0.1), size_t(nz * 0.1));
+      const size_t n2 = cube.square_node_coord_to_idx(size_t(nx * 0.9), size_t(ny * 0.9), size_t(nz * 0.9));
+      BoundaryFNCU sine = [n1, n2](Mesh3D*, float* field, const DT* d) {
+        // sin of float(step) * 0.2 in double, stored as float (main_3d_wave.cu:33-42)
+        const float s = float(std::sin(double(float(d->_current_time_step_int)) * 0.2));
+        check(cfdb_op_fill(CFDArcoGlobalInit::ctx(), CFDB_F32, field + n1, s, 1), "cfdb_op_fill");
+        check(cfdb_op_fill(CFDArcoGlobalInit::ctx(), CFDB_F32, field + n2, s, 1), "cfdb_op_fill");
+      };
+      Variable u(&cube, U0, boundary_none, sine, "u");
+      std::vector<Variable*> vars{&u};
+      DT dt(&cube, UpdatePolicies::constant_dt, 0.1f, vars);
+      const float c = 0.3f;
+      EquationTemplate eqs = {{d2t(u), '=', c * c * (d2dx(u) + d2dy(u)), jit}};
+      jitted = timed_evaluate(steps, vars, eqs, dt, twice);
+      result.push_back(u.host());
     } else {
       std::fprintf(stderr, "unknown mode %s\n", mode.c_str());
       return 2;

@@ -88,6 +88,20 @@ def test_jit_equations_equal_operator_path_bitwise(tmp_path, mode, nfields, n):
     assert np.array_equal(J, P)
 
 
+@pytest.mark.parametrize("n", [16, 13])
+def test_reference_euler_system_jit_equals_operator_path(tmp_path, n):
+    """The reference's 3-D Euler benchmark system (examples/main_3d.cpp: 15
+    use_jit equations incl. d1dx of products, 5 operator-path updates with
+    stab_tot, CFL time step, Dirichlet boundary layers): the generated
+    kernels give the operator path's bits; the state stays finite."""
+    steps = 6
+    J, out_j = run_example(tmp_path, "euler3d", n, n, n, steps, 5)
+    P, out_p = run_example(tmp_path, "euler3d_nojit", n, n, n, steps, 5)
+    assert "jit_equations=15" in out_j and "jit_equations=0" in out_p
+    assert np.isfinite(J).all()
+    assert np.array_equal(J, P)
+
+
 def test_jit_heat_on_a_mesh_the_sweep_cannot_take(oracle, tmp_path):
     """The heat template on nz % 4 != 0 cannot use the fused TMA step; with
     use_jit it runs as a generated kernel and matches the oracle."""
@@ -98,6 +112,47 @@ def test_jit_heat_on_a_mesh_the_sweep_cannot_take(oracle, tmp_path):
     T0 = gaussian(m, (0.5, 0.5, 0.5), 0.1)
     dt = float(np.float32(0.1 * (1 / n) ** 2 / 0.01))
     assert rel_l2(T, m.heat_solve(T0, 0.01, dt, steps)) <= 1e-5
+
+
+def test_reference_heat_benchmark_row(oracle, tmp_path):
+    """examples/main_3d_heat.cpp as its benchmark runs it: unit cells, T = 100
+    in the two lowest z layers, d1t(T) = 3 lapl(T), dt 0.005, the boundary
+    cells copied back from T0 after every step (fused step + device copy)."""
+    n, steps = 12, 25
+    (T,), out = run_example(tmp_path, "ref_heat", n, n, n, steps)
+    assert "fused_equations=1" in out and "evaluate_us=" in out
+    m = oracle.Mesh(n, n, n, 1.0, 1.0, 1.0)
+    z = m.geometry()["center"].reshape(3, -1)[2].astype(np.float32)
+    T0 = np.where(z < 2.0, 100.0, 0.0)
+    isb = m.geometry()["is_boundary"] > 0
+    ref = T0.copy()
+    for _ in range(steps):
+        ref = m.heat_solve(ref, 3.0, float(np.float32(0.005)), 1)
+        ref[isb] = T0[isb]
+    assert rel_l2(T, ref) <= 1e-5
+
+
+def test_reference_wave_benchmark_row(oracle, tmp_path):
+    """examples/main_3d_wave.cu as its benchmark runs it: u = 0, d2t(u) =
+    c^2 (d2dx(u) + d2dy(u)) with c 0.3 and dt 0.1, and after every step the
+    cells at 0.1 and 0.9 of the box set to sin(0.2 step) (step counted from
+    1, computed in double and stored as float)."""
+    n, steps = 10, 30
+    (U,), out = run_example(tmp_path, "ref_wave", n, n, n, steps)
+    assert "jit_equations=1" in out
+    m = oracle.Mesh(n, n, n, 1.0, 1.0, 1.0)
+    n1 = n * n * int(n * 0.1) + n * int(n * 0.1) + int(n * 0.1)
+    n2 = n * n * int(n * 0.9) + n * int(n * 0.9) + int(n * 0.9)
+    u = np.zeros(n ** 3)
+    prev = None
+    dt, c = float(np.float32(0.1)), float(np.float32(0.3))
+    for t in range(1, steps + 1):
+        R = c * c * (m.lapl(u, 1) + m.lapl(u, 2))
+        nxt = dt * R + u if prev is None else (dt * dt * R + 2 * u) - prev
+        prev, u = u, nxt
+        u[[n1, n2]] = float(np.float32(np.sin(float(np.float32(t)) * 0.2)))
+    assert np.abs(U).max() > 0.1
+    assert rel_l2(U, u) <= 1e-5
 
 
 def test_store_history_files(oracle, tmp_path):
