@@ -566,34 +566,50 @@ REFERENCE_ROWS = [
 
 
 def run_reference_rows(args):
-    """One JSON line per reference benchmark row: value = cells x 200 steps /
-    the wall time of the first Equation::evaluate (kernel builds included,
-    as the reference times it); steady = the same for a second evaluate."""
+    """One JSON line per reference benchmark row.  As the reference's script
+    does, each row runs as 3 separate processes and the best is kept: value =
+    cells x 200 steps / the wall time of Equation::evaluate (kernel builds
+    included).  The kernel cache starts empty, so the first process compiles
+    and the later ones load the cached kernels, as OCCA's cache behaves for
+    the reference; cold = that first process.  steady = a second evaluate in
+    the same process (nothing left to build)."""
     import subprocess
+    import tempfile
     exe = os.path.join(ROOT, "cfdarcov2_b200", "_lib", "fvm_example")
     if not os.path.exists(exe):
         raise SystemExit("fvm_example is not built; run `python -m cfdarcov2_b200.build`")
-    steps = 200
+    steps, repeats = 200, 3
+    cache = tempfile.mkdtemp(prefix="cfdb_kernel_cache_")
+    env = dict(os.environ, CFDB_KERNEL_CACHE=cache)
     for name, mode, n, published, what in REFERENCE_ROWS:
-        r = subprocess.run([exe, mode + "_twice", os.devnull, str(n), str(n), str(n), str(steps)],
-                           capture_output=True, text=True, timeout=900)
-        if r.returncode != 0:
-            raise SystemExit(f"{mode}: exit {r.returncode}: {r.stderr[-2000:]}")
-        kv = dict(tok.split("=", 1) for line in r.stdout.splitlines() for tok in line.split() if "=" in tok)
-        first_us, steady_us = float(kv["evaluate_us"]), float(kv["steady_us"])
         cells = n ** 3 * steps
-        value = cells / (first_us * 1e-6) / 1e6
+        runs = []
+        for _ in range(repeats):
+            r = subprocess.run([exe, mode + "_twice", os.devnull, str(n), str(n), str(n), str(steps)],
+                               capture_output=True, text=True, timeout=900, env=env)
+            if r.returncode != 0:
+                raise SystemExit(f"{mode}: exit {r.returncode}: {r.stderr[-2000:]}")
+            kv = dict(tok.split("=", 1) for line in r.stdout.splitlines() for tok in line.split() if "=" in tok)
+            runs.append(kv)
+        first = [float(kv["evaluate_us"]) for kv in runs]
+        steady = [float(kv["steady_us"]) for kv in runs]
+        best_us = min(first)
+        value = cells / (best_us * 1e-6) / 1e6
         print(json.dumps({
             "metric": "Mcell-updates/s (reference benchmark row, wall time of Equation::evaluate)",
-            "value": value, "unit": "Mcell-updates/s", "n_gpus": 1, "steps": 1, "warmup": 0,
-            "ms_per_step": first_us / 1e3 / steps, "higher_is_better": True, "scaling": "weak",
+            "value": value, "unit": "Mcell-updates/s", "n_gpus": 1, "steps": repeats, "warmup": 0,
+            "ms_per_step": best_us / 1e3 / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": value / published, "baseline_published": published, "baseline_hardware": "A100",
             "dtype": "f32", "data": "synthetic (the reference example's initial state)",
             "config": {"workload": f"reference_{name}_{n}^3_x{steps}_steps", "system": what,
-                       "path": "C++ facade (include/cfdb/fvm3d.hpp), use_jit equations"},
-            "steady": {"value": cells / (steady_us * 1e-6) / 1e6, "unit": "Mcell-updates/s",
-                       "note": "second evaluate on the same variables: no kernel builds"},
-            "facade_counts": {k: int(kv[k]) for k in ("jit_equations", "fused_equations") if k in kv},
+                       "path": "C++ facade (include/cfdb/fvm3d.hpp), use_jit equations",
+                       "protocol": "best of 3 processes, as scripts/benchmark_cfdarchov2.py"},
+            "cold": {"value": cells / (first[0] * 1e-6) / 1e6, "unit": "Mcell-updates/s",
+                     "note": "first process: empty kernel cache, every generated kernel compiled"},
+            "steady": {"value": cells / (min(steady) * 1e-6) / 1e6, "unit": "Mcell-updates/s",
+                       "note": "second evaluate in the same process: no kernel builds"},
+            "facade_counts": {k: int(runs[0][k]) for k in ("jit_equations", "fused_equations", "lattice_equations")
+                              if k in runs[0]},
         }), flush=True)
 
 

@@ -143,6 +143,11 @@ class Context:
         call("cfdb_op_boundary_copy", self.h, mesh.h, _dtype_code(arr), _ptr(arr), _ptr(copy), _ptr(out), ctx=self.h)
         return out
 
+    def boundary_set(self, mesh, field, values):
+        """field[i] = values[i] on the boundary cells, in place."""
+        call("cfdb_op_boundary_set", self.h, mesh.h, _dtype_code(field), _ptr(field), _ptr(values), ctx=self.h)
+        return field
+
     def cfl_dt(self, mesh, cfl, gamma, p, rho, u, v=None, w=None) -> float:
         out = C.c_double()
         call("cfdb_cfl_dt", self.h, mesh.h, _dtype_code(p), float(cfl), float(gamma), _ptr(p), _ptr(rho), _ptr(u),
@@ -231,6 +236,29 @@ class Mesh:
         call("cfdb_mesh_geometry", self.h, int(which), out.ctypes.data_as(C.c_void_p),
              ctx=self.ctx.h if self.ctx else None)
         return out
+
+    def plain_geometry(self) -> dict:
+        """The FP32 face arrays the plain and generated kernels read, copied
+        back from the device: ids (int32), normal, normal_alt (3 x 6n),
+        area, alpha, len (6n), volume (n)."""
+        g = capi.PlainGeometry()
+        call("cfdb_mesh_plain_geometry", self.h, C.byref(g), ctx=self.ctx.h)
+        sizes = {"ids": 6, "normal": 18, "normal_alt": 18, "area": 6, "alpha": 6, "len": 6, "volume": 1}
+        out = {}
+        for name, k in sizes.items():
+            a = np.empty(k * self.n, np.int32 if name == "ids" else np.float32)
+            call("cfdb_download", self.ctx.h, a.ctypes.data_as(C.c_void_p), C.c_void_p(getattr(g, name)),
+                 a.nbytes, ctx=self.ctx.h)
+            out[name] = a
+        return out
+
+    def lattice_geometry(self):
+        """cfdb_mesh_lattice_geometry: (exact, constants dict)."""
+        g = capi.LatticeGeometry()
+        call("cfdb_mesh_lattice_geometry", self.h, C.byref(g), ctx=self.ctx.h)
+        consts = {k: np.array(getattr(g, k), np.float32) for k in ("normal", "normal_alt", "area", "alpha", "len")}
+        consts["volume"] = np.float32(g.volume)
+        return bool(g.exact), consts
 
     def ids(self):
         ids = np.empty(6 * self.n, np.int64)

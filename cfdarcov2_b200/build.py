@@ -27,7 +27,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 # Sources whose arithmetic must round every operation separately (the FP64
 # plain path is compared bit for bit with the CPU oracle).
-NO_FMA = {"plain_ops.cu", "euler_plain.cu"}
+NO_FMA = {"plain_ops.cu", "euler_plain.cu", "geometry_dev.cu"}
 
 
 def host_cxx() -> str:

@@ -47,6 +47,19 @@ class GradientStats(C.Structure):
                 ("reserved", C.c_int32), ("forward_ms", C.c_double), ("reverse_ms", C.c_double)]
 
 
+class PlainGeometry(C.Structure):
+    """cfdb_plain_geometry: device pointers of a mesh's FP32 face arrays."""
+    _fields_ = [("ids", C.c_void_p), ("normal", C.c_void_p), ("normal_alt", C.c_void_p), ("area", C.c_void_p),
+                ("alpha", C.c_void_p), ("len", C.c_void_p), ("volume", C.c_void_p), ("n", C.c_int64)]
+
+
+class LatticeGeometry(C.Structure):
+    """cfdb_lattice_geometry: per-slot FP32 constants of an exact lattice."""
+    _fields_ = [("nx", C.c_int64), ("ny", C.c_int64), ("nz", C.c_int64), ("exact", C.c_int32),
+                ("reserved", C.c_int32), ("normal", C.c_float * 18), ("normal_alt", C.c_float * 18),
+                ("area", C.c_float * 6), ("alpha", C.c_float * 12), ("len", C.c_float * 12), ("volume", C.c_float)]
+
+
 # name -> (restype, argtypes)
 PROTOTYPES = {
     "cfdb_abi_version": (_I, []),
@@ -60,9 +73,11 @@ PROTOTYPES = {
     "cfdb_ctx_trim": (_I, [_P]),
     "cfdb_ctx_launch_count": (_I, [_P, _PI64]),
     "cfdb_kernel_build": (_I, [_P, C.c_char_p, C.c_char_p, _PP]),
+    "cfdb_kernel_build_many": (_I, [_P, _I, C.POINTER(C.c_char_p), C.POINTER(C.c_char_p), _PP]),
     "cfdb_kernel_launch": (_I, [_P, _I64, _I, _P]),
     "cfdb_kernel_destroy": (_I, [_P]),
     "cfdb_mesh_plain_geometry": (_I, [_P, _P]),
+    "cfdb_mesh_lattice_geometry": (_I, [_P, _P]),
     "cfdb_write_vti": (_I, [C.c_char_p, C.c_char_p, _I64, _I64, _I64, _P]),
     "cfdb_write_mesh_json": (_I, [C.c_char_p, _I64, _I64, _I64, _D, _D, _D, _P]),
     "cfdb_alloc": (_I, [_P, _I64, _PP]),
@@ -85,6 +100,7 @@ PROTOTYPES = {
     "cfdb_op_d1t": (_I, [_P, _I, _P, _P, _D, _P, _I64]),
     "cfdb_op_d2t": (_I, [_P, _I, _P, _P, _P, _D, _I, _P, _I64]),
     "cfdb_op_boundary_copy": (_I, [_P, _P, _I, _P, _P, _P]),
+    "cfdb_op_boundary_set": (_I, [_P, _P, _I, _P, _P]),
     "cfdb_cfl_dt": (_I, [_P, _P, _I, _D, _D, _P, _P, _P, _P, _P, _PD]),
     "cfdb_total_fp64": (_I, [_P, _P, _I, _P, _PD]),
     "cfdb_total_fp64_noalloc": (_I, [_I, _P, _P, _D, _I64, _P, _P]),

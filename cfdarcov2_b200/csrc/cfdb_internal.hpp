@@ -130,6 +130,8 @@ struct cfdb_mesh {
   int32_t* d_ids = nullptr;
   PlainGeomDev plain[2];
   CompactGeomDev compact;
+  int lattice_state = 0;  // 0 not checked, 1 exact lattice, 2 not one
+  cfdb_lattice_geometry lattice{};
 };
 
 // ---- error plumbing --------------------------------------------------------
@@ -164,6 +166,10 @@ void cfdb_ws_free(cfdb_ctx* ctx, void* p);
 // ---- geometry helpers ------------------------------------------------------
 int cfdb_mesh_need_host_geom(cfdb_mesh* m);
 int cfdb_mesh_need_plain(cfdb_mesh* m, int dtype);
+// fills the plain arrays of dtype on the device (geometry_dev.cu)
+int cfdb_build_plain_device(cfdb_mesh* m, int dtype, PlainGeomDev& p);
+// samples and checks the lattice constants on the device (geometry_dev.cu)
+int cfdb_check_lattice_device(cfdb_mesh* m, cfdb_lattice_geometry* out);
 int cfdb_mesh_need_compact(cfdb_mesh* m);
 
 inline size_t dtype_size(int dtype) { return dtype == CFDB_F64 ? 8 : 4; }

@@ -3,6 +3,7 @@
 // expression node evaluates through a cfdb_op_* kernel into a buffer it
 // allocates once.
 #include <algorithm>
+#include <cstddef>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -34,6 +35,8 @@ cfdb_ctx* g_ctx = nullptr;
 bool CFDArcoGlobalInit::skip_history = true;
 bool CFDArcoGlobalInit::cuda_enabled = false;
 bool CFDArcoGlobalInit::store_stepping = false;
+bool CFDArcoGlobalInit::jit_lattice = true;
+bool CFDArcoGlobalInit::jit_all = true;
 std::string CFDArcoGlobalInit::store_dir;
 
 void CFDArcoGlobalInit::initialize(int, char**, bool skip_hist, const std::string& store_path) {
@@ -209,12 +212,14 @@ const float* eval_node(Node* n) {
 
 // ---- run-time generated equation kernels (KernelBuilder, src/fvm3d.cpp:1071-1394)
 // An equation becomes a short plan of generated kernels: the pointwise part
-// of the right-hand side, the operators on fields and the time update fuse
-// into the last one; an operator whose operand is an expression first
-// materialises the operand in its own pass (so no cell recomputes a
-// neighbour's expression), and a stabilisation first writes its stage-1
-// face values in a pass of their own.  Inside a kernel there is one device
-// function per expression node, e<k>(i, A) = the node's value at cell i.
+// of the right-hand side, the operators and the time update fuse into the
+// last one.  An operator whose operand is a pointwise expression of fields
+// evaluates it at the neighbours inline; an operand that holds operators
+// itself is first materialised in a pass of its own (so no cell recomputes a
+// neighbour's neighbour operators), and a stabilisation first stores the
+// operand's gradient (3 floats per cell) in a pass of its own.  Inside a
+// kernel there is one device function per expression node, e<k>(i, A) = the
+// node's value at cell i.
 // Operand order and constants are those of the operator path (a constant
 // operand as a scalar operation), and the library compiles with
 // --fmad=false, so the plan's result equals the operator chain's bit for
@@ -230,6 +235,7 @@ struct JitInput {
 
 struct JitPass {
   cfdb_kernel* k = nullptr;
+  std::string source, entry;  // compiled by jit_compile, all passes of all equations at once
   std::vector<JitInput> inputs;
   int out_scratch = -1;  // -1: the equation's output (the last pass)
   ~JitPass() {
@@ -239,10 +245,18 @@ struct JitPass {
 
 struct JitPlan {
   Mesh3D* mesh = nullptr;
+  // an exact lattice: the kernels take per-slot geometry constants instead of the face arrays
+  bool lattice = false;
+  cfdb_lattice_geometry lat{};
+  std::string geom_type() const {
+    if (!lattice) return "CfdbGeom";
+    return "CfdbLattice<" + std::to_string(lat.nx) + "LL, " + std::to_string(lat.ny) + "LL, " +
+           std::to_string(lat.nz) + "LL>";
+  }
   std::vector<std::unique_ptr<JitPass>> passes;  // run order; the last computes the equation
   std::vector<float*> scratch;
   std::map<const Node*, int> materialised;
-  std::vector<std::pair<JitInput, int>> stab_stage1;
+  std::map<const void*, int> stab_grads;  // by field, or by operand node
   bool ok = true;
   ~JitPlan() {
     for (float* p : scratch) device_free(p);
@@ -252,10 +266,11 @@ struct JitPlan {
     return int(scratch.size() - 1);
   }
   int materialise(const Node* n);
-  int stab1(const JitInput& in);
+  int stab_grad(const Node* operand);
   void add_pass(const std::string& src, const char* entry, std::vector<JitInput> inputs, int out) {
     auto p = std::make_unique<JitPass>();
-    check(cfdb_kernel_build(CFDArcoGlobalInit::ctx(), src.c_str(), entry, &p->k), "cfdb_kernel_build");
+    p->source = src;
+    p->entry = entry;
     p->inputs = std::move(inputs);
     p->out_scratch = out;
     passes.push_back(std::move(p));
@@ -284,12 +299,36 @@ struct JitGen {
     inputs.push_back(in);
     return int(inputs.size() - 1);
   }
-  // operand of a neighbour operator: a field as it is, an expression materialised by an earlier pass
-  JitInput operand(const Node* n) {
-    JitInput in;
-    if (n->kind == Node::kField) in.field = n->field;
-    else in.scratch = plan.materialise(n);
-    return in;
+  // an expression of fields, constants and dt alone (evaluated at any cell inline)
+  static bool pointwise(const Node* n, int* budget) {
+    if (--*budget < 0) return false;
+    switch (n->kind) {
+      case Node::kField:
+      case Node::kConst:
+      case Node::kDt: return true;
+      case Node::kBinary: return pointwise(n->a.get(), budget) && pointwise(n->b.get(), budget);
+      case Node::kNeg: return pointwise(n->a.get(), budget);
+      default: return false;
+    }
+  }
+  static bool inline_operand(const Node* n) {
+    int budget = 48;
+    return pointwise(n, &budget);
+  }
+  // operand of a neighbour operator as a callable of the cell index: a
+  // field's buffer, a pointwise expression evaluated inline, or the buffer an
+  // earlier pass materialised it into
+  std::string operand(const Node* n) {
+    if (n->kind == Node::kField)
+      return "[&](long long j) { return A.f[" + std::to_string(input(JitInput{n->field, -1})) + "][j]; }";
+    if (inline_operand(n)) {
+      const int k = emit(n);
+      if (k < 0) return std::string();
+      return "[&](long long j) { return e" + std::to_string(k) + "(j, A); }";
+    }
+    const int s = plan.materialise(n);
+    if (s < 0) return std::string();
+    return "[&](long long j) { return A.f[" + std::to_string(input(JitInput{nullptr, s})) + "][j]; }";
   }
   std::string call(int k) { return "e" + std::to_string(k) + "(i, A)"; }
   int emit(const Node* n) {
@@ -320,19 +359,19 @@ struct JitGen {
       }
       case Node::kGrad:
       case Node::kLapl: {
-        const JitInput src = operand(n->a.get());
-        if (!plan.ok) return -1;
-        const std::string f = "A.f[" + std::to_string(input(src)) + "]";
-        body = std::string(n->kind == Node::kGrad ? "cfdb_grad" : "cfdb_lapl") + "([&](long long j) { return " + f +
-               "[j]; }, i, " + std::to_string(n->mask) + ", A.g)";
+        const std::string phi = operand(n->a.get());
+        if (!plan.ok || phi.empty()) return -1;
+        body = std::string(n->kind == Node::kGrad ? "cfdb_grad" : "cfdb_lapl") + "(" + phi + ", i, " +
+               std::to_string(n->mask) + ", A.g)";
         break;
       }
       case Node::kStab: {
-        const JitInput src = operand(n->a.get());
-        if (!plan.ok) return -1;
-        const int up = plan.stab1(src);
-        body = "cfdb_stab2(A.f[" + std::to_string(input(JitInput{nullptr, up})) + "], i, " + std::to_string(n->mask) +
-               ", A.g)";
+        const int gr = plan.stab_grad(n->a.get());
+        if (!plan.ok || gr < 0) return -1;
+        const std::string phi = operand(n->a.get());
+        if (!plan.ok || phi.empty()) return -1;
+        body = "cfdb_stab2g(" + phi + ", A.f[" + std::to_string(input(JitInput{nullptr, gr})) + "], i, " +
+               std::to_string(n->mask) + ", A.g)";
         break;
       }
       default:
@@ -347,7 +386,7 @@ struct JitGen {
   }
   std::string prelude() const {
     return "#include \"cfdb_jit.cuh\"\nstruct CfdbArgs { const float* f[" +
-           std::to_string(std::max<size_t>(1, inputs.size())) + "]; float dt; CfdbGeom g; };\n";
+           std::to_string(std::max<size_t>(1, inputs.size())) + "]; float dt; " + plan.geom_type() + " g; };\n";
   }
   // every generated kernel has the signature (A, out, cur, prev, mode, n)
   std::string equation_source(int root) const {
@@ -379,25 +418,38 @@ int JitPlan::materialise(const Node* n) {
   return s;
 }
 
-int JitPlan::stab1(const JitInput& in) {
-  for (auto& kv : stab_stage1)
-    if (kv.first == in) return kv.second;
-  const int s = new_scratch(18 * mesh->_num_nodes);
-  const std::string src = "#include \"cfdb_jit.cuh\"\nstruct CfdbArgs { const float* f[1]; float dt; CfdbGeom g; };\n"
-                          "extern \"C\" __global__ void cfdb_stab_stage1(CfdbArgs A, float* __restrict__ up, const float*,\n"
+// Stage 1 of a stabilisation: the operand's three gradient components per
+// cell, one pass per distinct operand (a field, or an operand node).
+int JitPlan::stab_grad(const Node* operand) {
+  const void* key = operand->kind == Node::kField ? static_cast<const void*>(operand->field) : operand;
+  auto it = stab_grads.find(key);
+  if (it != stab_grads.end()) return it->second;
+  JitGen g(*this);
+  const std::string phi = g.operand(operand);
+  if (!ok || phi.empty()) {
+    ok = false;
+    return -1;
+  }
+  const int s = new_scratch(3 * mesh->_num_nodes);
+  const std::string src = g.prelude() + g.funcs +
+                          "extern \"C\" __global__ void cfdb_stab_stage1(CfdbArgs A, float* __restrict__ gr, const float*,\n"
                           "                                           const float*, int, long long n) {\n"
                           "  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;\n"
                           "  if (i >= n) return;\n"
-                          "  cfdb_stab1([&](long long j) { return A.f[0][j]; }, i, up, A.g);\n"
+                          "  cfdb_stab_grad(" + phi + ", i, gr, A.g);\n"
                           "}\n";
-  add_pass(src, "cfdb_stab_stage1", {in}, s);
-  stab_stage1.emplace_back(in, s);
+  add_pass(src, "cfdb_stab_stage1", g.inputs, s);
+  stab_grads[key] = s;
   return s;
 }
 
 std::unique_ptr<JitPlan> jit_build(const Node* rhs, Mesh3D* mesh) {
   auto plan = std::make_unique<JitPlan>();
   plan->mesh = mesh;
+  if (CFDArcoGlobalInit::jit_lattice) {
+    check(cfdb_mesh_lattice_geometry(mesh->handle(), &plan->lat), "cfdb_mesh_lattice_geometry");
+    plan->lattice = plan->lat.exact != 0;
+  }
   JitGen g(*plan);
   const int root = g.emit(rhs);
   if (!plan->ok || root < 0) return nullptr;
@@ -405,30 +457,68 @@ std::unique_ptr<JitPlan> jit_build(const Node* rhs, Mesh3D* mesh) {
   return plan;
 }
 
+// KernelBuilder::build for every plan of an equation system in one call: the
+// library compiles the sources on several host threads (or loads them from
+// its on-disk kernel cache).
+void jit_compile(const std::vector<std::unique_ptr<JitPlan>>& plans) {
+  std::vector<JitPass*> passes;
+  for (const auto& plan : plans)
+    if (plan)
+      for (const auto& p : plan->passes)
+        if (!p->k) passes.push_back(p.get());
+  if (passes.empty()) return;
+  std::vector<const char*> srcs, names;
+  for (JitPass* p : passes) {
+    srcs.push_back(p->source.c_str());
+    names.push_back(p->entry.c_str());
+  }
+  std::vector<cfdb_kernel*> ks(passes.size(), nullptr);
+  check(cfdb_kernel_build_many(CFDArcoGlobalInit::ctx(), int(passes.size()), srcs.data(), names.data(), ks.data()),
+        "cfdb_kernel_build_many");
+  for (size_t k = 0; k < passes.size(); ++k) passes[k]->k = ks[k];
+}
+
 // KernelBuilder::run: the plan's passes in order; the last one writes the
 // equation's update (mode 0: value, 1: d1t, 2: d2t) into `out`.
 void jit_run(const JitPlan& plan, float dt, float* out, const float* cur, const float* prev, int mode) {
-  cfdb_plain_geometry g{};
-  check(cfdb_mesh_plain_geometry(plan.mesh->handle(), &g), "cfdb_mesh_plain_geometry");
+  // CfdbArgs { const float* f[nf]; float dt; G g; } laid out as the device
+  // compiler does: G = CfdbGeom (pointers, 8-byte aligned) or CfdbLattice
+  // (67 floats: the constants of cfdb_lattice_geometry from normal on)
   struct Geom {
     const int32_t* ids;
     const float *normal, *normal_alt, *area, *alpha, *len, *volume;
     long long n;
-  } geom{g.ids, g.normal, g.normal_alt, g.area, g.alpha, g.len, g.volume, (long long)g.n};
+  } geom{};
+  const unsigned char* gsrc;
+  size_t gsize, galign;
+  if (plan.lattice) {
+    gsrc = reinterpret_cast<const unsigned char*>(plan.lat.normal);
+    gsize = sizeof(float) * 67;
+    galign = alignof(float);
+    static_assert(offsetof(cfdb_lattice_geometry, volume) - offsetof(cfdb_lattice_geometry, normal) ==
+                      sizeof(float) * 66,
+                  "lattice constants are contiguous");
+  } else {
+    cfdb_plain_geometry g{};
+    check(cfdb_mesh_plain_geometry(plan.mesh->handle(), &g), "cfdb_mesh_plain_geometry");
+    geom = Geom{g.ids, g.normal, g.normal_alt, g.area, g.alpha, g.len, g.volume, (long long)g.n};
+    gsrc = reinterpret_cast<const unsigned char*>(&geom);
+    gsize = sizeof(geom);
+    galign = alignof(Geom);
+  }
   long long n = (long long)plan.mesh->_num_nodes;
   for (const auto& p : plan.passes) {
-    // CfdbArgs { const float* f[nf]; float dt; CfdbGeom g; } laid out as the device compiler does
     const size_t nf = std::max<size_t>(1, p->inputs.size());
     const size_t off_dt = nf * sizeof(void*);
-    const size_t off_g = (off_dt + sizeof(float) + 7) / 8 * 8;
-    std::vector<unsigned char> A(off_g + sizeof(Geom), 0);
+    const size_t off_g = (off_dt + sizeof(float) + galign - 1) / galign * galign;
+    std::vector<unsigned char> A(off_g + gsize, 0);
     for (size_t k = 0; k < p->inputs.size(); ++k) {
       const JitInput& in = p->inputs[k];
       const float* ptr = in.field ? in.field->current_cu : plan.scratch[size_t(in.scratch)];
       std::memcpy(&A[k * sizeof(void*)], &ptr, sizeof(ptr));
     }
     std::memcpy(&A[off_dt], &dt, sizeof(dt));
-    std::memcpy(&A[off_g], &geom, sizeof(geom));
+    std::memcpy(&A[off_g], gsrc, gsize);
     float* o = p->out_scratch >= 0 ? plan.scratch[size_t(p->out_scratch)] : out;
     int m = p->out_scratch >= 0 ? 0 : mode;
     void* args[] = {A.data(), &o, &cur, &prev, &m, &n};
@@ -580,9 +670,11 @@ BoundaryFNCU boundary_copy_cu(Mesh3D* mesh, const HostVec& values) {
   auto buf = std::shared_ptr<float>(device_alloc(values.size()), [](float* p) { device_free(p); });
   check(cfdb_upload(CFDArcoGlobalInit::ctx(), buf.get(), values.data(), int64_t(values.size() * sizeof(float))),
         "cfdb_upload");
+  // in place over the boundary cells only (the reference's blend
+  // arr * (1 - b) + copy * b leaves the interior as it is for finite states)
   return [buf](Mesh3D* m, float* field, const DT*) {
-    check(cfdb_op_boundary_copy(CFDArcoGlobalInit::ctx(), m->handle(), CFDB_F32, field, buf.get(), field),
-          "cfdb_op_boundary_copy");
+    check(cfdb_op_boundary_set(CFDArcoGlobalInit::ctx(), m->handle(), CFDB_F32, field, buf.get()),
+          "cfdb_op_boundary_set");
   };
 }
 
@@ -629,13 +721,15 @@ void Equation::evaluate(std::vector<Variable*>& all_vars, EquationTemplate& eqs,
   cfdb_ctx* ctx = CFDArcoGlobalInit::ctx();
   fused_equations = 0;
   jit_equations = 0;
-  // use_jit equations (tuple element 3) that are not the fused heat
-  // template become a plan of generated kernels each, built before the first step
+  lattice_equations = 0;
+  // use_jit equations (tuple element 3), and with jit_all the others too,
+  // that are not the fused heat template become a plan of generated kernels
+  // each, all compiled before the first step
   std::vector<std::unique_ptr<JitPlan>> jit(eqs.size());
   for (size_t e = 0; e < eqs.size(); ++e) {
     Variable* lhs = std::get<0>(eqs[e]);
     const Node* rhs = std::get<2>(eqs[e]).node.get();
-    if (!std::get<3>(eqs[e]) || !rhs) continue;
+    if (!rhs || (!std::get<3>(eqs[e]) && !CFDArcoGlobalInit::jit_all)) continue;
     float k = 0.f;
     auto* d = dynamic_cast<DtVar*>(lhs);
     auto* d2 = dynamic_cast<D2tVar*>(lhs);
@@ -643,8 +737,12 @@ void Equation::evaluate(std::vector<Variable*>& all_vars, EquationTemplate& eqs,
     if (!mesh) continue;
     if (d && match_heat(rhs, d->var, &k) && stencil_fusable(d->var->mesh)) continue;
     jit[e] = jit_build(rhs, mesh);
-    if (jit[e]) ++jit_equations;
+    if (jit[e]) {
+      ++jit_equations;
+      if (jit[e]->lattice) ++lattice_equations;
+    }
   }
+  jit_compile(jit);
   for (size_t t = 0; t < timesteps; ++t) {
     dt->update();
     const float dtv = dt->_dt;

@@ -208,6 +208,29 @@ template <class R> __global__ void bcopy_k(const R* __restrict__ arr, const R* _
   }
 }
 
+// the cells of the box surface: the two x planes (all y, z), the two y planes
+// and the two z planes; cells on edges and corners come up more than once and
+// are written with the same value each time
+template <class R>
+__global__ void bset_k(R* __restrict__ field, const R* __restrict__ values, int64_t nx, int64_t ny, int64_t nz) {
+  const int64_t px = ny * nz, py = nx * nz, pz = nx * ny, total = 2 * (px + py + pz);
+  GRID_STRIDE(t, total) {
+    int64_t x, y, z;
+    if (t < 2 * px) {
+      const int64_t r = t % px;
+      x = t < px ? 0 : nx - 1, y = r / nz, z = r % nz;
+    } else if (t < 2 * (px + py)) {
+      const int64_t u = t - 2 * px, r = u % py;
+      y = u < py ? 0 : ny - 1, x = r / nz, z = r % nz;
+    } else {
+      const int64_t u = t - 2 * (px + py), r = u % pz;
+      z = u < pz ? 0 : nz - 1, x = r / ny, y = r % ny;
+    }
+    const int64_t i = (x * ny + y) * nz + z;
+    field[i] = values[i];
+  }
+}
+
 // ---- reductions -------------------------------------------------------------
 __device__ __forceinline__ void atomic_min_pos(float* a, float v) { atomicMin(reinterpret_cast<int*>(a), __float_as_int(v)); }
 __device__ __forceinline__ void atomic_min_pos(double* a, double v) {
@@ -518,6 +541,17 @@ extern "C" int cfdb_op_boundary_copy(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, con
   if (int rc = check_ptrs(ctx, "cfdb_op_boundary_copy", {arr, cp, out})) return rc;
   const PlainGeomDev& p = m->plain[dtype == CFDB_F64 ? 1 : 0];
   DISPATCH(dtype, R, bcopy_k<R><<<grid_for(ctx, m->n, kThreads), kThreads, 0, ctx->stream>>>((const R*)arr, (const R*)cp, (const R*)p.isb, (R*)out, m->n));
+  CFDB_LAUNCHED(ctx);
+  return CFDB_OK;
+}
+
+extern "C" int cfdb_op_boundary_set(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, void* field, const void* values) {
+  if (int rc = cfdb_check_mesh(ctx, m)) return rc;
+  if (!dtype_ok(dtype)) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_op_boundary_set: unknown dtype %d", dtype);
+  if (int rc = check_ptrs(ctx, "cfdb_op_boundary_set", {field, values})) return rc;
+  CFDB_CUDA(ctx, cudaSetDevice(ctx->device));
+  const int64_t total = 2 * (m->ny * m->nz + m->nx * m->nz + m->nx * m->ny);
+  DISPATCH(dtype, R, bset_k<R><<<grid_for(ctx, total, kThreads), kThreads, 0, ctx->stream>>>((R*)field, (const R*)values, m->nx, m->ny, m->nz));
   CFDB_LAUNCHED(ctx);
   return CFDB_OK;
 }

@@ -443,30 +443,9 @@ int upload_as(cfdb_ctx* ctx, const double* src, int64_t count, void** dst) {
 int cfdb_mesh_need_plain(cfdb_mesh* m, int dtype) {
   PlainGeomDev& p = m->plain[dtype == CFDB_F64 ? 1 : 0];
   if (p.ready) return CFDB_OK;
-  if (int rc = cfdb_mesh_need_host_geom(m)) return rc;
-  const HostGeom& g = *m->geom;
-  cfdb_ctx* ctx = m->ctx;
-  if (!m->d_ids) {
-    std::vector<int32_t> ids(size_t(6 * m->n));
-    for (int64_t k = 0; k < 6 * m->n; ++k) ids[k] = int32_t(g.ids[k]);
-    if (int rc = cfdb_dev_alloc(ctx, int64_t(sizeof(int32_t)) * 6 * m->n, reinterpret_cast<void**>(&m->d_ids)))
-      return rc;
-    CFDB_CUDA(ctx, cudaMemcpy(m->d_ids, ids.data(), sizeof(int32_t) * ids.size(), cudaMemcpyHostToDevice));
-  }
-  auto up = [&](const std::vector<double>& v, void** dst) {
-    return dtype == CFDB_F64 ? upload_as<double>(ctx, v.data(), int64_t(v.size()), dst)
-                             : upload_as<float>(ctx, v.data(), int64_t(v.size()), dst);
-  };
-  int rc = CFDB_OK;
-  if (!rc) rc = up(g.normal, &p.normal);
-  if (!rc) rc = up(g.normal_alt, &p.normal_alt);
-  if (!rc) rc = up(g.area, &p.area);
-  if (!rc) rc = up(g.alpha, &p.alpha);
-  if (!rc) rc = up(g.len, &p.len);
-  if (!rc) rc = up(g.volume, &p.volume);
-  if (!rc) rc = up(g.isb, &p.isb);
-  if (rc) {
-    free_plain(ctx, p);
+  CFDB_CUDA(m->ctx, cudaSetDevice(m->ctx->device));
+  if (int rc = cfdb_build_plain_device(m, dtype, p)) {
+    free_plain(m->ctx, p);
     return rc;
   }
   p.ready = true;
@@ -487,6 +466,18 @@ extern "C" int cfdb_mesh_plain_geometry(cfdb_mesh* m, cfdb_plain_geometry* out) 
   out->len = static_cast<const float*>(p.len);
   out->volume = static_cast<const float*>(p.volume);
   out->n = m->n;
+  return CFDB_OK;
+}
+
+extern "C" int cfdb_mesh_lattice_geometry(cfdb_mesh* m, cfdb_lattice_geometry* out) {
+  if (!out) return cfdb_fail(m ? m->ctx : nullptr, CFDB_EINVAL, "cfdb_mesh_lattice_geometry: out is NULL");
+  if (!m || !m->ctx) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_mesh_lattice_geometry: mesh is NULL or host-only");
+  if (m->lattice_state == 0) {
+    CFDB_CUDA(m->ctx, cudaSetDevice(m->ctx->device));
+    if (int rc = cfdb_check_lattice_device(m, &m->lattice)) return rc;
+    m->lattice_state = m->lattice.exact ? 1 : 2;
+  }
+  *out = m->lattice;
   return CFDB_OK;
 }
 

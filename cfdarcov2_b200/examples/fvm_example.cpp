@@ -10,10 +10,13 @@
 //                                                 then d1t(r) = -d1dz(q) - r (operator tree)
 //   fvm_example <mode>_nojit ...                  the same with use_jit = false: operator by operator
 //                                                 instead of one generated kernel per equation
+//   fvm_example nested   out.bin nx ny nz steps   d1t(q) = 0.01 lapl(d1dx(q) + q) - 0.001 stab_tot(d1dy(q))
+//                                                 + d1dz(q q): operators of operators
 //   fvm_example euler3d  out.bin nx ny nz steps   the reference's 20-equation Euler system (main_3d.cpp)
 //   fvm_example ref_heat out.bin nx ny nz steps   the reference's heat benchmark (main_3d_heat.cpp)
 //   fvm_example ref_wave out.bin nx ny nz steps   the reference's wave benchmark (main_3d_wave.cu)
 //   fvm_example <mode>_twice ...                  evaluate twice, print evaluate_us and steady_us
+//   fvm_example <mode>_arrays ...                 generated kernels read the face arrays on exact lattices too
 //   fvm_example heat_store out.bin nx ny nz steps dir
 //                                                 heat with history kept, then the reference's output
 //                                                 calls: store_history (.vti per step), mesh.json and
@@ -29,6 +32,8 @@
 
 using namespace cfdb;
 
+static int g_lattice = 0;  // lattice_equations of the last evaluate
+
 // Equation(steps).evaluate timed on the wall clock around the call, as the
 // reference's examples time it (examples/main_3d.cpp: the time includes
 // building the generated kernels): evaluate_us.  With `twice` a second call
@@ -41,6 +46,7 @@ static int timed_evaluate(size_t steps, std::vector<Variable*>& vars, EquationTe
     eq.evaluate(vars, eqs, &dt, false);
     if (jitted) *jitted = eq.jit_equations;
     if (fused) *fused = eq.fused_equations;
+    g_lattice = eq.lattice_equations;
     return std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count();
   };
   int jitted = 0;
@@ -64,7 +70,8 @@ int main(int argc, char** argv) {
     return 2;
   }
   // "<mode>_twice": evaluate twice (second timing without kernel builds);
-  // "<mode>_nojit": the same equations with use_jit = false (operator-by-operator path)
+  // "<mode>_nojit": the same equations with use_jit = false (operator-by-operator path);
+  // "<mode>_arrays": generated kernels read the face arrays even on an exact lattice
   std::string mode = argv[1];
   auto suffix = [&](const char* s) {
     const size_t k = std::strlen(s);
@@ -73,6 +80,7 @@ int main(int argc, char** argv) {
     return true;
   };
   const bool twice = suffix("_twice");
+  const bool arrays = suffix("_arrays");
   const bool jit = !suffix("_nojit");
   const char* out = argv[2];
   const size_t nx = std::strtoul(argv[3], nullptr, 10), ny = std::strtoul(argv[4], nullptr, 10),
@@ -86,6 +94,8 @@ int main(int argc, char** argv) {
     }
     CFDArcoGlobalInit::initialize(argc, argv, !storing, storing ? argv[7] : "./dumps");
     CFDArcoGlobalInit::enable_cuda(0);
+    CFDArcoGlobalInit::jit_lattice = !arrays;
+    CFDArcoGlobalInit::jit_all = jit;
     Mesh3D mesh(nx, ny, nz, 1.f / float(nx), 1.f / float(ny), 1.f / float(nz));
     mesh.init_basic_internals();
     mesh.compute();
@@ -104,6 +114,7 @@ int main(int argc, char** argv) {
       eq.evaluate(space_vars, eqs, &dt, false, {&T});
       fused = eq.fused_equations;
       jitted = eq.jit_equations;
+      g_lattice = eq.lattice_equations;
       result.push_back(T.host());
       if (storing) {
         store_history({&T}, &mesh);
@@ -121,6 +132,7 @@ int main(int argc, char** argv) {
       Equation eq(steps);
       eq.evaluate(vars, eqs, &dt, false);
       jitted = eq.jit_equations;
+      g_lattice = eq.lattice_equations;
       result.push_back(u.host());
     } else if (mode == "advect") {
       HostVec Q0 = gaussian(mesh, 0.4f, 0.5f, 0.5f, 0.15f), Uv(mesh._num_nodes, 0.3f), Vv(mesh._num_nodes, -0.2f),
@@ -136,8 +148,24 @@ int main(int argc, char** argv) {
       Equation eq(steps);
       eq.evaluate(vars, eqs, &dt, false);
       jitted = eq.jit_equations;
+      g_lattice = eq.lattice_equations;
       result.push_back(q.host());
       result.push_back(r.host());
+    } else if (mode == "nested") {
+      // operators of operators: the generated plan materialises d1dx(q) + q and
+      // d1dy(q) in passes of their own before the outer lapl / stab_tot
+      HostVec Q0 = gaussian(mesh, 0.5f, 0.45f, 0.55f, 0.15f);
+      Variable q(&mesh, Q0, boundary_none, "q");
+      std::vector<Variable*> vars{&q};
+      DT dt(&mesh, UpdatePolicies::constant_dt, 0.001f, vars);
+      EquationTemplate eqs = {
+          {d1t(q), '=', 0.01f * lapl(d1dx(q) + q) - 0.001f * stab_tot(d1dy(q)) + d1dz(q * q), jit},
+      };
+      Equation eq(steps);
+      eq.evaluate(vars, eqs, &dt, false);
+      jitted = eq.jit_equations;
+      g_lattice = eq.lattice_equations;
+      result.push_back(q.host());
     } else if (mode == "euler3d") {
       // The reference's "euler" benchmark system (examples/main_3d.cpp): primitive
       // and conservative variables, 15 use_jit equations (primitive recovery,
@@ -261,8 +289,10 @@ int main(int argc, char** argv) {
       sum += x;
       mx = x > mx ? x : mx;
     }
-    std::printf("mode=%s cells=%zu steps=%zu fused_equations=%d jit_equations=%d sum=%.9g max=%.9g seconds=%.6f\n",
-                mode.c_str(), mesh._num_nodes, steps, fused, jitted, sum, mx, secs);
+    std::printf(
+        "mode=%s cells=%zu steps=%zu fused_equations=%d jit_equations=%d lattice_equations=%d sum=%.9g max=%.9g "
+        "seconds=%.6f\n",
+        mode.c_str(), mesh._num_nodes, steps, fused, jitted, g_lattice, sum, mx, secs);
     CFDArcoGlobalInit::finalize();
   } catch (const std::exception& e) {
     std::fprintf(stderr, "error: %s\n", e.what());

@@ -127,8 +127,10 @@ int cfdb_download(cfdb_ctx* ctx, void* dst_host, const void* src_device, int64_t
 
 /* Mesh3D(x, y, z, dx, dy, dz) + init_basic_internals() + compute() +
  * CudaMesh3D::host_to_device() (include/mesh3d.hpp:120-125,209-236;
- * src/mesh3d.cpp:151-385).  Geometry is built on the host in double; device
- * copies are made on first use.  ctx may be NULL for a host-only mesh (the
+ * src/mesh3d.cpp:151-385).  The device's face arrays are computed on the
+ * device on first use (in double, rounded to the storage type); the host
+ * copies (cfdb_mesh_geometry) are computed on the host, from the same
+ * formulas, when first asked for.  ctx may be NULL for a host-only mesh (the
  * geometry queries work; device calls fail with CFDB_EINVAL). */
 int cfdb_mesh_create_structured(cfdb_ctx* ctx, int64_t nx, int64_t ny, int64_t nz, double dx, double dy,
                                 double dz, cfdb_mesh** out);
@@ -199,6 +201,15 @@ int cfdb_op_d2t(cfdb_ctx* ctx, int dtype, const void* rhs, const void* cur, cons
  * (examples/main_3d_heat.cpp:41-46). */
 int cfdb_op_boundary_copy(cfdb_ctx* ctx, cfdb_mesh* mesh, int dtype, const void* arr, const void* copy,
                           void* out);
+
+/* The boundary copy in place, touching the boundary cells only: field[i] =
+ * values[i] for every cell on the box surface (the cells whose
+ * _node_is_boundary is 1), all other cells untouched.  Equals
+ * cfdb_op_boundary_copy(arr = out = field) for finite states up to the sign
+ * of interior zeros (the reference's blend turns -0 into +0), and reads and
+ * writes 2 x 6N^2 cells of an N^3 mesh instead of streaming all N^3 three
+ * times. */
+int cfdb_op_boundary_set(cfdb_ctx* ctx, cfdb_mesh* mesh, int dtype, void* field, const void* values);
 
 /* UpdatePolicies::CourantFriedrichsLewy3DCu / 1DCu + cfl_cu
  * (src/fvm3d.cpp:528-567; src/cuda_operators.cu:138-235):
@@ -385,6 +396,15 @@ typedef struct cfdb_kernel cfdb_kernel;
  * compile error returns CFDB_EINVAL with the compiler log in
  * cfdb_last_error. */
 int cfdb_kernel_build(cfdb_ctx* ctx, const char* source, const char* name, cfdb_kernel** out);
+/* KernelBuilder::build for a whole equation system at once: compiles the
+ * `count` sources (the distinct ones not yet loaded in ctx) on several host
+ * threads, or loads them from the on-disk kernel cache (the role of OCCA's
+ * cache: $CFDB_KERNEL_CACHE, else $XDG_CACHE_HOME/cfdb_kernels, else
+ * $HOME/.cache/cfdb_kernels; CFDB_KERNEL_CACHE=off disables it), then looks
+ * up names[k] in sources[k] into out[k].  On failure no kernel is
+ * returned. */
+int cfdb_kernel_build_many(cfdb_ctx* ctx, int count, const char* const* sources, const char* const* names,
+                           cfdb_kernel** out);
 /* KernelBuilder::run (src/fvm3d.cpp:1318-1394) without its two device
  * syncs: launches ceil(n_threads / block) CTAs of `block` threads on the
  * context's stream; args points to the kernel's argument values in order
@@ -408,6 +428,28 @@ typedef struct {
   int64_t n;
 } cfdb_plain_geometry;
 int cfdb_mesh_plain_geometry(cfdb_mesh* mesh, cfdb_plain_geometry* out);
+
+/* The same geometry as per-slot constants when the mesh is a lattice whose
+ * FP32 face values are identical in every cell (axis-aligned cells with
+ * exactly representable coordinates, e.g. unit cells): then a generated
+ * kernel may take the constants and compute the neighbour ids from the cell
+ * index instead of reading ~250 bytes of geometry per cell, and still round
+ * exactly like the array kernels.  exact = 0 otherwise (vertex meshes,
+ * spacings whose multiples round).  Per-slot arrays: normal / normal_alt
+ * entry d*6 + f, alpha / len entry wall*6 + f (wall = 1 for a boundary face).
+ * Checked once per mesh on the device, without building the arrays. */
+typedef struct {
+  int64_t nx, ny, nz;
+  int32_t exact;
+  int32_t reserved;
+  float normal[18];
+  float normal_alt[18];
+  float area[6];
+  float alpha[12];
+  float len[12];
+  float volume;
+} cfdb_lattice_geometry;
+int cfdb_mesh_lattice_geometry(cfdb_mesh* mesh, cfdb_lattice_geometry* out);
 
 /* ---- output files (host side, no GPU needed) ------------------------------
  * store_history's .vti writer (include/io_operators_tmpl.hpp:44-100) without

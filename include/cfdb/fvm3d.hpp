@@ -156,6 +156,8 @@ class Equation {
   // number of use_jit equations the last evaluate() ran as one generated,
   // run-time compiled kernel each (KernelBuilder, src/fvm3d.cpp:1219-1394)
   mutable int jit_equations = 0;
+  // of those, the equations whose kernels take an exact lattice's geometry as constants
+  mutable int lattice_equations = 0;
 };
 
 // Output of the reference's include/io_operators_tmpl.hpp, written through

@@ -31,6 +31,13 @@ class CFDArcoGlobalInit {
   static bool cuda_enabled;
   static bool store_stepping;
   static std::string store_dir;
+  // use_jit equations on an exact lattice (cfdb_mesh_lattice_geometry) take
+  // the geometry as constants instead of reading the face arrays; same bits
+  static bool jit_lattice;
+  // equations with use_jit = false run as generated kernels as well (the
+  // generated kernels give the operator path's bits); false keeps them on
+  // the operator-by-operator path as the reference runs them
+  static bool jit_all;
 };
 
 class Mesh3D {

@@ -73,33 +73,48 @@ def test_d2t_leapfrog_operator_tree(oracle, tmp_path):
     assert rel_l2(U, u) <= 1e-5
 
 
-@pytest.mark.parametrize("mode,nfields,n", [("advect", 2, 12), ("wave_d2t", 1, 16), ("advect", 2, 9)])
+@pytest.mark.parametrize("mode,nfields,n", [("advect", 2, 12), ("wave_d2t", 1, 16), ("advect", 2, 9),
+                                            ("advect", 2, 16), ("wave_d2t", 1, 13), ("nested", 1, 16),
+                                            ("nested", 1, 11)])
 def test_jit_equations_equal_operator_path_bitwise(tmp_path, mode, nfields, n):
-    """use_jit equations run as one NVRTC-compiled kernel each (KernelBuilder,
+    """use_jit equations run as generated kernels (KernelBuilder,
     src/fvm3d.cpp:1219-1394): grad, lapl and the two-stage stab of
     expressions, a plain left-hand side, d1t and d2t.  The generated kernel
     rounds like the operator-by-operator path (--fmad=false, same operand
-    order), so both give the same bits; n = 9 has nz % 4 != 0."""
+    order), so both give the same bits.  dx = 1/16 is an exact lattice: the
+    kernels take the geometry as constants, and the face-array form
+    (_arrays) gives the same bits too; n = 9, 11, 13 have nz % 4 != 0.
+    nested: operands holding operators, materialised in passes of their own."""
     steps = 7
     (J, out_j) = run_example(tmp_path, mode, n, n, n, steps, nfields)
     (P, out_p) = run_example(tmp_path, mode + "_nojit", n, n, n, steps, nfields)
+    (A, out_a) = run_example(tmp_path, mode + "_arrays", n, n, n, steps, nfields)
     jit_eqs = 2 if mode == "advect" else 1
     assert f"jit_equations={jit_eqs}" in out_j and "jit_equations=0" in out_p
+    assert "lattice_equations=0" in out_a
+    if n == 16:
+        assert f"lattice_equations={jit_eqs}" in out_j
     assert np.array_equal(J, P)
+    assert np.array_equal(A, P)
 
 
 @pytest.mark.parametrize("n", [16, 13])
 def test_reference_euler_system_jit_equals_operator_path(tmp_path, n):
     """The reference's 3-D Euler benchmark system (examples/main_3d.cpp: 15
-    use_jit equations incl. d1dx of products, 5 operator-path updates with
-    stab_tot, CFL time step, Dirichlet boundary layers): the generated
-    kernels give the operator path's bits; the state stays finite."""
+    use_jit equations incl. d1dx of products, 5 use_jit = false updates with
+    stab_tot of products, CFL time step, Dirichlet boundary layers) on unit
+    cells, an exact lattice.  All 20 run as generated kernels (geometry as
+    constants, and as face arrays) and give the bits of the operator path,
+    hence of any split between the two; the state stays finite."""
     steps = 6
     J, out_j = run_example(tmp_path, "euler3d", n, n, n, steps, 5)
     P, out_p = run_example(tmp_path, "euler3d_nojit", n, n, n, steps, 5)
-    assert "jit_equations=15" in out_j and "jit_equations=0" in out_p
+    A, out_a = run_example(tmp_path, "euler3d_arrays", n, n, n, steps, 5)
+    assert "jit_equations=20" in out_j and "jit_equations=0" in out_p
+    assert "lattice_equations=20" in out_j and "lattice_equations=0" in out_a
     assert np.isfinite(J).all()
     assert np.array_equal(J, P)
+    assert np.array_equal(A, P)
 
 
 def test_jit_heat_on_a_mesh_the_sweep_cannot_take(oracle, tmp_path):

@@ -44,6 +44,65 @@ def make_pair(cfdb, oracle, ctx, spec, np_dtype):
     return cfdb.Mesh.structured(ctx, *shape, *spacing), oracle.Mesh(*shape, *spacing, dtype=np_dtype)
 
 
+@pytest.mark.parametrize("spec", MESHES + [dict(shape=(7, 5, 9), spacing=(1 / 13, 0.3, 1 / 7), verts=None)],
+                         ids=["aniso", "cube8", "jitter6", "odd"])
+def test_device_built_geometry_equals_host_builder(cfdb, ctx, spec):
+    """The face arrays are built on the device from the same formulas as the
+    host builder: each FP32 array equals the host double rounded to float,
+    and the neighbour ids match."""
+    from cfdarcov2_b200.workloads import jittered_vertices
+    shape, spacing = spec["shape"], spec["spacing"]
+    if spec["verts"] == "jitter":
+        m = cfdb.Mesh.from_vertices(ctx, *shape, *spacing, jittered_vertices(shape[0], seed=2))
+    else:
+        m = cfdb.Mesh.structured(ctx, *shape, *spacing)
+    got = m.plain_geometry()
+    cap = cfdb.capi
+    for which, key in [(cap.GEOM_NORMAL, "normal"), (cap.GEOM_NORMAL_ALT, "normal_alt"), (cap.GEOM_AREA, "area"),
+                       (cap.GEOM_ALPHA_D, "alpha"), (cap.GEOM_LEN_C2F, "len"), (cap.GEOM_VOLUME, "volume")]:
+        assert np.array_equal(got[key], m.geometry(which).astype(np.float32)), key
+    ids, _ = m.ids()
+    assert np.array_equal(got["ids"].astype(np.int64), ids)
+
+
+@pytest.mark.parametrize("shape,spacing", [((8, 8, 8), (1.0, 1.0, 1.0)), ((6, 5, 4), (0.25, 0.5, 2.0)),
+                                           ((7, 5, 9), (1 / 13, 0.3, 1 / 7)), ((1, 4, 4), (1.0, 1.0, 1.0))])
+def test_lattice_constants_agree_with_face_arrays(cfdb, ctx, shape, spacing):
+    """cfdb_mesh_lattice_geometry says exact exactly when every cell's FP32
+    face arrays equal the per-slot constants (alpha and len split by wall)."""
+    m = cfdb.Mesh.structured(ctx, *shape, *spacing)
+    exact, c = m.lattice_geometry()
+    g = m.plain_geometry()
+    nx, ny, nz = shape
+    n = m.n
+    x, y, z = (a.ravel() for a in np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij"))
+    wall = np.stack([z == 0, z == nz - 1, y == 0, y == ny - 1, x == 0, x == nx - 1]).astype(int)  # (6, n)
+    f = np.arange(6)[:, None]
+    bits = lambda a: np.asarray(a, np.float32).view(np.uint32)
+    expect = {
+        "normal": np.concatenate([np.broadcast_to(c["normal"][d * 6:d * 6 + 6, None], (6, n)).ravel() for d in range(3)]),
+        "normal_alt": np.concatenate([np.broadcast_to(c["normal_alt"][d * 6:d * 6 + 6, None], (6, n)).ravel()
+                                      for d in range(3)]),
+        "area": np.broadcast_to(c["area"][:, None], (6, n)).ravel(),
+        "alpha": c["alpha"][wall * 6 + f].ravel(),
+        "len": c["len"][wall * 6 + f].ravel(),
+        "volume": np.full(n, c["volume"], np.float32),
+    }
+    step = np.array([-1, 1, -nz, nz, -ny * nz, ny * nz])[:, None]
+    i = np.arange(n)[None, :]
+    ids = np.where(wall == 1, i, i + step).ravel()
+    matches = all(np.array_equal(bits(g[k]), bits(v)) for k, v in expect.items()) and np.array_equal(g["ids"], ids)
+    assert exact == matches
+    if spacing == (1.0, 1.0, 1.0):
+        assert exact
+
+
+def test_lattice_check_rejects_vertex_meshes(cfdb, ctx):
+    from cfdarcov2_b200.workloads import jittered_vertices
+    m = cfdb.Mesh.from_vertices(ctx, 6, 6, 6, 1 / 6, 1 / 6, 1 / 6, jittered_vertices(6, seed=2))
+    assert not m.lattice_geometry()[0]
+
+
 @pytest.mark.parametrize("spec", MESHES, ids=["aniso", "cube8", "jitter6"])
 @pytest.mark.parametrize("op", ["grad", "lapl", "stab"])
 @pytest.mark.parametrize("mask", [7, 1, 6])
@@ -99,6 +158,15 @@ def test_boundary_copy_and_cfl(cfdb, oracle, ctx):
     isb = o.geometry()["is_boundary"]
     got = host(ctx.boundary_copy(m, dev(arr, torch.float64), dev(cp, torch.float64)))
     assert np.array_equal(got, arr * (1 - isb) + cp * isb)
+    # the in-place boundary-only form gives the same values (finite, no -0 here)
+    for shape in [(6, 5, 4), (1, 3, 4), (2, 2, 2), (7, 1, 1)]:
+        mb = cfdb.Mesh.structured(ctx, *shape, 0.1, 0.2, 0.3)
+        ob = oracle.Mesh(*shape, 0.1, 0.2, 0.3)
+        a, c = rng.standard_normal(mb.n).astype(np.float32), rng.standard_normal(mb.n).astype(np.float32)
+        b = ob.geometry()["is_boundary"].astype(np.float32)
+        ta = dev(a, torch.float32)
+        ctx.boundary_set(mb, ta, dev(c, torch.float32))
+        assert np.array_equal(host(ta), a * (1 - b) + c * b), shape
     p, rho = rng.uniform(0.5, 2, m.n), rng.uniform(0.5, 2, m.n)
     u, v, w = rng.standard_normal((3, m.n))
     d = lambda x: dev(x, torch.float64)  # noqa: E731
