@@ -3,6 +3,7 @@
 // expression node evaluates through a cfdb_op_* kernel into a buffer it
 // allocates once.
 #include <algorithm>
+#include <cmath>
 #include <cstddef>
 #include <cstdint>
 #include <cstdio>
@@ -248,10 +249,26 @@ struct JitPlan {
   // an exact lattice: the kernels take per-slot geometry constants instead of the face arrays
   bool lattice = false;
   cfdb_lattice_geometry lat{};
-  std::string geom_type() const {
-    if (!lattice) return "CfdbGeom";
-    return "CfdbLattice<" + std::to_string(lat.nx) + "LL, " + std::to_string(lat.ny) + "LL, " +
-           std::to_string(lat.nz) + "LL>";
+  std::string geom_type() const { return lattice ? "CfdbLattice<CfdbC>" : "CfdbGeom"; }
+  // the lattice's dimensions and constants as compile-time values of the source
+  std::string lattice_struct() const {
+    if (!lattice) return std::string();
+    auto hex = [](float v) {
+      char b[40];
+      std::snprintf(b, sizeof(b), "%af", double(v));
+      return std::string(b);
+    };
+    auto fn = [&](const char* name, const float* v, int count) {
+      std::string f = "  __device__ static constexpr float " + std::string(name) + "(int k) {\n    switch (k) {\n";
+      for (int k = 0; k < count; ++k) f += "      case " + std::to_string(k) + ": return " + hex(v[k]) + ";\n";
+      return f + "      default: return 0.f;\n    }\n  }\n";
+    };
+    std::string s = "struct CfdbC {\n  static constexpr long long NX = " + std::to_string(lat.nx) +
+                    "LL, NY = " + std::to_string(lat.ny) + "LL, NZ = " + std::to_string(lat.nz) + "LL;\n";
+    s += fn("nrm", lat.normal, 18) + fn("nalt", lat.normal_alt, 18) + fn("area", lat.area, 6) +
+         fn("alpha", lat.alpha, 12) + fn("len", lat.len, 12);
+    s += "  __device__ static constexpr float volume() { return " + hex(lat.volume) + "; }\n};\n";
+    return s;
   }
   std::vector<std::unique_ptr<JitPass>> passes;  // run order; the last computes the equation
   std::vector<float*> scratch;
@@ -385,7 +402,7 @@ struct JitGen {
     return k;
   }
   std::string prelude() const {
-    return "#include \"cfdb_jit.cuh\"\nstruct CfdbArgs { const float* f[" +
+    return "#include \"cfdb_jit.cuh\"\n" + plan.lattice_struct() + "struct CfdbArgs { const float* f[" +
            std::to_string(std::max<size_t>(1, inputs.size())) + "]; float dt; " + plan.geom_type() + " g; };\n";
   }
   // every generated kernel has the signature (A, out, cur, prev, mode, n)
@@ -449,6 +466,7 @@ std::unique_ptr<JitPlan> jit_build(const Node* rhs, Mesh3D* mesh) {
   if (CFDArcoGlobalInit::jit_lattice) {
     check(cfdb_mesh_lattice_geometry(mesh->handle(), &plan->lat), "cfdb_mesh_lattice_geometry");
     plan->lattice = plan->lat.exact != 0;
+    for (const float* v = plan->lat.normal; v <= &plan->lat.volume; ++v) plan->lattice = plan->lattice && std::isfinite(*v);
   }
   JitGen g(*plan);
   const int root = g.emit(rhs);
@@ -482,8 +500,8 @@ void jit_compile(const std::vector<std::unique_ptr<JitPlan>>& plans) {
 // equation's update (mode 0: value, 1: d1t, 2: d2t) into `out`.
 void jit_run(const JitPlan& plan, float dt, float* out, const float* cur, const float* prev, int mode) {
   // CfdbArgs { const float* f[nf]; float dt; G g; } laid out as the device
-  // compiler does: G = CfdbGeom (pointers, 8-byte aligned) or CfdbLattice
-  // (67 floats: the constants of cfdb_lattice_geometry from normal on)
+  // compiler does: G = CfdbGeom (pointers, 8-byte aligned) or the empty
+  // CfdbLattice<CfdbC>; the struct's size rounds up to its 8-byte alignment
   struct Geom {
     const int32_t* ids;
     const float *normal, *normal_alt, *area, *alpha, *len, *volume;
@@ -491,13 +509,11 @@ void jit_run(const JitPlan& plan, float dt, float* out, const float* cur, const 
   } geom{};
   const unsigned char* gsrc;
   size_t gsize, galign;
-  if (plan.lattice) {
-    gsrc = reinterpret_cast<const unsigned char*>(plan.lat.normal);
-    gsize = sizeof(float) * 67;
-    galign = alignof(float);
-    static_assert(offsetof(cfdb_lattice_geometry, volume) - offsetof(cfdb_lattice_geometry, normal) ==
-                      sizeof(float) * 66,
-                  "lattice constants are contiguous");
+  static const unsigned char empty = 0;
+  if (plan.lattice) {  // CfdbLattice<CfdbC> is an empty struct: its constants are in the source
+    gsrc = &empty;
+    gsize = 1;
+    galign = 1;
   } else {
     cfdb_plain_geometry g{};
     check(cfdb_mesh_plain_geometry(plan.mesh->handle(), &g), "cfdb_mesh_plain_geometry");
@@ -511,7 +527,7 @@ void jit_run(const JitPlan& plan, float dt, float* out, const float* cur, const 
     const size_t nf = std::max<size_t>(1, p->inputs.size());
     const size_t off_dt = nf * sizeof(void*);
     const size_t off_g = (off_dt + sizeof(float) + galign - 1) / galign * galign;
-    std::vector<unsigned char> A(off_g + gsize, 0);
+    std::vector<unsigned char> A((off_g + gsize + 7) / 8 * 8, 0);
     for (size_t k = 0; k < p->inputs.size(); ++k) {
       const JitInput& in = p->inputs[k];
       const float* ptr = in.field ? in.field->current_cu : plan.scratch[size_t(in.scratch)];

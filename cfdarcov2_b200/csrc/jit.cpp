@@ -38,9 +38,9 @@ const char* kJitHeader = R"CFDB(
 // Geometry of a generated kernel, read through accessors so that one set of
 // operator templates serves both forms: CfdbGeom reads the per-face arrays
 // (entry (i, f) at f*n + i, per-dimension arrays stacked at d*6n), and
-// CfdbLattice<NX, NY, NZ> holds the per-slot constants of an exact lattice
-// and derives the neighbour ids and wall faces from the cell index.  Both
-// give the same values, so the operator arithmetic rounds the same.
+// CfdbLattice<C> takes the per-slot constants of an exact lattice and derives
+// the neighbour ids and wall faces from the cell index.  Both give the same
+// values, so the operator arithmetic rounds the same.
 struct CfdbGeom {
   const int* ids;
   const float* normal;
@@ -58,37 +58,51 @@ struct CfdbGeom {
   __device__ __forceinline__ float alpha(int f, long long i) const { return alpha_[f * n + i]; }
   __device__ __forceinline__ float len(int f, long long i) const { return len_[f * n + i]; }
   __device__ __forceinline__ float volume(long long i) const { return volume_[i]; }
+  __device__ __forceinline__ static constexpr bool nrm_nonzero(int, int) { return true; }
+  __device__ __forceinline__ static constexpr bool nalt_nonzero(int, int) { return true; }
 };
 
-template <long long NX, long long NY, long long NZ> struct CfdbLattice {
-  float normal[18];      // d*6 + f
-  float normal_alt[18];  // d*6 + f
-  float area_[6];
-  float alpha_[12];      // wall*6 + f
-  float len_[12];        // wall*6 + f
-  float volume_;
-  __device__ __forceinline__ long long count() const { return NX * NY * NZ; }
-  __device__ __forceinline__ bool wall(int f, long long i) const {
-    const long long x = i / (NY * NZ), r = i - x * (NY * NZ), y = r / NZ, z = r - y * NZ;
+// C: a generated struct with the lattice's dimensions (NX, NY, NZ) and its
+// per-slot constants as constexpr functions (nrm(k), nalt(k) with k = d*6 + f;
+// area(f); alpha(k), len(k) with k = wall*6 + f; volume()).  Known at
+// compile time, a zero normal component drops its face term: the term is
+// +-0, and adding +-0 to an accumulator that starts at +0 never changes it,
+// so for finite operands the sum keeps the array form's bits.
+template <class C> struct CfdbLattice {
+  __device__ __forceinline__ static constexpr long long count() { return C::NX * C::NY * C::NZ; }
+  __device__ __forceinline__ static bool wall(int f, long long i) {
+    long long x, y, z;
+    if (count() < (1LL << 31)) {  // 32-bit division by constants
+      const unsigned ii = (unsigned)i, pl = (unsigned)(C::NY * C::NZ);
+      const unsigned xx = ii / pl, r = ii - xx * pl, yy = r / (unsigned)C::NZ;
+      x = xx, y = yy, z = r - yy * (unsigned)C::NZ;
+    } else {
+      x = i / (C::NY * C::NZ);
+      const long long r = i - x * (C::NY * C::NZ);
+      y = r / C::NZ, z = r - y * C::NZ;
+    }
     switch (f) {
       case 0: return z == 0;
-      case 1: return z == NZ - 1;
+      case 1: return z == C::NZ - 1;
       case 2: return y == 0;
-      case 3: return y == NY - 1;
+      case 3: return y == C::NY - 1;
       case 4: return x == 0;
-      default: return x == NX - 1;
+      default: return x == C::NX - 1;
     }
   }
-  __device__ __forceinline__ long long id(int f, long long i) const {
-    const long long step = f == 0 ? -1LL : f == 1 ? 1LL : f == 2 ? -NZ : f == 3 ? NZ : f == 4 ? -NY * NZ : NY * NZ;
+  __device__ __forceinline__ static long long id(int f, long long i) {
+    const long long step = f == 0 ? -1LL : f == 1 ? 1LL : f == 2 ? -C::NZ : f == 3 ? C::NZ
+                         : f == 4 ? -C::NY * C::NZ : C::NY * C::NZ;
     return wall(f, i) ? i : i + step;
   }
-  __device__ __forceinline__ float nrm(int d, int f, long long) const { return normal[d * 6 + f]; }
-  __device__ __forceinline__ float nalt(int d, int f, long long) const { return normal_alt[d * 6 + f]; }
-  __device__ __forceinline__ float area(int f, long long) const { return area_[f]; }
-  __device__ __forceinline__ float alpha(int f, long long i) const { return alpha_[(wall(f, i) ? 6 : 0) + f]; }
-  __device__ __forceinline__ float len(int f, long long i) const { return len_[(wall(f, i) ? 6 : 0) + f]; }
-  __device__ __forceinline__ float volume(long long) const { return volume_; }
+  __device__ __forceinline__ static constexpr bool nrm_nonzero(int d, int f) { return C::nrm(d * 6 + f) != 0.f; }
+  __device__ __forceinline__ static constexpr bool nalt_nonzero(int d, int f) { return C::nalt(d * 6 + f) != 0.f; }
+  __device__ __forceinline__ static float nrm(int d, int f, long long) { return C::nrm(d * 6 + f); }
+  __device__ __forceinline__ static float nalt(int d, int f, long long) { return C::nalt(d * 6 + f); }
+  __device__ __forceinline__ static float area(int f, long long) { return C::area(f); }
+  __device__ __forceinline__ static float alpha(int f, long long i) { return C::alpha((wall(f, i) ? 6 : 0) + f); }
+  __device__ __forceinline__ static float len(int f, long long i) { return C::len((wall(f, i) ? 6 : 0) + f); }
+  __device__ __forceinline__ static float volume(long long) { return C::volume(); }
 };
 
 // Green-Gauss gradient, component mask (bit d: d/dx_d), faces take the mean
@@ -104,6 +118,7 @@ template <class F, class G> __device__ __forceinline__ float cfdb_grad(F phi, lo
     float acc = 0.f;
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
+      if (!g.nalt_nonzero(d, f)) continue;
       const float itp = (crr + nb[f]) * 0.5f;
       const float t = itp * g.nalt(d, f, i);
       acc = acc + t * g.area(f, i);
@@ -120,6 +135,7 @@ template <class F, class G> __device__ __forceinline__ float cfdb_grad_component
   float acc = 0.f;
 #pragma unroll
   for (int f = 0; f < 6; ++f) {
+    if (!g.nalt_nonzero(d, f)) continue;
     const float itp = (crr + phi(g.id(f, j))) * 0.5f;
     const float t = itp * g.nalt(d, f, j);
     acc = acc + t * g.area(f, j);
@@ -140,6 +156,7 @@ template <class F, class G> __device__ __forceinline__ float cfdb_lapl(F phi, lo
     float acc = 0.f;
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
+      if (!g.nrm_nonzero(d, f)) continue;
       const float t = sn[f] * g.nrm(d, f, i);
       acc = acc + t * g.area(f, i);
     }
@@ -206,6 +223,7 @@ __device__ __forceinline__ float cfdb_stab2g(F phi, const float* gr, long long i
     float acc = 0.f;
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
+      if (!g.nrm_nonzero(d, f)) continue;
       const long long j = g.id(f, i);
       const float own = crr + g.len(f, i) * gi * g.nalt(d, f, i);
       const float col = phi(j) + g.len(f ^ 1, j) * gr[d * n + j] * g.nalt(d, f ^ 1, j);
