@@ -11,6 +11,7 @@
 #include <ctime>
 #include <filesystem>
 #include <map>
+#include <set>
 #include <memory>
 #include <stdexcept>
 #include <utility>
@@ -239,6 +240,8 @@ struct JitPass {
   std::string source, entry;  // compiled by jit_compile, all passes of all equations at once
   std::vector<JitInput> inputs;
   int out_scratch = -1;  // -1: the equation's output (the last pass)
+  bool group = false;    // a group pass: writes outputs[k]->next_cu, signature (A, n)
+  std::vector<Variable*> outputs;
   ~JitPass() {
     if (k) cfdb_kernel_destroy(k);
   }
@@ -301,6 +304,9 @@ struct JitGen {
   std::map<const Node*, int> done;
   std::string funcs;
   int next = 0;
+  // in a group kernel: fields written by earlier members -> their slot in V
+  // (the member's value at this cell, held in a register)
+  const std::map<Variable*, int>* written = nullptr;
   explicit JitGen(JitPlan& p) : plan(p) {}
 
   static std::string lit(float v) {
@@ -341,13 +347,13 @@ struct JitGen {
     if (inline_operand(n)) {
       const int k = emit(n);
       if (k < 0) return std::string();
-      return "[&](long long j) { return e" + std::to_string(k) + "(j, A); }";
+      return "[&](long long j) { return e" + std::to_string(k) + "(j, A, V); }";
     }
     const int s = plan.materialise(n);
     if (s < 0) return std::string();
     return "[&](long long j) { return A.f[" + std::to_string(input(JitInput{nullptr, s})) + "][j]; }";
   }
-  std::string call(int k) { return "e" + std::to_string(k) + "(i, A)"; }
+  std::string call(int k) { return "e" + std::to_string(k) + "(i, A, V)"; }
   int emit(const Node* n) {
     auto it = done.find(n);
     if (it != done.end()) return it->second;
@@ -355,7 +361,12 @@ struct JitGen {
     std::string body;
     static const char* ops[] = {" + ", " - ", " * ", " / "};
     switch (n->kind) {
-      case Node::kField: body = "A.f[" + std::to_string(input(JitInput{n->field, -1})) + "][i]"; break;
+      case Node::kField: {
+        auto w = written ? written->find(n->field) : std::map<Variable*, int>::const_iterator();
+        if (written && w != written->end()) body = "V[" + std::to_string(w->second) + "]";
+        else body = "A.f[" + std::to_string(input(JitInput{n->field, -1})) + "][i]";
+        break;
+      }
       case Node::kConst: body = lit(n->value); break;
       case Node::kDt: body = "A.dt"; break;
       case Node::kBinary: {
@@ -396,8 +407,8 @@ struct JitGen {
         return -1;
     }
     const int k = next++;
-    funcs += "__device__ __forceinline__ float e" + std::to_string(k) + "(long long i, const CfdbArgs& A) { return " +
-             body + "; }\n";
+    funcs += "__device__ __forceinline__ float e" + std::to_string(k) +
+             "(long long i, const CfdbArgs& A, const float* V) { return " + body + "; }\n";
     done[n] = k;
     return k;
   }
@@ -412,7 +423,8 @@ struct JitGen {
            "                                        const float* __restrict__ prev, int mode, long long n) {\n"
            "  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;\n"
            "  if (i >= n) return;\n"
-           "  const float R = e" + std::to_string(root) + "(i, A);\n"
+           "  const float* V = nullptr;\n"
+           "  const float R = e" + std::to_string(root) + "(i, A, V);\n"
            "  if (mode == 0) out[i] = R;                                      // plain left-hand side, scratch\n"
            "  else if (mode == 1) out[i] = A.dt * R + cur[i];                 // d1t, first d2t step\n"
            "  else out[i] = (A.dt * A.dt * R + 2.0f * cur[i]) - prev[i];      // d2t\n"
@@ -453,6 +465,7 @@ int JitPlan::stab_grad(const Node* operand) {
                           "                                           const float*, int, long long n) {\n"
                           "  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;\n"
                           "  if (i >= n) return;\n"
+                          "  const float* V = nullptr;\n"
                           "  cfdb_stab_grad(" + phi + ", i, gr, A.g);\n"
                           "}\n";
   add_pass(src, "cfdb_stab_stage1", g.inputs, s);
@@ -460,7 +473,7 @@ int JitPlan::stab_grad(const Node* operand) {
   return s;
 }
 
-std::unique_ptr<JitPlan> jit_build(const Node* rhs, Mesh3D* mesh) {
+std::unique_ptr<JitPlan> new_plan(Mesh3D* mesh) {
   auto plan = std::make_unique<JitPlan>();
   plan->mesh = mesh;
   if (CFDArcoGlobalInit::jit_lattice) {
@@ -468,6 +481,11 @@ std::unique_ptr<JitPlan> jit_build(const Node* rhs, Mesh3D* mesh) {
     plan->lattice = plan->lat.exact != 0;
     for (const float* v = plan->lat.normal; v <= &plan->lat.volume; ++v) plan->lattice = plan->lattice && std::isfinite(*v);
   }
+  return plan;
+}
+
+std::unique_ptr<JitPlan> jit_build(const Node* rhs, Mesh3D* mesh) {
+  auto plan = new_plan(mesh);
   JitGen g(*plan);
   const int root = g.emit(rhs);
   if (!plan->ok || root < 0) return nullptr;
@@ -475,14 +493,90 @@ std::unique_ptr<JitPlan> jit_build(const Node* rhs, Mesh3D* mesh) {
   return plan;
 }
 
+// Fields an expression reads inside the operand of a neighbour operator
+// (grad, lapl, stab: at other cells, or in a pass of their own) and the ones
+// it reads at its own cell only.
+void collect_fields(const Node* n, bool in_operand, std::set<Variable*>& nb, std::set<Variable*>& own) {
+  switch (n->kind) {
+    case Node::kField: (in_operand ? nb : own).insert(n->field); break;
+    case Node::kBinary:
+      collect_fields(n->a.get(), in_operand, nb, own);
+      collect_fields(n->b.get(), in_operand, nb, own);
+      break;
+    case Node::kNeg: collect_fields(n->a.get(), in_operand, nb, own); break;
+    case Node::kGrad:
+    case Node::kLapl:
+    case Node::kStab: collect_fields(n->a.get(), true, nb, own); break;
+    default: break;
+  }
+}
+
+// One member of a group: the equation's right-hand side, the field it
+// writes and its form (0 plain left-hand side, 1 d1t).
+struct GroupMember {
+  const Node* rhs;
+  Variable* target;
+  int form;
+};
+
+// A run of consecutive equations compiled into one kernel (after the
+// pre-passes their operands need).  Every member's right-hand side is
+// evaluated in order at the thread's cell; a field written by an earlier
+// member is read from that member's register value (the equations run in
+// sequence, so the later ones see it updated), and no member reads such a
+// field at another cell (the caller ends a group before that would happen).
+// Each written field's last value goes to its next buffer.  Arithmetic per
+// member is that of the single-equation kernel, so the bits are the same.
+std::unique_ptr<JitPlan> jit_group_build(const std::vector<GroupMember>& members, Mesh3D* mesh) {
+  auto plan = new_plan(mesh);
+  JitGen g(*plan);
+  std::map<Variable*, int> written;
+  std::string body;
+  for (size_t m = 0; m < members.size(); ++m) {
+    const GroupMember& gm = members[m];
+    g.done.clear();  // a node's value may differ once an earlier member wrote one of its fields
+    g.written = &written;
+    const int root = g.emit(gm.rhs);
+    if (!plan->ok || root < 0) return nullptr;
+    std::string update = "R";
+    if (gm.form == 1) {
+      auto w = written.find(gm.target);
+      const std::string cur = w != written.end() ? "V[" + std::to_string(w->second) + "]"
+                                                 : "A.f[" + std::to_string(g.input(JitInput{gm.target, -1})) + "][i]";
+      update = "A.dt * R + " + cur;
+    }
+    body += "  { const float R = e" + std::to_string(root) + "(i, A, V); V[" + std::to_string(m) + "] = " + update +
+            "; }\n";
+    written[gm.target] = int(m);
+  }
+  std::vector<Variable*> outputs;
+  std::string stores;
+  for (const auto& kv : written) {
+    stores += "  A.o[" + std::to_string(outputs.size()) + "][i] = V[" + std::to_string(kv.second) + "];\n";
+    outputs.push_back(kv.first);
+  }
+  const std::string src =
+      "#include \"cfdb_jit.cuh\"\n" + plan->lattice_struct() + "struct CfdbArgs { const float* f[" +
+      std::to_string(std::max<size_t>(1, g.inputs.size())) + "]; float* o[" + std::to_string(outputs.size()) +
+      "]; float dt; " + plan->geom_type() + " g; };\n" + g.funcs +
+      "extern \"C\" __global__ void cfdb_group(CfdbArgs A, long long n) {\n"
+      "  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;\n"
+      "  if (i >= n) return;\n"
+      "  float V[" + std::to_string(members.size()) + "];\n" + body + stores + "}\n";
+  plan->add_pass(src, "cfdb_group", g.inputs, -1);
+  plan->passes.back()->group = true;
+  plan->passes.back()->outputs = outputs;
+  return plan;
+}
+
 // KernelBuilder::build for every plan of an equation system in one call: the
 // library compiles the sources on several host threads (or loads them from
 // its on-disk kernel cache).
-void jit_compile(const std::vector<std::unique_ptr<JitPlan>>& plans) {
+void jit_compile(const std::vector<std::unique_ptr<JitPlan>*>& plans) {
   std::vector<JitPass*> passes;
-  for (const auto& plan : plans)
-    if (plan)
-      for (const auto& p : plan->passes)
+  for (const auto* plan : plans)
+    if (*plan)
+      for (const auto& p : (*plan)->passes)
         if (!p->k) passes.push_back(p.get());
   if (passes.empty()) return;
   std::vector<const char*> srcs, names;
@@ -524,8 +618,9 @@ void jit_run(const JitPlan& plan, float dt, float* out, const float* cur, const 
   }
   long long n = (long long)plan.mesh->_num_nodes;
   for (const auto& p : plan.passes) {
-    const size_t nf = std::max<size_t>(1, p->inputs.size());
-    const size_t off_dt = nf * sizeof(void*);
+    // group passes carry their output pointers after the inputs: { f[nf]; o[no]; dt; g }
+    const size_t nf = std::max<size_t>(1, p->inputs.size()), no = p->group ? p->outputs.size() : 0;
+    const size_t off_dt = (nf + no) * sizeof(void*);
     const size_t off_g = (off_dt + sizeof(float) + galign - 1) / galign * galign;
     std::vector<unsigned char> A((off_g + gsize + 7) / 8 * 8, 0);
     for (size_t k = 0; k < p->inputs.size(); ++k) {
@@ -533,8 +628,14 @@ void jit_run(const JitPlan& plan, float dt, float* out, const float* cur, const 
       const float* ptr = in.field ? in.field->current_cu : plan.scratch[size_t(in.scratch)];
       std::memcpy(&A[k * sizeof(void*)], &ptr, sizeof(ptr));
     }
+    for (size_t k = 0; k < no; ++k) std::memcpy(&A[(nf + k) * sizeof(void*)], &p->outputs[k]->next_cu, sizeof(void*));
     std::memcpy(&A[off_dt], &dt, sizeof(dt));
     std::memcpy(&A[off_g], gsrc, gsize);
+    if (p->group) {
+      void* args[] = {A.data(), &n};
+      check(cfdb_kernel_launch(p->k, n, 256, args), "cfdb_kernel_launch");
+      continue;
+    }
     float* o = p->out_scratch >= 0 ? plan.scratch[size_t(p->out_scratch)] : out;
     int m = p->out_scratch >= 0 ? 0 : mode;
     void* args[] = {A.data(), &o, &cur, &prev, &m, &n};
@@ -738,27 +839,83 @@ void Equation::evaluate(std::vector<Variable*>& all_vars, EquationTemplate& eqs,
   fused_equations = 0;
   jit_equations = 0;
   lattice_equations = 0;
+  jit_groups = 0;
   // use_jit equations (tuple element 3), and with jit_all the others too,
-  // that are not the fused heat template become a plan of generated kernels
-  // each, all compiled before the first step
-  std::vector<std::unique_ptr<JitPlan>> jit(eqs.size());
+  // that are not the fused heat template run as generated kernels, all
+  // compiled before the first step: consecutive plain and d1t equations fuse
+  // into groups (one kernel after their operands' pre-passes), a group ending
+  // where a member would read at other cells a field an earlier member wrote;
+  // d2t equations get a plan of their own.
+  struct Unit {
+    std::unique_ptr<JitPlan> plan;
+    size_t count = 1;    // equations the unit covers, from its first
+    bool group = false;
+  };
+  std::vector<Unit> units;
+  std::vector<int> unit_at(eqs.size(), -1);  // unit starting at this equation
+  std::vector<GroupMember> open;
+  size_t open_first = 0;
+  Mesh3D* open_mesh = nullptr;
+  std::set<Variable*> open_written;
+  auto close_group = [&] {
+    if (open.empty()) return;
+    auto plan = jit_group_build(open, open_mesh);
+    if (plan) {  // otherwise the members stay on the operator path
+      jit_equations += int(open.size());
+      if (plan->lattice) lattice_equations += int(open.size());
+      ++jit_groups;
+      unit_at[open_first] = int(units.size());
+      units.push_back(Unit{std::move(plan), open.size(), true});
+    }
+    open.clear();
+    open_written.clear();
+  };
+  jit_groups = 0;
+  constexpr size_t kMaxGroup = 16;
   for (size_t e = 0; e < eqs.size(); ++e) {
     Variable* lhs = std::get<0>(eqs[e]);
     const Node* rhs = std::get<2>(eqs[e]).node.get();
-    if (!rhs || (!std::get<3>(eqs[e]) && !CFDArcoGlobalInit::jit_all)) continue;
     float k = 0.f;
     auto* d = dynamic_cast<DtVar*>(lhs);
     auto* d2 = dynamic_cast<D2tVar*>(lhs);
     Mesh3D* mesh = d ? d->var->mesh : (d2 ? d2->var->mesh : lhs->mesh);
-    if (!mesh) continue;
-    if (d && match_heat(rhs, d->var, &k) && stencil_fusable(d->var->mesh)) continue;
-    jit[e] = jit_build(rhs, mesh);
-    if (jit[e]) {
-      ++jit_equations;
-      if (jit[e]->lattice) ++lattice_equations;
+    const bool generate = rhs && mesh && (std::get<3>(eqs[e]) || CFDArcoGlobalInit::jit_all) &&
+                          !(d && match_heat(rhs, d->var, &k) && stencil_fusable(d->var->mesh)) &&
+                          (d || d2 || lhs->is_field);
+    if (!generate) {
+      close_group();
+      continue;
     }
+    if (d2) {
+      close_group();
+      auto plan = jit_build(rhs, mesh);
+      if (plan) {
+        ++jit_equations;
+        if (plan->lattice) ++lattice_equations;
+        unit_at[e] = int(units.size());
+        units.push_back(Unit{std::move(plan), 1, false});
+      }
+      continue;
+    }
+    std::set<Variable*> nb, own;
+    collect_fields(rhs, false, nb, own);
+    bool clash = mesh != open_mesh || open.size() >= kMaxGroup;
+    for (Variable* v : nb) clash = clash || open_written.count(v) > 0;
+    if (clash) close_group();
+    if (open.empty()) {
+      open_first = e;
+      open_mesh = mesh;
+    }
+    Variable* target = d ? d->var : lhs;
+    open.push_back(GroupMember{rhs, target, d ? 1 : 0});
+    open_written.insert(target);
   }
-  jit_compile(jit);
+  close_group();
+  {
+    std::vector<std::unique_ptr<JitPlan>*> plans;
+    for (Unit& u : units) plans.push_back(&u.plan);
+    jit_compile(plans);
+  }
   for (size_t t = 0; t < timesteps; ++t) {
     dt->update();
     const float dtv = dt->_dt;
@@ -766,16 +923,21 @@ void Equation::evaluate(std::vector<Variable*>& all_vars, EquationTemplate& eqs,
       auto& eq = eqs[e];
       Variable* lhs = std::get<0>(eq);
       Variable& rhs = std::get<2>(eq);
-      const JitPlan* J = jit[e].get();
+      const Unit* U = unit_at[e] >= 0 ? &units[size_t(unit_at[e])] : nullptr;
+      if (U && U->group) {
+        jit_run(*U->plan, dtv, nullptr, nullptr, nullptr, 0);
+        for (Variable* v : U->plan->passes.back()->outputs) std::swap(v->current_cu, v->next_cu);
+        e += U->count - 1;
+        continue;
+      }
+      const JitPlan* J = U ? U->plan.get() : nullptr;
       if (auto* d = dynamic_cast<DtVar*>(lhs)) {
         Variable* T = d->var;
         const int64_t N = int64_t(T->mesh->_num_nodes);
         float k = 0.f;
-        if (J) {
-          jit_run(*J, dtv, T->next_cu, T->current_cu, nullptr, 1);
-        } else if (match_heat(rhs.node.get(), T, &k) &&
-                   cfdb_heat_step(ctx, T->mesh->handle(), CFDB_F32, CFDB_PATH_FUSED, T->current_cu, T->next_cu, k,
-                                  dtv) == CFDB_OK) {
+        if (match_heat(rhs.node.get(), T, &k) &&
+            cfdb_heat_step(ctx, T->mesh->handle(), CFDB_F32, CFDB_PATH_FUSED, T->current_cu, T->next_cu, k,
+                           dtv) == CFDB_OK) {
           if (t == 0) ++fused_equations;
         } else {
           const float* R = eval_node(rhs.node.get());
@@ -783,27 +945,24 @@ void Equation::evaluate(std::vector<Variable*>& all_vars, EquationTemplate& eqs,
         }
         std::swap(T->current_cu, T->next_cu);
       } else if (auto* d2 = dynamic_cast<D2tVar*>(lhs)) {
-        Variable* U = d2->var;
-        const int64_t N = int64_t(U->mesh->_num_nodes);
-        if (!U->prev_cu) U->prev_cu = device_alloc(U->mesh->_num_nodes);
+        Variable* Uv = d2->var;
+        const int64_t N = int64_t(Uv->mesh->_num_nodes);
+        if (!Uv->prev_cu) Uv->prev_cu = device_alloc(Uv->mesh->_num_nodes);
         if (J) {
-          jit_run(*J, dtv, U->next_cu, U->current_cu, U->prev_cu, U->has_prev ? 2 : 1);
+          jit_run(*J, dtv, Uv->next_cu, Uv->current_cu, Uv->prev_cu, Uv->has_prev ? 2 : 1);
         } else {
           const float* R = eval_node(rhs.node.get());
-          check(cfdb_op_d2t(ctx, CFDB_F32, R, U->current_cu, U->prev_cu, dtv, U->has_prev ? 1 : 0, U->next_cu, N),
+          check(cfdb_op_d2t(ctx, CFDB_F32, R, Uv->current_cu, Uv->prev_cu, dtv, Uv->has_prev ? 1 : 0, Uv->next_cu,
+                            N),
                 "cfdb_op_d2t");
         }
-        std::swap(U->prev_cu, U->current_cu);  // prev <- current
-        std::swap(U->current_cu, U->next_cu);  // current <- next
-        U->has_prev = true;
+        std::swap(Uv->prev_cu, Uv->current_cu);  // prev <- current
+        std::swap(Uv->current_cu, Uv->next_cu);  // current <- next
+        Uv->has_prev = true;
       } else if (lhs->is_field) {
-        if (J) {
-          jit_run(*J, dtv, lhs->next_cu, nullptr, nullptr, 0);
-        } else {
-          const float* R = eval_node(rhs.node.get());
-          check(cfdb_op_scalar(ctx, CFDB_F32, CFDB_OP_MUL, R, 1.0, lhs->next_cu, int64_t(lhs->mesh->_num_nodes)),
-                "cfdb_op_scalar");
-        }
+        const float* R = eval_node(rhs.node.get());
+        check(cfdb_op_scalar(ctx, CFDB_F32, CFDB_OP_MUL, R, 1.0, lhs->next_cu, int64_t(lhs->mesh->_num_nodes)),
+              "cfdb_op_scalar");
         std::swap(lhs->current_cu, lhs->next_cu);
       } else {
         throw std::runtime_error("Equation: left-hand side must be a field, d1t(field) or d2t(field)");

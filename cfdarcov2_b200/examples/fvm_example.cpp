@@ -33,6 +33,7 @@
 using namespace cfdb;
 
 static int g_lattice = 0;  // lattice_equations of the last evaluate
+static int g_groups = 0;   // jit_groups of the last evaluate
 
 // Equation(steps).evaluate timed on the wall clock around the call, as the
 // reference's examples time it (examples/main_3d.cpp: the time includes
@@ -47,6 +48,7 @@ static int timed_evaluate(size_t steps, std::vector<Variable*>& vars, EquationTe
     if (jitted) *jitted = eq.jit_equations;
     if (fused) *fused = eq.fused_equations;
     g_lattice = eq.lattice_equations;
+    g_groups = eq.jit_groups;
     return std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count();
   };
   int jitted = 0;
@@ -115,6 +117,8 @@ int main(int argc, char** argv) {
       fused = eq.fused_equations;
       jitted = eq.jit_equations;
       g_lattice = eq.lattice_equations;
+      g_groups = eq.jit_groups;
+    g_groups = eq.jit_groups;
       result.push_back(T.host());
       if (storing) {
         store_history({&T}, &mesh);
@@ -133,6 +137,8 @@ int main(int argc, char** argv) {
       eq.evaluate(vars, eqs, &dt, false);
       jitted = eq.jit_equations;
       g_lattice = eq.lattice_equations;
+      g_groups = eq.jit_groups;
+    g_groups = eq.jit_groups;
       result.push_back(u.host());
     } else if (mode == "advect") {
       HostVec Q0 = gaussian(mesh, 0.4f, 0.5f, 0.5f, 0.15f), Uv(mesh._num_nodes, 0.3f), Vv(mesh._num_nodes, -0.2f),
@@ -149,6 +155,8 @@ int main(int argc, char** argv) {
       eq.evaluate(vars, eqs, &dt, false);
       jitted = eq.jit_equations;
       g_lattice = eq.lattice_equations;
+      g_groups = eq.jit_groups;
+    g_groups = eq.jit_groups;
       result.push_back(q.host());
       result.push_back(r.host());
     } else if (mode == "nested") {
@@ -165,6 +173,8 @@ int main(int argc, char** argv) {
       eq.evaluate(vars, eqs, &dt, false);
       jitted = eq.jit_equations;
       g_lattice = eq.lattice_equations;
+      g_groups = eq.jit_groups;
+    g_groups = eq.jit_groups;
       result.push_back(q.host());
     } else if (mode == "euler3d") {
       // The reference's "euler" benchmark system (examples/main_3d.cpp): primitive
@@ -290,9 +300,9 @@ int main(int argc, char** argv) {
       mx = x > mx ? x : mx;
     }
     std::printf(
-        "mode=%s cells=%zu steps=%zu fused_equations=%d jit_equations=%d lattice_equations=%d sum=%.9g max=%.9g "
-        "seconds=%.6f\n",
-        mode.c_str(), mesh._num_nodes, steps, fused, jitted, g_lattice, sum, mx, secs);
+        "mode=%s cells=%zu steps=%zu fused_equations=%d jit_equations=%d lattice_equations=%d jit_groups=%d sum=%.9g "
+        "max=%.9g seconds=%.6f\n",
+        mode.c_str(), mesh._num_nodes, steps, fused, jitted, g_lattice, g_groups, sum, mx, secs);
     CFDArcoGlobalInit::finalize();
   } catch (const std::exception& e) {
     std::fprintf(stderr, "error: %s\n", e.what());

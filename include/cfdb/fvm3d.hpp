@@ -158,6 +158,8 @@ class Equation {
   mutable int jit_equations = 0;
   // of those, the equations whose kernels take an exact lattice's geometry as constants
   mutable int lattice_equations = 0;
+  // kernels the generated plain / d1t equations fuse into (one per group of consecutive equations)
+  mutable int jit_groups = 0;
 };
 
 // Output of the reference's include/io_operators_tmpl.hpp, written through

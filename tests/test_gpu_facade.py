@@ -84,13 +84,17 @@ def test_jit_equations_equal_operator_path_bitwise(tmp_path, mode, nfields, n):
     order), so both give the same bits.  dx = 1/16 is an exact lattice: the
     kernels take the geometry as constants, and the face-array form
     (_arrays) gives the same bits too; n = 9, 11, 13 have nz % 4 != 0.
-    nested: operands holding operators, materialised in passes of their own."""
+    nested: operands holding operators, materialised in passes of their own.
+    advect: the second equation reads q at neighbours after the first wrote
+    it, so the two run as two kernels."""
     steps = 7
     (J, out_j) = run_example(tmp_path, mode, n, n, n, steps, nfields)
     (P, out_p) = run_example(tmp_path, mode + "_nojit", n, n, n, steps, nfields)
     (A, out_a) = run_example(tmp_path, mode + "_arrays", n, n, n, steps, nfields)
     jit_eqs = 2 if mode == "advect" else 1
     assert f"jit_equations={jit_eqs}" in out_j and "jit_equations=0" in out_p
+    if mode == "advect":
+        assert "jit_groups=2" in out_j
     assert "lattice_equations=0" in out_a
     if n == 16:
         assert f"lattice_equations={jit_eqs}" in out_j
@@ -112,6 +116,9 @@ def test_reference_euler_system_jit_equals_operator_path(tmp_path, n):
     A, out_a = run_example(tmp_path, "euler3d_arrays", n, n, n, steps, 5)
     assert "jit_equations=20" in out_j and "jit_equations=0" in out_p
     assert "lattice_equations=20" in out_j and "lattice_equations=0" in out_a
+    # fused into 4 kernels: [rho, u, v, w, p recovery], [predictor rho, u, v, w],
+    # [predictor p, mass flux], [4 fluxes + 5 updates]
+    assert "jit_groups=4" in out_j
     assert np.isfinite(J).all()
     assert np.array_equal(J, P)
     assert np.array_equal(A, P)
