@@ -430,13 +430,28 @@ def run_secondary(args):
         if args.no_extras:
             res["fp64_plain"] = res["fp32_fused"]
         err = l2(res["fp32_fused"][2], res["fp64_plain"][2])
+        extra = {"fp64_plain": {"value": res["fp64_plain"][0], "unit": "cell-updates/s"},
+                 "speedup_fused_fp32_vs_plain_fp64": res["fp32_fused"][0] / res["fp64_plain"][0],
+                 "accuracy_vs_fp64": {"l2_rel": err[0], "linf_rel": err[1]},
+                 "path": "cluster-resident (one launch per solve)" if res["fp32_fused"][3] == K else "per-step sweep"}
+        if not args.no_extras:
+            # the same step beyond L2: 512^3 (2 x 537 MB), 50 steps, per-step TMA sweep
+            nb, Tb = 512, 50
+            mb = cfdb.Mesh.structured(ctx, nb, nb, nb, 1 / nb, 1 / nb, 1 / nb)
+            Tl = torch.rand(nb ** 3, dtype=torch.float32, device=dev)
+            al, bl = Tl.clone(), torch.empty_like(Tl)
+            dtb = 0.1 * (1 / nb) ** 2 / cfg["k"]
+            msb = _timed(lambda: ctx.heat_run(mb, al, bl, cfg["k"], dtb, Tb, path=cfdb.FUSED, use_graph=True), 3, 2,
+                         flush, prep=lambda: al.copy_(Tl)) / 3 / Tb
+            peak, _ = measured_peak_hbm()
+            ach = 8 * nb ** 3 / (msb * 1e-3) / 1e9
+            extra["roofline_beyond_l2"] = {"mesh": [nb] * 3, "time_steps": Tb, "achieved": ach, "peak": peak,
+                                           "unit": "GB/s", "frac": ach / peak, "ms_per_step": msb,
+                                           "cell_updates_per_s": nb ** 3 / (msb * 1e-3)}
+            del mb, Tl, al, bl
         _line(args, "heat3d_64^3_x200_steps", res["fp32_fused"][0], res["fp32_fused"][1],
               {"mesh": [n] * 3, "k": cfg["k"], "dt": cfg["dt"], "time_steps_per_bench_step": T}, 8, n ** 3, T,
-              {"fp64_plain": {"value": res["fp64_plain"][0], "unit": "cell-updates/s"},
-               "speedup_fused_fp32_vs_plain_fp64": res["fp32_fused"][0] / res["fp64_plain"][0],
-               "accuracy_vs_fp64": {"l2_rel": err[0], "linf_rel": err[1]},
-               "path": "cluster-resident (one launch per solve)" if res["fp32_fused"][3] == K else "per-step sweep"},
-              launches=res["fp32_fused"][3])
+              extra, launches=res["fp32_fused"][3])
     elif args.workload == "wave_distorted":
         cfg = W.wave_config(n=args.n, steps=args.tsteps or 500)
         n, T = cfg["n"], cfg["steps"]
@@ -490,21 +505,44 @@ def run_secondary(args):
         ex = riemann.sample(xc, 0.2, 0.5, (1.0, 0.0, 1.0), (0.125, 0.0, 0.1))
         tot = res["fp32_fused"][4]
         steps = res["fp32_fused"][3]
+        extra = {"fp64_plain": {"value": res["fp64_plain"][0], "unit": "cell-updates/s", "time_steps": res["fp64_plain"][3]},
+                 "speedup_fused_fp32_vs_plain_fp64": res["fp32_fused"][0] / res["fp64_plain"][0],
+                 "accuracy_vs_fp64": {"l2_rel": err[0], "linf_rel": err[1]},
+                 "fp64_totals_drift": {"mass": float(np.abs(tot[:, 0] - tot[0, 0]).max() / tot[0, 0]),
+                                       "energy": float(np.abs(tot[:, 1] - tot[0, 1]).max() / tot[0, 1])},
+                 "l1_rho_vs_exact_riemann": float(np.mean(np.abs(rho - ex[0])))}
+        if not args.no_extras:
+            # the same scheme beyond L2: 2048x256x256 (2 x 2.7 GB), the first 40 steps
+            mb = cfdb.Mesh.structured(ctx, 2048, 256, 256, 1 / 2048, 0.125 / 256, 0.125 / 256)
+            Nb, Tb = 2048 * 256 * 256, 40
+            eb = cfdb.Euler(ctx, mb, dtype=cfdb.F32, path=cfdb.FUSED, gamma=1.4, cfl=0.4, t_end=0.2, max_steps=Tb)
+            left = (torch.arange(2048, device=dev, dtype=torch.float64) + 0.5) / 2048 < 0.5
+            Ub = torch.zeros(5 * Nb, dtype=torch.float32, device=dev)  # the Sod state of sod_state(), built on the device
+            Ub[:Nb] = torch.where(left, 1.0, 0.125).float().repeat_interleave(256 * 256)
+            Ub[4 * Nb:] = (torch.where(left, 1.0, 0.1) / 0.4).float().repeat_interleave(256 * 256)
+            ab, bb = torch.empty_like(Ub), torch.empty_like(Ub)
+            outb = {}
+
+            def solve_b():
+                eb.begin(ab)
+                outb["r"] = eb.run(ab, bb, 256)
+            msb = _timed(solve_b, 3, 2, flush, prep=lambda: ab.copy_(Ub)) / 3 / Tb
+            peak, _ = measured_peak_hbm()
+            ach = 40 * Nb / (msb * 1e-3) / 1e9
+            extra["roofline_beyond_l2"] = {"mesh": [2048, 256, 256], "time_steps": outb["r"][0], "achieved": ach,
+                                           "peak": peak, "unit": "GB/s", "frac": ach / peak, "ms_per_step": msb,
+                                           "cell_updates_per_s": Nb / (msb * 1e-3)}
+            del eb, mb, Ub, ab, bb
         _line(args, "sod_512x64x64_rusanov_to_t0.2", res["fp32_fused"][0], res["fp32_fused"][1],
               {"mesh": [nx, ny, nz], "gamma": 1.4, "cfl": 0.4, "t_end": 0.2, "time_steps": steps}, 40, N, steps,
-              {"fp64_plain": {"value": res["fp64_plain"][0], "unit": "cell-updates/s", "time_steps": res["fp64_plain"][3]},
-               "speedup_fused_fp32_vs_plain_fp64": res["fp32_fused"][0] / res["fp64_plain"][0],
-               "accuracy_vs_fp64": {"l2_rel": err[0], "linf_rel": err[1]},
-               "fp64_totals_drift": {"mass": float(np.abs(tot[:, 0] - tot[0, 0]).max() / tot[0, 0]),
-                                     "energy": float(np.abs(tot[:, 1] - tot[0, 1]).max() / tot[0, 1])},
-               "l1_rho_vs_exact_riemann": float(np.mean(np.abs(rho - ex[0])))},
-              launches=res["fp32_fused"][5])
+              extra, launches=res["fp32_fused"][5])
     elif args.workload == "ensemble":
         probs = W.ensemble_problems()
         b = cfdb.Batch(ctx, probs)
         pool0 = torch.tensor(W.ensemble_initial(probs, b.offsets, b.pool_elems), device=dev)
         a, c = pool0.clone(), torch.empty_like(pool0)
-        b.tune(a, c, os.path.join(ROOT, "_work", "ensemble_tune.json") if os.path.isdir(os.path.join(ROOT, "_work")) else None)
+        import tempfile
+        b.tune(a, c, os.path.join(tempfile.gettempdir(), "cfdb_ensemble_tune.json"))
         T = args.tsteps or 300
         cells = sum(p["n"] ** 3 for p in probs)
         alg = sum(p["n"] ** 3 * (8 if p["kind"] == 0 else 32) for p in probs)

@@ -7,6 +7,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <ctime>
 #include <filesystem>
@@ -240,8 +241,10 @@ struct JitPass {
   std::string source, entry;  // compiled by jit_compile, all passes of all equations at once
   std::vector<JitInput> inputs;
   int out_scratch = -1;  // -1: the equation's output (the last pass)
-  bool group = false;    // a group pass: writes outputs[k]->next_cu, signature (A, n)
-  std::vector<Variable*> outputs;
+  // a multi-output pass (a group, the merged stab stage 1): signature (A, n),
+  // A.o[k] = outputs[k]: a field's next buffer or a scratch buffer
+  bool multi = false;
+  std::vector<JitInput> outputs;
   ~JitPass() {
     if (k) cfdb_kernel_destroy(k);
   }
@@ -287,7 +290,19 @@ struct JitPlan {
   }
   int materialise(const Node* n);
   int stab_grad(const Node* operand);
+  // stab stage-1 passes not yet emitted: (operand: a field, a scratch buffer
+  // or an inline node; output scratch).  They are merged into one kernel,
+  // emitted before the next pass that may read them.
+  struct PendingStab {
+    JitInput src;
+    const Node* node;  // inline operand, else null
+    int out;
+  };
+  std::vector<PendingStab> pending_stab;
+  bool flushing = false;
+  void flush_stab();
   void add_pass(const std::string& src, const char* entry, std::vector<JitInput> inputs, int out) {
+    flush_stab();
     auto p = std::make_unique<JitPass>();
     p->source = src;
     p->entry = entry;
@@ -448,29 +463,75 @@ int JitPlan::materialise(const Node* n) {
 }
 
 // Stage 1 of a stabilisation: the operand's three gradient components per
-// cell, one pass per distinct operand (a field, or an operand node).
+// cell into a 3n scratch, one per distinct operand (a field, or an operand
+// node); the kernel is emitted later, merged with the plan's other stage-1
+// passes (flush_stab).  An operand that holds operators is materialised now.
 int JitPlan::stab_grad(const Node* operand) {
   const void* key = operand->kind == Node::kField ? static_cast<const void*>(operand->field) : operand;
   auto it = stab_grads.find(key);
   if (it != stab_grads.end()) return it->second;
-  JitGen g(*this);
-  const std::string phi = g.operand(operand);
-  if (!ok || phi.empty()) {
-    ok = false;
-    return -1;
+  PendingStab ps{};
+  if (operand->kind == Node::kField) {
+    ps.src = JitInput{operand->field, -1};
+  } else if (JitGen::inline_operand(operand)) {
+    ps.node = operand;
+  } else {
+    const int m = materialise(operand);
+    if (m < 0) {
+      ok = false;
+      return -1;
+    }
+    ps.src = JitInput{nullptr, m};
   }
-  const int s = new_scratch(3 * mesh->_num_nodes);
-  const std::string src = g.prelude() + g.funcs +
-                          "extern \"C\" __global__ void cfdb_stab_stage1(CfdbArgs A, float* __restrict__ gr, const float*,\n"
-                          "                                           const float*, int, long long n) {\n"
-                          "  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;\n"
-                          "  if (i >= n) return;\n"
-                          "  const float* V = nullptr;\n"
-                          "  cfdb_stab_grad(" + phi + ", i, gr, A.g);\n"
-                          "}\n";
-  add_pass(src, "cfdb_stab_stage1", g.inputs, s);
-  stab_grads[key] = s;
-  return s;
+  ps.out = new_scratch(3 * mesh->_num_nodes);
+  pending_stab.push_back(ps);
+  stab_grads[key] = ps.out;
+  return ps.out;
+}
+
+// Emits the pending stage-1 passes, one kernel per operand.  (One kernel for
+// all of them, sharing the loads of common fields, measured 1.3x slower on
+// the reference's Euler system at 200^3: fewer resident warps, no reuse won.)
+void JitPlan::flush_stab() {
+  if (pending_stab.empty() || flushing) return;
+  if (pending_stab.size() > 1) {  // one kernel per operand (measured faster than one merged kernel)
+    const auto all = pending_stab;
+    for (const auto& ps : all) {
+      pending_stab.assign(1, ps);
+      flush_stab();
+    }
+    return;
+  }
+  flushing = true;
+  JitGen g(*this);
+  std::string body;
+  std::vector<JitInput> outs;
+  for (const PendingStab& ps : pending_stab) {
+    const std::string phi =
+        ps.node ? g.operand(ps.node)
+                : "[&](long long j) { return A.f[" + std::to_string(g.input(ps.src)) + "][j]; }";
+    if (!ok || phi.empty()) {
+      ok = false;
+      break;
+    }
+    body += "  cfdb_stab_grad(" + phi + ", i, A.o[" + std::to_string(outs.size()) + "], A.g);\n";
+    outs.push_back(JitInput{nullptr, ps.out});
+  }
+  pending_stab.clear();
+  if (ok) {
+    const std::string src =
+        "#include \"cfdb_jit.cuh\"\n" + lattice_struct() + "struct CfdbArgs { const float* f[" +
+        std::to_string(std::max<size_t>(1, g.inputs.size())) + "]; float* o[" + std::to_string(outs.size()) +
+        "]; float dt; " + geom_type() + " g; };\n" + g.funcs +
+        "extern \"C\" __global__ void cfdb_stab_stage1(CfdbArgs A, long long n) {\n"
+        "  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;\n"
+        "  if (i >= n) return;\n"
+        "  const float* V = nullptr;\n" + body + "}\n";
+    add_pass(src, "cfdb_stab_stage1", g.inputs, -1);
+    passes.back()->multi = true;
+    passes.back()->outputs = outs;
+  }
+  flushing = false;
 }
 
 std::unique_ptr<JitPlan> new_plan(Mesh3D* mesh) {
@@ -564,8 +625,8 @@ std::unique_ptr<JitPlan> jit_group_build(const std::vector<GroupMember>& members
       "  if (i >= n) return;\n"
       "  float V[" + std::to_string(members.size()) + "];\n" + body + stores + "}\n";
   plan->add_pass(src, "cfdb_group", g.inputs, -1);
-  plan->passes.back()->group = true;
-  plan->passes.back()->outputs = outputs;
+  plan->passes.back()->multi = true;
+  for (Variable* v : outputs) plan->passes.back()->outputs.push_back(JitInput{v, -1});
   return plan;
 }
 
@@ -619,7 +680,7 @@ void jit_run(const JitPlan& plan, float dt, float* out, const float* cur, const 
   long long n = (long long)plan.mesh->_num_nodes;
   for (const auto& p : plan.passes) {
     // group passes carry their output pointers after the inputs: { f[nf]; o[no]; dt; g }
-    const size_t nf = std::max<size_t>(1, p->inputs.size()), no = p->group ? p->outputs.size() : 0;
+    const size_t nf = std::max<size_t>(1, p->inputs.size()), no = p->multi ? p->outputs.size() : 0;
     const size_t off_dt = (nf + no) * sizeof(void*);
     const size_t off_g = (off_dt + sizeof(float) + galign - 1) / galign * galign;
     std::vector<unsigned char> A((off_g + gsize + 7) / 8 * 8, 0);
@@ -628,10 +689,14 @@ void jit_run(const JitPlan& plan, float dt, float* out, const float* cur, const 
       const float* ptr = in.field ? in.field->current_cu : plan.scratch[size_t(in.scratch)];
       std::memcpy(&A[k * sizeof(void*)], &ptr, sizeof(ptr));
     }
-    for (size_t k = 0; k < no; ++k) std::memcpy(&A[(nf + k) * sizeof(void*)], &p->outputs[k]->next_cu, sizeof(void*));
+    for (size_t k = 0; k < no; ++k) {
+      const JitInput& o = p->outputs[k];
+      float* ptr = o.field ? o.field->next_cu : plan.scratch[size_t(o.scratch)];
+      std::memcpy(&A[(nf + k) * sizeof(void*)], &ptr, sizeof(ptr));
+    }
     std::memcpy(&A[off_dt], &dt, sizeof(dt));
     std::memcpy(&A[off_g], gsrc, gsize);
-    if (p->group) {
+    if (p->multi) {
       void* args[] = {A.data(), &n};
       check(cfdb_kernel_launch(p->k, n, 256, args), "cfdb_kernel_launch");
       continue;
@@ -926,7 +991,7 @@ void Equation::evaluate(std::vector<Variable*>& all_vars, EquationTemplate& eqs,
       const Unit* U = unit_at[e] >= 0 ? &units[size_t(unit_at[e])] : nullptr;
       if (U && U->group) {
         jit_run(*U->plan, dtv, nullptr, nullptr, nullptr, 0);
-        for (Variable* v : U->plan->passes.back()->outputs) std::swap(v->current_cu, v->next_cu);
+        for (const JitInput& o : U->plan->passes.back()->outputs) std::swap(o.field->current_cu, o.field->next_cu);
         e += U->count - 1;
         continue;
       }
