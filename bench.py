@@ -381,7 +381,7 @@ def _timed(fn, steps, warmup, flush, prep=None, ctx=None):
 
 
 def _line(args, workload, value, ms_per_step, cfg, alg_bytes_per_update, updates_per_launch, launches_per_step,
-          extra, dtype="f32", launches=None):
+          extra, dtype="f32", launches=None, traffic_profile=None):
     """One JSON line.  launches_per_step: time steps per bench step (the
     roofline's per-step time); launches: kernels counted by the library in
     the timed region (gpu_launches)."""
@@ -392,7 +392,9 @@ def _line(args, workload, value, ms_per_step, cfg, alg_bytes_per_update, updates
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded)", "config": dict(cfg, workload=workload),
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                         "traffic": None, "peak_source": f"{kind} hbm_gbs",
+                         "traffic": profiled_traffic(traffic_profile) if traffic_profile else None,
+                         "traffic_source": f"profiles/{traffic_profile}" if traffic_profile else None,
+                         "peak_source": f"{kind} hbm_gbs",
                          "algorithmic_bytes_per_cell_update": alg_bytes_per_update},
             "gpu_launches": launches if launches is not None else args.steps * launches_per_step}
     line.update(extra)
@@ -474,7 +476,7 @@ def run_secondary(args):
               T, {"fp64_plain": {"value": res["fp64_plain"][0], "unit": "cell-updates/s"},
                   "speedup_fused_fp32_vs_plain_fp64": res["fp32_fused"][0] / res["fp64_plain"][0],
                   "accuracy_vs_fp64": {"l2_rel": err[0], "linf_rel": err[1]}},
-              launches=res["fp32_fused"][3])
+              launches=res["fp32_fused"][3], traffic_profile="distorted_sweep_128.txt" if n == 128 else None)
     elif args.workload == "sod":
         from oracle import riemann
         cfg = W.sod_config()
@@ -535,7 +537,7 @@ def run_secondary(args):
             del eb, mb, Ub, ab, bb
         _line(args, "sod_512x64x64_rusanov_to_t0.2", res["fp32_fused"][0], res["fp32_fused"][1],
               {"mesh": [nx, ny, nz], "gamma": 1.4, "cfl": 0.4, "t_end": 0.2, "time_steps": steps}, 40, N, steps,
-              extra, launches=res["fp32_fused"][5])
+              extra, launches=res["fp32_fused"][5], traffic_profile="euler_sweep_sod.txt")
     elif args.workload == "ensemble":
         probs = W.ensemble_problems()
         b = cfdb.Batch(ctx, probs)
@@ -553,7 +555,8 @@ def run_secondary(args):
               {"problems": len(probs), "cells": cells, "time_steps_per_bench_step": T,
                "heat": sum(1 for p in probs if p["kind"] == 0), "wave": sum(1 for p in probs if p["kind"] == 1),
                "tuned_config": list(b.get_config())}, alg / cells, cells, T,
-              {"launches_per_step": b.launch_count() // T}, launches=ens_launches)
+              {"launches_per_step": b.launch_count() // T}, launches=ens_launches,
+              traffic_profile="ensemble_batch_512.txt")
     elif args.workload == "adjoint":
         cfg = W.adjoint_config(n=args.n, steps=args.tsteps or 400)
         n, T, dt = cfg["n"], cfg["steps"], cfg["dt"]
@@ -588,7 +591,7 @@ def run_secondary(args):
                "forward_solve_ms": ms_fwd / K, "gradient_ms": ms_grad / K,
                "grad_rel_err_vs_fd": abs(adj - fd) / abs(fd), "fd_eps": eps, "J": J,
                "note": "value counts forward + adjoint cell-updates; roofline uses the adjoint sweep's 60 B/cell"},
-              launches=grad_launches)
+              launches=grad_launches, traffic_profile="adjoint_sweep_128.txt" if n == 128 else None)
 
 
 # the reference's own benchmark rows (scripts/benchmark_cfdarchov2.py: 200
