@@ -107,7 +107,7 @@ struct DistPhys {
   static constexpr int NA = 10;
   static constexpr bool HAS_C = false;
   static constexpr int FT = 14;
-  static constexpr int MIN_BLOCKS = 2;
+  static constexpr int MIN_BLOCKS = 3;
   struct Params {
     float dt, c;
     int mode;
