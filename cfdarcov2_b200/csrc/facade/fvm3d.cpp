@@ -228,6 +228,15 @@ const float* eval_node(Node* n) {
 // --fmad=false, so the plan's result equals the operator chain's bit for
 // bit.
 
+// Cells per thread of the generated kernels (JitPlan::cells).
+// Measured on the reference's benchmark systems: the single-equation wave
+// kernel 206 -> 308 G cell-updates/s at 4 cells per thread (400^3); the
+// Euler system's group kernels lose with 2 (7.4 -> 6.6 G at 200^3: the
+// 9-member group's registers double) and its stab passes are level.
+constexpr int kCptEquation = 4;
+constexpr int kCptGroup = 1;
+constexpr int kCptStab = 1;
+
 // An input of a generated kernel: a field's current buffer (looked up at
 // launch time: fields swap buffers every step) or a scratch buffer of the plan.
 struct JitInput {
@@ -245,6 +254,7 @@ struct JitPass {
   // A.o[k] = outputs[k]: a field's next buffer or a scratch buffer
   bool multi = false;
   std::vector<JitInput> outputs;
+  int cpt = 1;  // cells per thread (consecutive chunks of the CTA size)
   ~JitPass() {
     if (k) cfdb_kernel_destroy(k);
   }
@@ -256,6 +266,19 @@ struct JitPlan {
   bool lattice = false;
   cfdb_lattice_geometry lat{};
   std::string geom_type() const { return lattice ? "CfdbLattice<CfdbC>" : "CfdbGeom"; }
+  // Kernel body over `cpt` cells per thread, i = chunk start + c x CTA size:
+  // every cell's values are computed (`compute`, may use c and i) before any
+  // is stored (`store`), so the loads of all of a thread's cells are in
+  // flight together: a one-cell thread has two DRAM misses in flight (its
+  // new plane and its previous value), too few to cover the DRAM latency.
+  static std::string cells(int cpt, const std::string& decls, const std::string& compute, const std::string& store) {
+    const std::string c = std::to_string(cpt);
+    return "  const long long i0 = (long long)blockIdx.x * (blockDim.x * " + c + ") + threadIdx.x;\n" + decls +
+           "#pragma unroll\n  for (int c = 0; c < " + c + "; ++c) {\n"
+           "    const long long i = i0 + (long long)c * blockDim.x;\n    if (i < n) {\n" + compute + "    }\n  }\n"
+           "#pragma unroll\n  for (int c = 0; c < " + c + "; ++c) {\n"
+           "    const long long i = i0 + (long long)c * blockDim.x;\n    if (i < n) {\n" + store + "    }\n  }\n";
+  }
   // the lattice's dimensions and constants as compile-time values of the source
   std::string lattice_struct() const {
     if (!lattice) return std::string();
@@ -436,13 +459,13 @@ struct JitGen {
     return prelude() + funcs +
            "extern \"C\" __global__ void cfdb_equation(CfdbArgs A, float* __restrict__ out, const float* __restrict__ cur,\n"
            "                                        const float* __restrict__ prev, int mode, long long n) {\n"
-           "  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;\n"
-           "  if (i >= n) return;\n"
-           "  const float* V = nullptr;\n"
-           "  const float R = e" + std::to_string(root) + "(i, A, V);\n"
-           "  if (mode == 0) out[i] = R;                                      // plain left-hand side, scratch\n"
-           "  else if (mode == 1) out[i] = A.dt * R + cur[i];                 // d1t, first d2t step\n"
-           "  else out[i] = (A.dt * A.dt * R + 2.0f * cur[i]) - prev[i];      // d2t\n"
+           "  const float* V = nullptr;\n" +
+           JitPlan::cells(kCptEquation, "  float Rv[" + std::to_string(kCptEquation) + "];\n",
+                          "      Rv[c] = e" + std::to_string(root) + "(i, A, V);\n",
+                          "      const float R = Rv[c];\n"
+                          "      if (mode == 0) out[i] = R;                                  // plain left-hand side, scratch\n"
+                          "      else if (mode == 1) out[i] = A.dt * R + cur[i];             // d1t, first d2t step\n"
+                          "      else out[i] = (A.dt * A.dt * R + 2.0f * cur[i]) - prev[i];  // d2t\n") +
            "}\n";
   }
 };
@@ -458,6 +481,7 @@ int JitPlan::materialise(const Node* n) {
   }
   const int s = new_scratch(mesh->_num_nodes);
   add_pass(g.equation_source(root), "cfdb_equation", g.inputs, s);
+  passes.back()->cpt = kCptEquation;
   materialised[n] = s;
   return s;
 }
@@ -504,7 +528,7 @@ void JitPlan::flush_stab() {
   }
   flushing = true;
   JitGen g(*this);
-  std::string body;
+  std::string body, stores;
   std::vector<JitInput> outs;
   for (const PendingStab& ps : pending_stab) {
     const std::string phi =
@@ -514,7 +538,12 @@ void JitPlan::flush_stab() {
       ok = false;
       break;
     }
-    body += "  cfdb_stab_grad(" + phi + ", i, A.o[" + std::to_string(outs.size()) + "], A.g);\n";
+    const std::string k = std::to_string(outs.size());
+    for (int d = 0; d < 3; ++d) {  // the components cfdb_stab_grad stores, each at d*n + i of its buffer
+      const std::string slot = std::to_string(3 * outs.size() + size_t(d));
+      body += "      G[c][" + slot + "] = cfdb_grad_component(" + phi + ", i, " + std::to_string(d) + ", A.g);\n";
+      stores += "      A.o[" + k + "][" + std::to_string(d) + " * n + i] = G[c][" + slot + "];\n";
+    }
     outs.push_back(JitInput{nullptr, ps.out});
   }
   pending_stab.clear();
@@ -524,12 +553,14 @@ void JitPlan::flush_stab() {
         std::to_string(std::max<size_t>(1, g.inputs.size())) + "]; float* o[" + std::to_string(outs.size()) +
         "]; float dt; " + geom_type() + " g; };\n" + g.funcs +
         "extern \"C\" __global__ void cfdb_stab_stage1(CfdbArgs A, long long n) {\n"
-        "  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;\n"
-        "  if (i >= n) return;\n"
-        "  const float* V = nullptr;\n" + body + "}\n";
+        "  const float* V = nullptr;\n" +
+        cells(kCptStab, "  float G[" + std::to_string(kCptStab) + "][" + std::to_string(3 * outs.size()) + "];\n",
+              body, stores) +
+        "}\n";
     add_pass(src, "cfdb_stab_stage1", g.inputs, -1);
     passes.back()->multi = true;
     passes.back()->outputs = outs;
+    passes.back()->cpt = kCptStab;
   }
   flushing = false;
 }
@@ -551,6 +582,7 @@ std::unique_ptr<JitPlan> jit_build(const Node* rhs, Mesh3D* mesh) {
   const int root = g.emit(rhs);
   if (!plan->ok || root < 0) return nullptr;
   plan->add_pass(g.equation_source(root), "cfdb_equation", g.inputs, -1);
+  plan->passes.back()->cpt = kCptEquation;
   return plan;
 }
 
@@ -606,25 +638,27 @@ std::unique_ptr<JitPlan> jit_group_build(const std::vector<GroupMember>& members
                                                  : "A.f[" + std::to_string(g.input(JitInput{gm.target, -1})) + "][i]";
       update = "A.dt * R + " + cur;
     }
-    body += "  { const float R = e" + std::to_string(root) + "(i, A, V); V[" + std::to_string(m) + "] = " + update +
+    body += "      { const float R = e" + std::to_string(root) + "(i, A, V); V[" + std::to_string(m) + "] = " + update +
             "; }\n";
     written[gm.target] = int(m);
   }
   std::vector<Variable*> outputs;
   std::string stores;
   for (const auto& kv : written) {
-    stores += "  A.o[" + std::to_string(outputs.size()) + "][i] = V[" + std::to_string(kv.second) + "];\n";
+    stores += "      A.o[" + std::to_string(outputs.size()) + "][i] = VV[c][" + std::to_string(kv.second) + "];\n";
     outputs.push_back(kv.first);
   }
   const std::string src =
       "#include \"cfdb_jit.cuh\"\n" + plan->lattice_struct() + "struct CfdbArgs { const float* f[" +
       std::to_string(std::max<size_t>(1, g.inputs.size())) + "]; float* o[" + std::to_string(outputs.size()) +
       "]; float dt; " + plan->geom_type() + " g; };\n" + g.funcs +
-      "extern \"C\" __global__ void cfdb_group(CfdbArgs A, long long n) {\n"
-      "  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;\n"
-      "  if (i >= n) return;\n"
-      "  float V[" + std::to_string(members.size()) + "];\n" + body + stores + "}\n";
+      "extern \"C\" __global__ void cfdb_group(CfdbArgs A, long long n) {\n" +
+      JitPlan::cells(kCptGroup,
+                     "  float VV[" + std::to_string(kCptGroup) + "][" + std::to_string(members.size()) + "];\n",
+                     "      float* V = VV[c];\n" + body, stores) +
+      "}\n";
   plan->add_pass(src, "cfdb_group", g.inputs, -1);
+  plan->passes.back()->cpt = kCptGroup;
   plan->passes.back()->multi = true;
   for (Variable* v : outputs) plan->passes.back()->outputs.push_back(JitInput{v, -1});
   return plan;
@@ -696,15 +730,17 @@ void jit_run(const JitPlan& plan, float dt, float* out, const float* cur, const 
     }
     std::memcpy(&A[off_dt], &dt, sizeof(dt));
     std::memcpy(&A[off_g], gsrc, gsize);
+    // cpt cells per thread: chunks of 256 cells, one CTA per 256 * cpt cells
+    const long long blocks = (n + 256LL * p->cpt - 1) / (256LL * p->cpt);
     if (p->multi) {
       void* args[] = {A.data(), &n};
-      check(cfdb_kernel_launch(p->k, n, 256, args), "cfdb_kernel_launch");
+      check(cfdb_kernel_launch(p->k, blocks * 256, 256, args), "cfdb_kernel_launch");
       continue;
     }
     float* o = p->out_scratch >= 0 ? plan.scratch[size_t(p->out_scratch)] : out;
     int m = p->out_scratch >= 0 ? 0 : mode;
     void* args[] = {A.data(), &o, &cur, &prev, &m, &n};
-    check(cfdb_kernel_launch(p->k, n, 256, args), "cfdb_kernel_launch");
+    check(cfdb_kernel_launch(p->k, blocks * 256, 256, args), "cfdb_kernel_launch");
   }
 }
 
