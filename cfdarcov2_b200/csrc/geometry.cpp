@@ -58,12 +58,9 @@ bool cfdb_build_geometry(HostGeom& g, int64_t nx, int64_t ny, int64_t nz, double
     for (int64_t y = 0; y < ny; ++y)
       for (int64_t z = 0; z < nz; ++z) {
         const int64_t i = L.id(x, y, z);
-        CellFace fs[6];
         bool bnd = false;
-        const double vol = cell_geometry(L, x, y, z, mode, center_of, fs, &bnd);
-        for (int f = 0; f < 6; ++f) {
+        auto store = [&](int f, const CellFace& o) {
           const int64_t k6 = int64_t(f) * n + i;
-          const CellFace& o = fs[f];
           g.normal[k6] = o.uns.x; g.normal[6 * n + k6] = o.uns.y; g.normal[12 * n + k6] = o.uns.z;
           g.normal_alt[k6] = o.good.x; g.normal_alt[6 * n + k6] = o.good.y; g.normal_alt[12 * n + k6] = o.good.z;
           g.area[k6] = o.area;
@@ -71,7 +68,8 @@ bool cfdb_build_geometry(HostGeom& g, int64_t nx, int64_t ny, int64_t nz, double
           g.len[k6] = o.len;
           g.ids[k6] = o.id;
           g.ibf[k6] = o.ibf;
-        }
+        };
+        const double vol = cell_geometry(L, x, y, z, mode, center_of, store, &bnd);
         g.volume[i] = vol;
         g.isb[i] = bnd ? 1.0 : 0.0;
       }

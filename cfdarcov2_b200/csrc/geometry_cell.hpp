@@ -99,12 +99,14 @@ struct CellFace {
   int64_t id, ibf;  // neighbour (the cell itself on a wall) and -1 on a wall
 };
 
-// Computes the six faces of cell (x, y, z) into out[6] and returns its
-// volume; *boundary is set when a face lies on the wall.  center_of(x, y, z)
-// gives a cell centre (the same value Lattice::center computes).
-template <class CenterOf>
+// Computes the six faces of cell (x, y, z), handing each to face(f, o) as
+// it is done (no per-cell face array: the device builders keep one face in
+// registers), and returns the cell's volume; *boundary is set when a face
+// lies on the wall.  center_of(x, y, z) gives a cell centre (the same value
+// Lattice::center computes).
+template <class CenterOf, class FaceSink>
 CFDB_HD double cell_geometry(const Lattice& L, int64_t x, int64_t y, int64_t z, int mode, CenterOf center_of,
-                             CellFace out[6], bool* boundary) {
+                             FaceSink face, bool* boundary) {
   const int64_t i = L.id(x, y, z);
   P3 v[8];
   L.corners(x, y, z, v);
@@ -117,7 +119,7 @@ CFDB_HD double cell_geometry(const Lattice& L, int64_t x, int64_t y, int64_t z, 
     const Face fg = face_of(fc, mode);
     const P3 good = dot(fg.normal, sub(fg.center, cc)) >= 0.0 ? fg.normal : neg(fg.normal);
     const P3 uns = (f == 0 || f == 1 || f == 4 || f == 5) ? neg(fg.normal) : fg.normal;
-    CellFace& o = out[f];
+    CellFace o;
     o.uns = uns;
     o.good = good;
     o.area = fg.area;
@@ -148,6 +150,7 @@ CFDB_HD double cell_geometry(const Lattice& L, int64_t x, int64_t y, int64_t z, 
     const double alpha = 1.0 / cos_phi;
     o.alpha = interior ? fabs(alpha / nrm(d)) : fabs(alpha / (nrm(d) * 2.0));
     o.len = nrm(sub(fg.center, cc));
+    face(f, o);
   }
   *boundary = bnd;
   return vol / 3.0;

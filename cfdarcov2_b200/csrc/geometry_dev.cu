@@ -24,13 +24,9 @@ __global__ void __launch_bounds__(128) plain_geometry_k(Lattice L, int mode, T* 
   auto center_of = [&](int64_t x, int64_t y, int64_t z) { return L.center(x, y, z); };
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
     const int64_t x = i / plane, r = i - x * plane, y = r / L.nz, z = r - y * L.nz;
-    CellFace fs[6];
     bool bnd = false;
-    const double vol = cfdb_geom::cell_geometry(L, x, y, z, mode, center_of, fs, &bnd);
-#pragma unroll
-    for (int f = 0; f < 6; ++f) {
+    auto store = [&](int f, const CellFace& o) {
       const int64_t k6 = int64_t(f) * n + i;
-      const CellFace& o = fs[f];
       normal[k6] = T(o.uns.x);
       normal[6 * n + k6] = T(o.uns.y);
       normal[12 * n + k6] = T(o.uns.z);
@@ -41,7 +37,8 @@ __global__ void __launch_bounds__(128) plain_geometry_k(Lattice L, int mode, T* 
       alpha[k6] = T(o.alpha);
       len[k6] = T(o.len);
       if (ids) ids[k6] = int32_t(o.id);
-    }
+    };
+    const double vol = cfdb_geom::cell_geometry(L, x, y, z, mode, center_of, store, &bnd);
     volume[i] = T(vol);
     isb[i] = T(bnd ? 1.0 : 0.0);
   }
@@ -102,11 +99,8 @@ struct FaceSample {
 __device__ __forceinline__ void sample_cell(const Lattice& L, int64_t x, int64_t y, int64_t z, int mode,
                                             FaceSample* s) {
   auto center_of = [&](int64_t a, int64_t b, int64_t c) { return L.center(a, b, c); };
-  CellFace fs[6];
   bool bnd = false;
-  s->volume = float(cfdb_geom::cell_geometry(L, x, y, z, mode, center_of, fs, &bnd));
-  for (int f = 0; f < 6; ++f) {
-    const CellFace& o = fs[f];
+  auto store = [&](int f, const CellFace& o) {
     s->normal[f] = float(o.uns.x);
     s->normal[6 + f] = float(o.uns.y);
     s->normal[12 + f] = float(o.uns.z);
@@ -116,7 +110,8 @@ __device__ __forceinline__ void sample_cell(const Lattice& L, int64_t x, int64_t
     s->area[f] = float(o.area);
     s->alpha[f] = float(o.alpha);
     s->len[f] = float(o.len);
-  }
+  };
+  s->volume = float(cfdb_geom::cell_geometry(L, x, y, z, mode, center_of, store, &bnd));
 }
 
 // the first and the last cell: between them every slot is seen once as a
@@ -134,21 +129,21 @@ __global__ void __launch_bounds__(128) lattice_check_k(Lattice L, int mode, cfdb
   auto center_of = [&](int64_t a, int64_t b, int64_t cz) { return L.center(a, b, cz); };
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
     const int64_t x = i / plane, r = i - x * plane, y = r / L.nz, z = r - y * L.nz;
-    CellFace fs[6];
     bool bnd = false;
-    const double vol = cfdb_geom::cell_geometry(L, x, y, z, mode, center_of, fs, &bnd);
-    bool ok = same(float(vol), c.volume);
-    const bool wall[6] = {z == 0, z == L.nz - 1, y == 0, y == L.ny - 1, x == 0, x == L.nx - 1};
-    const int64_t step[6] = {-1, 1, -L.nz, L.nz, -plane, plane};
-    for (int f = 0; f < 6; ++f) {
-      const CellFace& o = fs[f];
-      const int w = wall[f] ? 1 : 0;
+    bool ok = true;
+    auto check = [&](int f, const CellFace& o) {
+      const bool wall = f == 0 ? z == 0 : f == 1 ? z == L.nz - 1 : f == 2 ? y == 0 : f == 3 ? y == L.ny - 1
+                      : f == 4 ? x == 0 : x == L.nx - 1;
+      const int64_t step = f == 0 ? -1 : f == 1 ? 1 : f == 2 ? -L.nz : f == 3 ? L.nz : f == 4 ? -plane : plane;
+      const int w = wall ? 1 : 0;
       ok = ok && same(float(o.uns.x), c.normal[f]) && same(float(o.uns.y), c.normal[6 + f]) &&
            same(float(o.uns.z), c.normal[12 + f]) && same(float(o.good.x), c.normal_alt[f]) &&
            same(float(o.good.y), c.normal_alt[6 + f]) && same(float(o.good.z), c.normal_alt[12 + f]) &&
            same(float(o.area), c.area[f]) && same(float(o.alpha), c.alpha[w * 6 + f]) &&
-           same(float(o.len), c.len[w * 6 + f]) && o.id == (w ? i : i + step[f]);
-    }
+           same(float(o.len), c.len[w * 6 + f]) && o.id == (w ? i : i + step);
+    };
+    const double vol = cfdb_geom::cell_geometry(L, x, y, z, mode, center_of, check, &bnd);
+    ok = ok && same(float(vol), c.volume);
     if (!ok) atomicOr(bad, 1);
   }
 }
