@@ -2,12 +2,17 @@
 
 The product is libcfdb.so (C ABI in include/cfdb.h, CUDA kernels for
 sm_100a under csrc/) and the drop-in C++ facade (include/cfdb/).  This Python
-package only binds the C ABI for tests and benchmarks; importing it fails if
-the library has not been built (``python -m cfdarcov2_b200.build``).
+package only binds the C ABI for tests and benchmarks.  It has no other
+implementation: when libcfdb.so is present it is loaded at import, and when
+it is not (a fresh checkout, before ``python -m cfdarcov2_b200.build``, which
+itself imports this package) every call into the library raises ImportError.
 """
+import os as _os
+
 from . import capi  # noqa: F401
 from .capi import F32, F64, FUSED, PLAIN, CfdbError, lib  # noqa: F401
 
-lib()  # fail loudly at import time when the CUDA library is missing
+if _os.path.exists(capi.LIB_PATH):
+    lib()  # load (and bind) the CUDA library now; a broken build fails here
 
 from .api import Batch, Context, Euler, Mesh, revolve_plan, write_mesh_json, write_vti  # noqa: E402,F401

@@ -27,6 +27,7 @@ def oracle():
 @pytest.fixture(scope="session")
 def cfdb():
     import cfdarcov2_b200
+    cfdarcov2_b200.lib()  # fails loudly when libcfdb.so is not built
     return cfdarcov2_b200
 
 
