@@ -6,6 +6,7 @@
 // its six faces from both sides, so no scatter or atomics are needed.  Uses
 // the volume-scaled adjoint lt = lam / V (R(N) carries 1/V_N).  The same
 // arithmetic on the general geometry is plain_ops.cu's wave_adjoint_plain_k.
+#include "f32x2.cuh"
 #include "tma_host.hpp"
 
 namespace {
@@ -92,6 +93,63 @@ struct AdjPhys {
     o[2] = P[2] + s * au[1];
     o[3] = P[3] + s * au[2];
     a.gc[in.idx] = g0 + s * gg;
+  }
+  // The same update for the thread's two cells at once (the sweep runs two
+  // z cells per thread): every value is a (cell 0, cell 1) pair and every
+  // operation one packed f32x2 instruction, halving the FP32 instruction
+  // count of the issue-bound step.
+  static constexpr bool PAIRED = true;
+  __device__ static void cell2(const stencil::CellIn<FT>& i0, const stencil::CellIn<FT>& i1, const Params& a,
+                               float o0[NF], float o1[NF]) {
+    using namespace f2;
+    auto pr = [](float u, float v) { return make_float2(u, v); };
+    float2 P[FT];
+#pragma unroll
+    for (int f = 0; f < FT; ++f) P[f] = pr(i0.P[f], i1.P[f]);
+    const float2 cP = P[8];
+    float2 ap = splat(0.f), au[3] = {splat(0.f), splat(0.f), splat(0.f)}, gq = splat(0.f), gw = splat(0.f);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      float2 M[FT], N[FT];
+#pragma unroll
+      for (int f = 0; f < FT; ++f) {
+        M[f] = pr(i0.nb[2 * d][f], i1.nb[2 * d][f]);
+        N[f] = pr(i0.nb[2 * d + 1][f], i1.nb[2 * d + 1][f]);
+      }
+      const float2 A4 = splat(a.A4[d]), A2 = splat(a.A2[d]);
+      float2 w = splat(0.f);
+#pragma unroll
+      for (int side = 0; side < 2; ++side) {
+        const float2* X = side ? N : M;
+        const float2 h = mul(A4, add(cP, X[8]));
+        const float2 dl0 = sub(X[0], P[0]), dl1 = sub(X[1], P[1]), dl2 = sub(X[2], P[2]), dl3 = sub(X[3], P[3]);
+        const float2 dq0 = sub(X[4], P[4]), dq1 = sub(X[5], P[5]), dq2 = sub(X[6], P[6]), dq3 = sub(X[7], P[7]);
+        ap = fma(h, dl0, ap);
+        au[0] = fma(h, dl1, au[0]);
+        au[1] = fma(h, dl2, au[1]);
+        au[2] = fma(h, dl3, au[2]);
+        w = add(w, add(fma(dq1, dl1, mul(dq0, dl0)), fma(dq3, dl3, mul(dq2, dl2))));
+      }
+      ap = fma(A2, sub(N[1 + d], M[1 + d]), ap);
+      au[d] = fma(A2, sub(mul(mul(N[8], N[8]), N[0]), mul(mul(M[8], M[8]), M[0])), au[d]);
+      gq = fma(splat(a.A[d]), sub(N[5 + d], M[5 + d]), gq);
+      gw = fma(A4, w, gw);
+    }
+    const float2 gg = sub(neg(mul(mul(cP, P[0]), gq)), gw);
+    const float2 s = splat(a.dt * a.iV);
+    const float2 r0 = fma(s, ap, P[0]), r1 = fma(s, au[0], P[1]), r2 = fma(s, au[1], P[2]), r3 = fma(s, au[2], P[3]);
+    const float2 gn = fma(s, gg, pr(i0.pre, i1.pre));
+    o0[0] = r0.x; o1[0] = r0.y;
+    o0[1] = r1.x; o1[1] = r1.y;
+    o0[2] = r2.x; o1[2] = r2.y;
+    o0[3] = r3.x; o1[3] = r3.y;
+    // the two cells are consecutive in z: one 8-byte store (idx even: z tiles start at multiples of 2)
+    if ((i0.idx & 1) == 0) {
+      *reinterpret_cast<float2*>(a.gc + i0.idx) = gn;
+    } else {
+      a.gc[i0.idx] = gn.x;
+      a.gc[i1.idx] = gn.y;
+    }
   }
   __device__ static void acc_init(Acc&) {}
   __device__ static void acc_cell(Acc&, const float*, const Params&) {}

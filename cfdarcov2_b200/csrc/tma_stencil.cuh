@@ -128,6 +128,11 @@ template <class P> struct derived_count<P, decltype(void(P::ND))> { static const
 // cells once, instead of two one-sided evaluations per face.
 template <class P, class = void> struct is_face_flux { static constexpr bool value = false; };
 template <class P> struct is_face_flux<P, decltype(void(P::FACE_FLUX))> { static constexpr bool value = P::FACE_FLUX; };
+// Paired physics (Phys::PAIRED): with two cells per thread (VZ == 2) the sweep
+// calls Phys::cell2(in0, in1, params, o0, o1) once instead of cell() twice, so
+// the physics can advance both cells with packed FP32 pairs (f32x2.cuh).
+template <class P, class = void> struct is_paired { static constexpr bool value = false; };
+template <class P> struct is_paired<P, decltype(void(P::PAIRED))> { static constexpr bool value = P::PAIRED; };
 
 // Phys provides:
 //   static constexpr int NF, NA;        state fields (read and written), auxiliary fields (read)
@@ -196,6 +201,7 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
   constexpr int NDA = ND > 0 ? ND : 1;  // array extent
   constexpr bool FF = is_face_flux<Phys>::value;
   constexpr bool PRE = has_pre<Phys>::value;
+  constexpr bool PAIR = is_paired<Phys>::value && VZ == 2;
   using L = Layout<TZ, TY, S, NF, NA, Phys::HAS_C, VZ, ND>;
   constexpr int FT = L::FT;
   // Indexing the extern array directly keeps the accesses in the shared
@@ -497,9 +503,10 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
           for (int f = 0; f < NF; ++f) res[f][j] = o[f];
         }
       } else {
+      CellIn<FT, ND> ins[VZ];
 #pragma unroll
       for (int j = 0; j < VZ; ++j) {
-        CellIn<FT, ND> in;
+        CellIn<FT, ND>& in = ins[j];
 #pragma unroll
         for (int f = 0; f < FT; ++f) {
           in.P[f] = cur[f][j];
@@ -536,11 +543,24 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
         in.walls = w;
         in.idx = (long long)x * plane + (long long)y * g.Z + zb + j;
         if constexpr (PRE) in.pre = preC[j];
-        float o[NF];
-        Phys::cell(in, P, o);
-        Phys::acc_cell(acc, o, P);
+        if constexpr (!PAIR) {
+          float o[NF];
+          Phys::cell(in, P, o);
+          Phys::acc_cell(acc, o, P);
 #pragma unroll
-        for (int f = 0; f < NF; ++f) res[f][j] = o[f];
+          for (int f = 0; f < NF; ++f) res[f][j] = o[f];
+        }
+      }
+      if constexpr (PAIR) {
+        float o0[NF], o1[NF];
+        Phys::cell2(ins[0], ins[1], P, o0, o1);
+        Phys::acc_cell(acc, o0, P);
+        Phys::acc_cell(acc, o1, P);
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+          res[f][0] = o0[f];
+          res[f][1] = o1[f];
+        }
       }
       }
       const long long idx = (long long)x * plane + (long long)y * g.Z + zb;
