@@ -445,6 +445,22 @@ def _line(args, workload, value, ms_per_step, cfg, alg_bytes_per_update, updates
     print(json.dumps(line), flush=True)
 
 
+def _cpu_baseline(fn, cells_per_call, sample, budget_s=4.0, max_calls=40):
+    """cpu_baseline of a secondary line: the CPU restatement (oracle) timed on
+    all host threads on a bounded sample of the workload.  fn() runs one call
+    and returns its seconds (or None: wall time is used); cells_per_call =
+    cell-updates one call performs."""
+    from oracle import oracle as O
+    secs, calls = 0.0, 0
+    while secs < budget_s and calls < max_calls:
+        t0 = time.perf_counter()
+        r = fn()
+        secs += r if isinstance(r, float) else time.perf_counter() - t0
+        calls += 1
+    return {"value": cells_per_call * calls / secs, "unit": "cell-updates/s", "cores": O.max_threads(), "kind": "port",
+            "sample": f"{calls} x ({sample})"}
+
+
 def run_secondary(args):
     import numpy as np
     import torch
@@ -495,6 +511,10 @@ def run_secondary(args):
                                            "unit": "GB/s", "frac": ach / peak, "ms_per_step": msb,
                                            "cell_updates_per_s": nb ** 3 / (msb * 1e-3)}
             del mb, Tl, al, bl
+            from oracle import oracle as O
+            oc = O.Mesh(n, n, n, cfg["dx"], cfg["dx"], cfg["dx"], dtype=np.float32)
+            extra["cpu_baseline"] = _cpu_baseline(lambda: oc.heat_time(cfg["T0"], cfg["k"], cfg["dt"], 10, faithful=True),
+                                                  n ** 3 * 10, f"{n}^3 heat, 10 steps, FP32 operator-by-operator")
         _line(args, "heat3d_64^3_x200_steps", res["fp32_fused"][0], res["fp32_fused"][1],
               {"mesh": [n] * 3, "k": cfg["k"], "dt": cfg["dt"], "time_steps_per_bench_step": T}, 8, n ** 3, T,
               extra, launches=res["fp32_fused"][3])
@@ -515,11 +535,17 @@ def run_secondary(args):
         if args.no_extras:
             res["fp64_plain"] = res["fp32_fused"]
         err = l2(res["fp32_fused"][2], res["fp64_plain"][2])
+        cpu = {}
+        if not args.no_extras:
+            from oracle import oracle as O
+            oc = O.Mesh(n, n, n, cfg["dx"], cfg["dx"], cfg["dx"], vertices=V, dtype=np.float32)
+            cpu["cpu_baseline"] = _cpu_baseline(lambda: oc.wave_time(cfg["q0"], dt, 2, faithful=True), n ** 3 * 2,
+                                                f"{n}^3 jittered wave, 2 steps, FP32 operator-by-operator")
         _line(args, f"wave3d_rusanov_{n}^3_x{T}_steps_jittered_0.2dx", res["fp32_fused"][0], res["fp32_fused"][1],
               {"mesh": [n] * 3, "jitter": "U(-0.2,0.2) dx, seed 2", "path": "compact area-vector gather"}, 72, n ** 3,
               T, {"fp64_plain": {"value": res["fp64_plain"][0], "unit": "cell-updates/s"},
                   "speedup_fused_fp32_vs_plain_fp64": res["fp32_fused"][0] / res["fp64_plain"][0],
-                  "accuracy_vs_fp64": {"l2_rel": err[0], "linf_rel": err[1]}},
+                  "accuracy_vs_fp64": {"l2_rel": err[0], "linf_rel": err[1]}, **cpu},
               launches=res["fp32_fused"][3], traffic_profile="distorted_sweep_128.txt" if n == 128 else None)
     elif args.workload == "sod":
         from oracle import riemann
@@ -579,6 +605,11 @@ def run_secondary(args):
                                            "peak": peak, "unit": "GB/s", "frac": ach / peak, "ms_per_step": msb,
                                            "cell_updates_per_s": Nb / (msb * 1e-3)}
             del eb, mb, Ub, ab, bb
+            from oracle import oracle as O
+            oc = O.Mesh(nx, ny, nz, cfg["dx"], cfg["dy"], cfg["dz"], dtype=np.float32)
+            extra["cpu_baseline"] = _cpu_baseline(
+                lambda: oc.euler_solve(cfg["U0"], cfg["gamma"], cfg["cfl"], cfg["t_end"], max_steps=4, want_totals=False),
+                N * 4, f"{nx}x{ny}x{nz} Sod, first 4 steps, FP32 per-cell Rusanov")
         _line(args, "sod_512x64x64_rusanov_to_t0.2", res["fp32_fused"][0], res["fp32_fused"][1],
               {"mesh": [nx, ny, nz], "gamma": 1.4, "cfl": 0.4, "t_end": 0.2, "time_steps": steps}, 40, N, steps,
               extra, launches=res["fp32_fused"][5], traffic_profile="euler_sweep_sod.txt")
@@ -595,11 +626,30 @@ def run_secondary(args):
         ms = _timed(lambda: b.run(a, c, T, use_graph=not args.eager), K, Wm, flush, prep=lambda: a.copy_(pool0),
                     ctx=ctx)
         ens_launches = LAUNCHES["last"]
+        cpu = {}
+        if not args.no_extras:  # every 16th problem, 2 steps each
+            from oracle import oracle as O
+            sub = probs[::16]
+            meshes = [(O.Mesh(p["n"], p["n"], p["n"], 1 / p["n"], 1 / p["n"], 1 / p["n"], dtype=np.float32), p)
+                      for p in sub]
+            init = W.ensemble_initial(probs, b.offsets, b.pool_elems)
+
+            def run_sample():
+                t = 0.0
+                for (om, p), k in zip(meshes, range(0, len(probs), 16)):
+                    off, nn = int(b.offsets[k]), p["n"] ** 3
+                    if p["kind"] == 0:
+                        t += om.heat_time(init[off:off + nn], p["param"], p["dt"], 2, faithful=True)
+                    else:
+                        t += om.wave_time(init[off:off + 4 * nn], p["dt"], 2, cconst=p["param"], faithful=True)
+                return t
+            cpu["cpu_baseline"] = _cpu_baseline(run_sample, 2 * sum(p["n"] ** 3 for p in sub),
+                                                f"{len(sub)} of the {len(probs)} problems, 2 steps each, FP32")
         _line(args, "ensemble_512_cubes_n16-96_x300_steps", cells * T * K / (ms * 1e-3), ms / K,
               {"problems": len(probs), "cells": cells, "time_steps_per_bench_step": T,
                "heat": sum(1 for p in probs if p["kind"] == 0), "wave": sum(1 for p in probs if p["kind"] == 1),
                "tuned_config": list(b.get_config())}, alg / cells, cells, T,
-              {"launches_per_step": b.launch_count() // T}, launches=ens_launches,
+              {"launches_per_step": b.launch_count() // T, **cpu}, launches=ens_launches,
               traffic_profile="ensemble_batch_512.txt")
     elif args.workload == "adjoint":
         cfg = W.adjoint_config(n=args.n, steps=args.tsteps or 400)
@@ -627,6 +677,11 @@ def run_secondary(args):
         fd = (ctx.wave_objective(m, q64, c64 + eps * d, t64, T, dt, path=cfdb.PLAIN)
               - ctx.wave_objective(m, q64, c64 - eps * d, t64, T, dt, path=cfdb.PLAIN)) / (2 * eps)
         adj = float(torch.dot(g_c.double(), d))
+        from oracle import oracle as O
+        oc = O.Mesh(n, n, n, 1 / n, 1 / n, 1 / n, dtype=np.float32)
+        tgt_h = tgt.cpu().numpy()
+        cpu = _cpu_baseline(lambda: oc.wave_gradient(cfg["q0"], cfg["c"], tgt_h, dt, 4), 2 * n ** 3 * 4,
+                            f"{n}^3 wave gradient over 4 steps (forward + adjoint), FP32", max_calls=20)
         _line(args, f"wave_adjoint_{n}^3_x{T}_steps", 2 * n ** 3 * T * K / (ms_grad * 1e-3), ms_grad / K,
               {"mesh": [n] * 3, "time_steps": T, "snapshots": T, "c": "exp(0.2 g), g Gaussian random field, seed 5"},
               60, n ** 3, T,
@@ -634,7 +689,8 @@ def run_secondary(args):
                "reverse_over_forward_sweep": st.reverse_ms / st.forward_ms,
                "forward_solve_ms": ms_fwd / K, "gradient_ms": ms_grad / K,
                "grad_rel_err_vs_fd": abs(adj - fd) / abs(fd), "fd_eps": eps, "J": J,
-               "note": "value counts forward + adjoint cell-updates; roofline uses the adjoint sweep's 60 B/cell"},
+               "note": "value counts forward + adjoint cell-updates; roofline uses the adjoint sweep's 60 B/cell",
+               "cpu_baseline": cpu},
               launches=grad_launches, traffic_profile="adjoint_sweep_128.txt" if n == 128 else None)
 
 
