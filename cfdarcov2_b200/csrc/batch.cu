@@ -41,7 +41,8 @@ struct ProbDev {
 // four planes ahead into L2 gained nothing and added DRAM reads; loading
 // plane x + 2 into registers one iteration early (two planes in flight per
 // warp) was 8 % slower (items of the tuned size march only 8 planes); two
-// heat columns per thread (two independent load chains) changed nothing.
+// heat columns per thread (two independent load chains) changed nothing, nor
+// did fetching the next item's descriptors while the current item marches.
 struct ItemDev {
   int32_t prob;
   int32_t yz0;
