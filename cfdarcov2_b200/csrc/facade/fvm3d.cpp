@@ -96,7 +96,10 @@ Mesh3D::~Mesh3D() {
 
 void Mesh3D::init_basic_internals() {}
 
-void Mesh3D::compute() { handle(); }
+void Mesh3D::compute() {
+  cfdb_lattice_geometry lat{};
+  check(cfdb_mesh_lattice_geometry(handle(), &lat), "cfdb_mesh_lattice_geometry");  // cached in the mesh
+}
 
 cfdb_mesh* Mesh3D::handle() {
   if (!mesh_)

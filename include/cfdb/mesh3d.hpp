@@ -47,8 +47,12 @@ class Mesh3D {
   Mesh3D(const Mesh3D&) = delete;
   Mesh3D& operator=(const Mesh3D&) = delete;
 
-  // The reference builds object graphs here; the library builds its geometry
-  // lazily, so these only create the library mesh (src/mesh3d.cpp:151-385).
+  // The reference builds object graphs and computes every face's geometry
+  // here (src/mesh3d.cpp:151-385).  init_basic_internals() does nothing;
+  // compute() creates the library mesh and settles, on the GPU, whether it
+  // is an exact lattice (cfdb_mesh_lattice_geometry), so that geometry work
+  // happens before Equation::evaluate as in the reference.  Face arrays are
+  // built on the device when an operator first needs them.
   void init_basic_internals();
   void compute();
 
