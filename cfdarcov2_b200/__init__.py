@@ -15,4 +15,5 @@ from .capi import F32, F64, FUSED, PLAIN, CfdbError, lib  # noqa: F401
 if _os.path.exists(capi.LIB_PATH):
     lib()  # load (and bind) the CUDA library now; a broken build fails here
 
-from .api import Batch, Context, Euler, Mesh, revolve_plan, write_mesh_json, write_vti  # noqa: E402,F401
+from .api import (Batch, Context, Euler, Mesh, load_state, revolve_plan, save_state,  # noqa: E402,F401
+                  write_mesh_json, write_vti)

@@ -13,7 +13,8 @@ import numpy as np
 from . import capi
 from .capi import F32, F64, FUSED, PLAIN, call, lib
 
-__all__ = ["Context", "Mesh", "Euler", "Batch", "F32", "F64", "PLAIN", "FUSED", "write_vti", "write_mesh_json"]
+__all__ = ["Context", "Mesh", "Euler", "Batch", "F32", "F64", "PLAIN", "FUSED", "write_vti", "write_mesh_json",
+           "save_state", "load_state"]
 
 
 def _ptr(t):
@@ -418,3 +419,24 @@ def write_mesh_json(path, nx, ny, nz, dx, dy, dz, vertices=None):
             raise ValueError("vertices do not match the mesh size")
         ptr = vertices.ctypes.data_as(C.c_void_p)
     call("cfdb_write_mesh_json", os.fsencode(path), int(nx), int(ny), int(nz), float(dx), float(dy), float(dz), ptr)
+
+
+def save_state(path, values, nx, ny, nz, fields, step=0, t=0.0):
+    """Checkpoint (cfdb_state_save) of host data holding `fields` x n values
+    in field order; float32 or float64 as given."""
+    v = np.ascontiguousarray(np.asarray(values).reshape(-1))
+    if v.dtype not in (np.float32, np.float64) or v.size != fields * nx * ny * nz:
+        raise ValueError("values must be float32 or float64 with fields x nx x ny x nz entries")
+    call("cfdb_state_save", os.fsencode(path), F64 if v.dtype == np.float64 else F32, int(nx), int(ny), int(nz),
+         int(fields), int(step), float(t), v.ctypes.data_as(C.c_void_p))
+
+
+def load_state(path, nx, ny, nz, fields, dtype=np.float32):
+    """(values, step, t) of a checkpoint written by save_state; the dtype,
+    dimensions and field count must match the file's."""
+    dt = np.dtype(dtype)
+    out = np.empty(fields * nx * ny * nz, dt)
+    step, t = C.c_int64(), C.c_double()
+    call("cfdb_state_load", os.fsencode(path), F64 if dt == np.float64 else F32, int(nx), int(ny), int(nz),
+         int(fields), C.byref(step), C.byref(t), out.ctypes.data_as(C.c_void_p))
+    return out, step.value, t.value

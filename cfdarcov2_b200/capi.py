@@ -80,6 +80,8 @@ PROTOTYPES = {
     "cfdb_mesh_lattice_geometry": (_I, [_P, _P]),
     "cfdb_write_vti": (_I, [C.c_char_p, C.c_char_p, _I64, _I64, _I64, _P]),
     "cfdb_write_mesh_json": (_I, [C.c_char_p, _I64, _I64, _I64, _D, _D, _D, _P]),
+    "cfdb_state_save": (_I, [C.c_char_p, _I, _I64, _I64, _I64, _I32, _I64, _D, _P]),
+    "cfdb_state_load": (_I, [C.c_char_p, _I, _I64, _I64, _I64, _I32, _PI64, _PD, _P]),
     "cfdb_alloc": (_I, [_P, _I64, _PP]),
     "cfdb_free": (_I, [_P, _P]),
     "cfdb_upload": (_I, [_P, _P, _P, _I64]),

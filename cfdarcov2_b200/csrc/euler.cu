@@ -360,6 +360,14 @@ extern "C" int cfdb_euler_run(cfdb_euler* e, void* Ua, void* Ub, int64_t check_e
       if (int rc = cfdb_euler_step(e, even ? Ua : Ub, even ? Ub : Ua)) return rc;
     }
     if (int rc = cfdb_euler_status(e, nullptr, &steps, &finished)) return rc;
+    // the conservation totals of the latest step double as the health check:
+    // a NaN or Inf anywhere in the state reaches them (and would otherwise
+    // end the run early through a non-finite dt)
+    double last[2] = {0.0, 0.0};
+    CFDB_CUDA(e->ctx, cudaMemcpy(last, e->totals + 2 * steps, sizeof(last), cudaMemcpyDeviceToHost));
+    if (!std::isfinite(last[0]) || !std::isfinite(last[1]))
+      return cfdb_fail(e->ctx, CFDB_ENUMERIC, "cfdb_euler_run: the state is not finite at step %lld (totals %g, %g)",
+                       (long long)steps, last[0], last[1]);
     if (!finished && e->launches > e->max_steps + check_every)
       return cfdb_fail(e->ctx, CFDB_ENUMERIC, "cfdb_euler_run: the clock did not reach t_end within max_steps");
   }

@@ -173,3 +173,85 @@ extern "C" int cfdb_write_mesh_json(const char* path, int64_t nx, int64_t ny, in
           double(float(dy) * float(Y)), double(float(dz) * float(Z)));
   return close_out(file, path, fn);
 }
+
+// ---- checkpoints -------------------------------------------------------------
+// Header (little-endian, 64 bytes): magic "CFDBCKPT", u32 version, i32 dtype,
+// i64 nx, ny, nz, i32 fields, i32 reserved, i64 step, f64 t; then fields x n
+// values of the dtype in field order and reference cell order.
+namespace {
+constexpr char kCkptMagic[8] = {'C', 'F', 'D', 'B', 'C', 'K', 'P', 'T'};
+constexpr uint32_t kCkptVersion = 1;
+
+struct CkptHeader {
+  char magic[8];
+  uint32_t version;
+  int32_t dtype;
+  int64_t nx, ny, nz;
+  int32_t fields, reserved;
+  int64_t step;
+  double t;
+};
+static_assert(sizeof(CkptHeader) == 64, "checkpoint header is 64 bytes");
+
+int ckpt_args(const char* fn, int dtype, int64_t nx, int64_t ny, int64_t nz, int32_t fields, const void* data) {
+  if (!data || !dims_ok(nx, ny, nz) || fields < 1 || fields > 64 || (dtype != CFDB_F32 && dtype != CFDB_F64))
+    return cfdb_fail(nullptr, CFDB_EINVAL, "%s: bad dtype, dimensions, field count or NULL data", fn);
+  return CFDB_OK;
+}
+}  // namespace
+
+extern "C" int cfdb_state_save(const char* path, int dtype, int64_t nx, int64_t ny, int64_t nz, int32_t fields,
+                               int64_t step, double t, const void* host_data) {
+  const char* fn = "cfdb_state_save";
+  if (int rc = ckpt_args(fn, dtype, nx, ny, nz, fields, host_data)) return rc;
+  CkptHeader h{};
+  std::memcpy(h.magic, kCkptMagic, 8);
+  h.version = kCkptVersion;
+  h.dtype = dtype;
+  h.nx = nx; h.ny = ny; h.nz = nz;
+  h.fields = fields;
+  h.step = step;
+  h.t = t;
+  const size_t bytes = size_t(fields) * size_t(nx * ny * nz) * (dtype == CFDB_F64 ? 8 : 4);
+  // written to a temporary name and renamed, so an interrupted save never
+  // leaves a truncated checkpoint under the final name
+  const std::string tmp = std::string(path ? path : "") + ".tmp";
+  File file;
+  if (int rc = open_out(file, path ? tmp.c_str() : nullptr, fn)) return rc;
+  fwrite(&h, sizeof(h), 1, file.f);
+  fwrite(host_data, 1, bytes, file.f);
+  if (int rc = close_out(file, tmp.c_str(), fn)) {
+    std::remove(tmp.c_str());
+    return rc;
+  }
+  if (std::rename(tmp.c_str(), path) != 0) {
+    std::remove(tmp.c_str());
+    return cfdb_fail(nullptr, CFDB_EIO, "%s: cannot rename %s to %s: %s", fn, tmp.c_str(), path, strerror(errno));
+  }
+  return CFDB_OK;
+}
+
+extern "C" int cfdb_state_load(const char* path, int dtype, int64_t nx, int64_t ny, int64_t nz, int32_t fields,
+                               int64_t* step, double* t, void* host_data) {
+  const char* fn = "cfdb_state_load";
+  if (int rc = ckpt_args(fn, dtype, nx, ny, nz, fields, host_data)) return rc;
+  if (!path || !*path) return cfdb_fail(nullptr, CFDB_EINVAL, "%s: empty path", fn);
+  File file;
+  file.f = fopen(path, "rb");
+  if (!file.f) return cfdb_fail(nullptr, CFDB_EIO, "%s: cannot open %s: %s", fn, path, strerror(errno));
+  CkptHeader h{};
+  if (fread(&h, sizeof(h), 1, file.f) != 1 || std::memcmp(h.magic, kCkptMagic, 8) != 0 || h.version != kCkptVersion)
+    return cfdb_fail(nullptr, CFDB_EIO, "%s: %s is not a version-%u checkpoint", fn, path, kCkptVersion);
+  if (h.dtype != dtype || h.nx != nx || h.ny != ny || h.nz != nz || h.fields != fields)
+    return cfdb_fail(nullptr, CFDB_EINVAL,
+                     "%s: %s holds dtype %d, %lld x %lld x %lld cells, %d fields; asked for dtype %d, "
+                     "%lld x %lld x %lld, %d fields",
+                     fn, path, h.dtype, (long long)h.nx, (long long)h.ny, (long long)h.nz, h.fields, dtype,
+                     (long long)nx, (long long)ny, (long long)nz, fields);
+  const size_t bytes = size_t(fields) * size_t(nx * ny * nz) * (dtype == CFDB_F64 ? 8 : 4);
+  if (fread(host_data, 1, bytes, file.f) != bytes)
+    return cfdb_fail(nullptr, CFDB_EIO, "%s: %s is truncated", fn, path);
+  if (step) *step = h.step;
+  if (t) *t = h.t;
+  return CFDB_OK;
+}

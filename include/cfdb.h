@@ -296,7 +296,9 @@ int cfdb_euler_status(cfdb_euler* e, double* t, int64_t* steps_done, int* finish
 /* Synchronous: totals rows (2 doubles each: sum rho V, sum E V), row 0 = initial state. */
 int cfdb_euler_totals(cfdb_euler* e, double* out, int64_t max_rows, int64_t* rows);
 /* Runs to t_end alternating U_a -> U_b -> U_a ..., checking the clock every
- * check_every steps; *final_in_b = 1 when the last state is in U_b. */
+ * check_every steps; *final_in_b = 1 when the last state is in U_b.  At each
+ * check a non-finite conservation total (a NaN or Inf in the state) stops
+ * the run with CFDB_ENUMERIC. */
 int cfdb_euler_run(cfdb_euler* e, void* U_a, void* U_b, int64_t check_every, int64_t* steps_done,
                    int* final_in_b);
 
@@ -469,6 +471,21 @@ int cfdb_write_vti(const char* path, const char* name, int64_t nx, int64_t ny, i
  * the vertex numbering, or NULL for the uniform lattice of spacing dx, dy, dz. */
 int cfdb_write_mesh_json(const char* path, int64_t nx, int64_t ny, int64_t nz, double dx, double dy, double dz,
                          const double* vertices);
+
+/* Checkpoint and resume of a solver state (host memory).  No counterpart in
+ * the reference, which keeps history in RAM and whose raw stepping writer
+ * (include/io_operators_tmpl.hpp:131-159) has no header and no reader: here
+ * the file carries a 64-byte header (magic, version, dtype, nx/ny/nz, field
+ * count, step, t) and then the `fields` x n values in field order and the
+ * reference's cell order.  save writes a temporary file and renames it, so
+ * an interrupted save leaves no truncated checkpoint; load fails with
+ * CFDB_EINVAL when dtype, dimensions or field count differ from the file's
+ * and with CFDB_EIO for a missing, foreign or truncated file.  Errors go to
+ * cfdb_last_error(NULL). */
+int cfdb_state_save(const char* path, int dtype, int64_t nx, int64_t ny, int64_t nz, int32_t fields, int64_t step,
+                    double t, const void* host_data);
+int cfdb_state_load(const char* path, int dtype, int64_t nx, int64_t ny, int64_t nz, int32_t fields, int64_t* step,
+                    double* t, void* host_data);
 
 #ifdef __cplusplus
 }

@@ -93,3 +93,40 @@ def test_mesh_json_takes_given_vertices(cfdb, tmp_path):
     cfdb.write_mesh_json(p, n, n, n, 1 / n, 1 / n, 1 / n, Vx)
     V = np.array(json.loads(p.read_text())["vertexes"])
     assert np.allclose(V, np.asarray(Vx).reshape(-1, 3).astype(np.float32), rtol=0, atol=1e-7)
+
+
+@pytest.mark.parametrize("dtype,fields", [(np.float32, 4), (np.float64, 5), (np.float32, 1)])
+def test_checkpoint_round_trip(cfdb, tmp_path, dtype, fields):
+    """cfdb_state_save / cfdb_state_load: values, step and time come back
+    exactly; no temporary file is left behind."""
+    nx, ny, nz = 5, 3, 4
+    rng = np.random.default_rng(21)
+    v = rng.standard_normal(fields * nx * ny * nz).astype(dtype)
+    p = tmp_path / "state.ckpt"
+    cfdb.save_state(p, v, nx, ny, nz, fields, step=123, t=0.0625)
+    got, step, t = cfdb.load_state(p, nx, ny, nz, fields, dtype=dtype)
+    assert np.array_equal(got, v) and step == 123 and t == 0.0625
+    assert sorted(q.name for q in tmp_path.iterdir()) == ["state.ckpt"]
+    assert p.stat().st_size == 64 + v.nbytes
+
+
+def test_checkpoint_rejects_mismatch_and_damage(cfdb, tmp_path):
+    cap = cfdb.capi
+    nx, ny, nz = 4, 4, 4
+    v = np.arange(2 * nx * ny * nz, dtype=np.float32)
+    p = tmp_path / "s.ckpt"
+    cfdb.save_state(p, v, nx, ny, nz, 2, step=7, t=1.5)
+    for args in [(nx, ny, nz, 3, np.float32), (nx, ny, 8, 2, np.float32), (nx, ny, nz, 2, np.float64)]:
+        with pytest.raises(cap.CfdbError) as e:
+            cfdb.load_state(p, *args[:4], dtype=args[4])
+        assert e.value.code == cap.EINVAL
+    data = p.read_bytes()
+    (tmp_path / "short.ckpt").write_bytes(data[:-8])
+    (tmp_path / "foreign.ckpt").write_bytes(b"NOTACKPT" + data[8:])
+    for name in ["short.ckpt", "foreign.ckpt", "missing.ckpt"]:
+        with pytest.raises(cap.CfdbError) as e:
+            cfdb.load_state(tmp_path / name, nx, ny, nz, 2)
+        assert e.value.code == cap.EIO, name
+    with pytest.raises(cap.CfdbError) as e:
+        cfdb.save_state(tmp_path / "no_such_dir" / "x.ckpt", v, nx, ny, nz, 2)
+    assert e.value.code == cap.EIO
