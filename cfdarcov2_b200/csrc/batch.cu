@@ -356,6 +356,7 @@ extern "C" int cfdb_batch_step(cfdb_batch* b, const void* a, void* out) {
 }
 
 extern "C" int cfdb_batch_run(cfdb_batch* b, void* a, void* out, int32_t steps, int use_graph) {
+  CfdbRange range_("cfdb_batch_run");
   if (!b || !b->ctx) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_batch_run: handle is NULL or its context was destroyed");
   if (!a || !out || a == out || steps < 0) return cfdb_fail(b->ctx, CFDB_EINVAL, "cfdb_batch_run: bad arguments");
   CFDB_CUDA(b->ctx, cudaSetDevice(b->ctx->device));

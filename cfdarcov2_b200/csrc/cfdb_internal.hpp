@@ -134,6 +134,19 @@ struct cfdb_mesh {
   cfdb_lattice_geometry lattice{};
 };
 
+// ---- tracing -----------------------------------------------------------------
+// An NVTX range over a library call (the reference times Equation::evaluate
+// with std::chrono only, examples/main_3d_heat.cpp:96-99): profilers and
+// timeline tools show each run / build / gradient phase by name.  NVTX 3 is
+// header-only; without a tool attached a range costs a few nanoseconds.
+#include <nvtx3/nvToolsExt.h>
+struct CfdbRange {
+  explicit CfdbRange(const char* name) { nvtxRangePushA(name); }
+  ~CfdbRange() { nvtxRangePop(); }
+  CfdbRange(const CfdbRange&) = delete;
+  CfdbRange& operator=(const CfdbRange&) = delete;
+};
+
 // ---- error plumbing --------------------------------------------------------
 int cfdb_fail(cfdb_ctx* ctx, int code, const char* fmt, ...);
 int cfdb_cuda_fail(cfdb_ctx* ctx, cudaError_t e, const char* what);

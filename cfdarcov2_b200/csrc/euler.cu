@@ -348,6 +348,7 @@ extern "C" int cfdb_euler_totals(cfdb_euler* e, double* out, int64_t max_rows, i
 
 extern "C" int cfdb_euler_run(cfdb_euler* e, void* Ua, void* Ub, int64_t check_every, int64_t* steps_done,
                               int* final_in_b) {
+  CfdbRange range_("cfdb_euler_run");
   if (!e || !e->ctx) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_euler_run: handle is NULL or its context was destroyed");
   if (!Ua || !Ub || Ua == Ub || check_every < 1)
     return cfdb_fail(e->ctx, CFDB_EINVAL, "cfdb_euler_run: need distinct buffers and check_every >= 1");

@@ -122,6 +122,7 @@ struct Bufs {
 
 extern "C" int cfdb_wave_objective(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, int path, const void* q0, const void* c,
                                    const void* target, int32_t steps, double dt, double* J_out) {
+  CfdbRange range_("cfdb_wave_objective");
   if (int rc = check_args(ctx, m, dtype, path, q0, c, target, steps, dt, "cfdb_wave_objective")) return rc;
   if (!J_out) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_wave_objective: J_out is NULL");
   Run R{ctx, m, dtype, path, c, dt, dtype_size(dtype), m->n};
@@ -140,6 +141,7 @@ extern "C" int cfdb_wave_objective(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, int p
 extern "C" int cfdb_wave_gradient(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, int path, const void* q0, const void* c,
                                   const void* target, int32_t steps, double dt, int32_t snapshots, double* J_out,
                                   void* grad_c, void* grad_p0, cfdb_gradient_stats* stats) {
+  CfdbRange range_("cfdb_wave_gradient");
   if (int rc = check_args(ctx, m, dtype, path, q0, c, target, steps, dt, "cfdb_wave_gradient")) return rc;
   if (!J_out || !grad_c || !grad_p0) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_wave_gradient: NULL output");
   if (snapshots < 1) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_wave_gradient: snapshots must be >= 1");
@@ -179,12 +181,16 @@ extern "C" int cfdb_wave_gradient(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, int pa
     auto slot = [&](int t) { return static_cast<void*>(states + sb * int64_t(t)); };
     if ((rc = R.copy(slot(0), q0))) return rc;
     cudaEventRecord(e0, ctx->stream);
-    for (int t = 0; t < steps && !rc; ++t) rc = R.step(slot(t), slot(t + 1));
+    {
+      CfdbRange forward("cfdb_wave_gradient: forward sweep");
+      for (int t = 0; t < steps && !rc; ++t) rc = R.step(slot(t), slot(t + 1));
+    }
     cudaEventRecord(e1, ctx->stream);
     if (rc) return rc;
     st.forward_steps = steps;
     st.snapshots_used = steps + 1;
     if ((rc = R.misfit(slot(steps), target, lam, J_out, scratch))) return rc;
+    CfdbRange reverse("cfdb_wave_gradient: reverse sweep");
     for (int t = steps - 1; t >= 0 && !rc; --t) rc = adj(slot(t));
   } else {
     std::vector<int32_t> act, arg, at;

@@ -395,6 +395,7 @@ void cfdb_jit_release(cfdb_ctx* ctx) {
 
 extern "C" int cfdb_kernel_build_many(cfdb_ctx* ctx, int count, const char* const* sources, const char* const* names,
                                       cfdb_kernel** out) {
+  CfdbRange range_("cfdb_kernel_build_many");
   if (!out || count < 0 || (count > 0 && (!sources || !names)))
     return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_kernel_build_many: bad arguments");
   for (int k = 0; k < count; ++k) out[k] = nullptr;

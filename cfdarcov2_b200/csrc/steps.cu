@@ -54,6 +54,7 @@ extern "C" int cfdb_wave_adjoint_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, in
 
 extern "C" int cfdb_heat_run(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, int path, void* Ta, void* Tb, double k, double dt,
                              int32_t steps, int use_graph, int* final_in_b) {
+  CfdbRange range_("cfdb_heat_run");
   if (int rc = check_step(ctx, m, dtype, path, "cfdb_heat_run")) return rc;
   if (!Ta || !Tb || Ta == Tb) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_heat_run: need distinct T_a and T_b");
   if (path == CFDB_PATH_FUSED && dtype == CFDB_F32 && std::isfinite(k) && std::isfinite(dt)) {
@@ -75,6 +76,7 @@ extern "C" int cfdb_heat_run(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, int path, v
 
 extern "C" int cfdb_wave_run(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, int path, void* qa, void* qb, const void* c,
                              double cconst, int mode, double dt, int32_t steps, int use_graph, int* final_in_b) {
+  CfdbRange range_("cfdb_wave_run");
   if (int rc = check_step(ctx, m, dtype, path, "cfdb_wave_run")) return rc;
   if (!qa || !qb || qa == qb) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_wave_run: need distinct q_a and q_b");
   int rc = cfdb_run_steps(
