@@ -94,3 +94,16 @@ def test_wave_dt_matches_oracle_on_vertex_mesh(cfdb, oracle):
     rng = np.random.default_rng(0)
     c = np.exp(0.2 * rng.standard_normal(m.n))
     assert m.wave_dt(0.4, c=c) == pytest.approx(o.wave_dt(0.4, c=c), rel=1e-15)
+
+
+def test_missing_library_fails_loudly(cfdb, monkeypatch, tmp_path):
+    """No fallback: with libcfdb.so absent every entry into the library raises
+    ImportError naming the build command (the package itself still imports,
+    because the build module lives in it)."""
+    cap = cfdb.capi
+    monkeypatch.setattr(cap, "LIB_PATH", str(tmp_path / "libcfdb.so"))
+    monkeypatch.setattr(cap, "_lib", None)
+    with pytest.raises(ImportError, match="cfdarcov2_b200.build"):
+        cap.lib()
+    with pytest.raises(ImportError):
+        cfdb.Mesh.structured(None, 4, 4, 4, 1.0, 1.0, 1.0)
