@@ -91,6 +91,37 @@ def test_heat_conserves_and_decays_cosine_mode(oracle):
     assert np.allclose(amp, expect, rtol=1e-10)
 
 
+def test_d2t_standing_wave_mode(oracle):
+    """The reference's wave scheme (examples/main_3d_wave.cu: d2t(u) =
+    c^2 (d2dx(u) + d2dy(u)), leapfrog after a first d1t-form step) on the
+    standing mode cos(pi x) cos(pi y), the discrete eigenvector of the
+    zero-gradient Laplacian: every step multiplies the mode by the scalar
+    recurrence a' = (2 - w^2 dt^2) a - a_prev (first step a' = (1 - w^2 dt) a),
+    w^2 = c^2 (l_x + l_y), l_d = 2 (1 - cos(pi h)) / h^2; and for small dt
+    the amplitude follows the analytic standing wave, the check the
+    reference ran in reports/compare_gauss_pulse.py:57-116.  The first step
+    in d1t form starts the oscillator with velocity -w^2 (not 0), so the
+    analytic amplitude is cos(w t) - w sin(w t)."""
+    n = 24
+    m = oracle.Mesh(n, n, 4, 1 / n, 1 / n, 0.25)
+    c3 = centers(m)
+    mode = np.cos(np.pi * c3[0]) * np.cos(np.pi * c3[1])
+    c, dt, steps = 0.3, 2e-3, 400
+    h = 1 / n
+    w2 = c * c * 2 * (2 * (1 - np.cos(np.pi * h)) / h ** 2)
+    u, prev = mode.copy(), None
+    a, a_prev = 1.0, None
+    for _ in range(steps):
+        R = c * c * (m.lapl(u, 1) + m.lapl(u, 2))
+        nxt = dt * R + u if prev is None else (dt * dt * R + 2 * u) - prev
+        prev, u = u, nxt
+        a_next = (1 - w2 * dt) * a if a_prev is None else (2 - w2 * dt * dt) * a - a_prev
+        a_prev, a = a, a_next
+    assert np.allclose(u, a * mode, rtol=0, atol=1e-10)  # round-off of 400 leapfrog steps
+    w, t = np.sqrt(w2), steps * dt
+    assert abs(a - (np.cos(w * t) - w * np.sin(w * t))) < 2 * w * dt
+
+
 def test_heat_faithful_equals_fused(oracle):
     m = oracle.Mesh(10, 9, 8, 0.1, 0.1, 0.1)
     rng = np.random.default_rng(0)
