@@ -233,7 +233,8 @@ const float* eval_node(Node* n) {
 
 // Cells per thread of the generated kernels (JitPlan::cells).
 // Measured on the reference's benchmark systems: the single-equation wave
-// kernel 206 -> 308 G cell-updates/s at 4 cells per thread (400^3); the
+// kernel 206 -> 308 G cell-updates/s at 4 cells per thread (400^3; 8 cells
+// per thread fall back to 239 G); the
 // Euler system's group kernels lose with 2 (7.4 -> 6.6 G at 200^3: the
 // 9-member group's registers double) and its stab passes are level.
 constexpr int kCptEquation = 4;
