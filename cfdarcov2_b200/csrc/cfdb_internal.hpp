@@ -134,6 +134,9 @@ struct cfdb_mesh {
   cfdb_lattice_geometry lattice{};
 };
 
+// Device ordinals the per-device caches of kernel attributes cover.
+constexpr int kMaxDevices = 64;
+
 // ---- tracing -----------------------------------------------------------------
 // An NVTX range over a library call (the reference times Equation::evaluate
 // with std::chrono only, examples/main_3d_heat.cpp:96-99): profilers and

@@ -25,6 +25,7 @@
 #include <filesystem>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -243,10 +244,15 @@ struct Module {
 };
 
 // modules of every context, by context and source text (a context owns its
-// modules until it is destroyed)
+// modules until it is destroyed); contexts may live on different host
+// threads, so the table is guarded by modules_mutex()
 std::map<const cfdb_ctx*, std::map<std::string, std::shared_ptr<Module>>>& modules() {
   static std::map<const cfdb_ctx*, std::map<std::string, std::shared_ptr<Module>>> m;
   return m;
+}
+std::mutex& modules_mutex() {
+  static std::mutex mu;
+  return mu;
 }
 
 const char* const kOpts[] = {"--gpu-architecture=sm_100a", "--fmad=false", "--prec-div=true", "--prec-sqrt=true",
@@ -386,6 +392,7 @@ struct cfdb_kernel {
 
 // Releases the modules of a context (called when it is destroyed).
 void cfdb_jit_release(cfdb_ctx* ctx) {
+  std::lock_guard<std::mutex> lock(modules_mutex());
   auto it = modules().find(ctx);
   if (it == modules().end()) return;
   for (auto& kv : it->second)
@@ -403,6 +410,7 @@ extern "C" int cfdb_kernel_build_many(cfdb_ctx* ctx, int count, const char* cons
   for (int k = 0; k < count; ++k)
     if (!sources[k] || !names[k] || !*names[k]) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_kernel_build: NULL argument");
   CFDB_CUDA(ctx, cudaSetDevice(ctx->device));
+  std::lock_guard<std::mutex> lock(modules_mutex());  // held through the build: one context's table at a time
   auto& mine = modules()[ctx];
   // distinct sources without a module in this context: from the disk cache or compiled, in parallel
   std::vector<std::string> todo;

@@ -138,11 +138,8 @@ int heat_resident_run(cfdb_ctx* ctx, cfdb_mesh* m, const void* Ta, void* Tb, dou
     const long long smem = 2 * P * plane * 4;
     if (smem > max_smem) break;  // fewer CTAs only make the slabs larger
     if (P * plane / 4 > (long long)kMaxGroups * kThreads) continue;
-    static bool attr_set = false;
-    if (!attr_set) {
-      CFDB_CUDA(ctx, cudaFuncSetAttribute(heat_resident_k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-      attr_set = true;
-    }
+    // per-device kernel attribute; cheap enough to set on every call
+    CFDB_CUDA(ctx, cudaFuncSetAttribute(heat_resident_k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     CFDB_CUDA(ctx, cudaFuncSetAttribute(heat_resident_k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(CL);

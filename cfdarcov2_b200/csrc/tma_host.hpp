@@ -1,6 +1,7 @@
 // Host side of the TMA stencil sweep: tensor-map encoding through the driver
 // entry point (no libcuda link), tile/chunk selection and the launch.
 #pragma once
+#include <atomic>
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -109,11 +110,17 @@ int launch_sweep(cfdb_ctx* ctx, const cfdb_mesh* m, const void* q, const void* a
     if (int rc = encode_field(ctx, &tc, c, m, TZ, TY)) return rc;
   }
   auto kern = sweep_kernel<Phys, TZ, TY, S, VZ>;
-  static int resident = 0;
+  // the shared-memory attribute is a per-device setting: set it (and measure
+  // the occupancy) once per device and kernel instantiation
+  static std::atomic<int> resident_of[kMaxDevices] = {};
+  if (ctx->device < 0 || ctx->device >= kMaxDevices)
+    return cfdb_fail(ctx, CFDB_EUNSUPPORTED, "device ordinal %d beyond %d", ctx->device, kMaxDevices);
+  int resident = resident_of[ctx->device].load(std::memory_order_acquire);
   if (!resident) {
     CFDB_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L::SMEM_BYTES)));
     CFDB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kern, L::THREADS, L::SMEM_BYTES));
     if (resident < 1) return cfdb_fail(ctx, CFDB_EUNSUPPORTED, "sweep kernel does not fit on an SM");
+    resident_of[ctx->device].store(resident, std::memory_order_release);
   }
   const SweepShape sh = sweep_shape(ctx, m, TZ, TY, ctas_per_sm > 0 ? std::min(ctas_per_sm, resident) : resident);
   Geometry g{int(m->nx), int(m->ny), int(m->nz), sh.chunks, (long long)m->n};
