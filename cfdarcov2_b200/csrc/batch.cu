@@ -19,6 +19,8 @@
 #include <string>
 #include <vector>
 
+#include <unistd.h>
+
 #include "cfdb_internal.hpp"
 
 namespace {
@@ -244,16 +246,27 @@ std::map<std::string, std::vector<int>> read_cache(const char* path) {
   return out;
 }
 
+// Written to a temporary file and renamed into place, so processes tuning
+// at the same time (one per GPU) never leave a torn cache for each other.
 void write_cache(const char* path, const std::map<std::string, std::vector<int>>& m) {
   if (!path) return;
-  std::ofstream f(path);
-  f << "{\n";
-  size_t k = 0;
-  for (const auto& kv : m) {
-    f << "  \"" << kv.first << "\": [" << kv.second[0] << ", " << kv.second[1] << ", " << kv.second[2] << "]"
-      << (++k < m.size() ? ",\n" : "\n");
+  const std::string tmp = std::string(path) + ".tmp" + std::to_string(long(getpid()));
+  {
+    std::ofstream f(tmp);
+    if (!f) return;
+    f << "{\n";
+    size_t k = 0;
+    for (const auto& kv : m) {
+      f << "  \"" << kv.first << "\": [" << kv.second[0] << ", " << kv.second[1] << ", " << kv.second[2] << "]"
+        << (++k < m.size() ? ",\n" : "\n");
+    }
+    f << "}\n";
+    if (!f) {
+      std::remove(tmp.c_str());
+      return;
+    }
   }
-  f << "}\n";
+  if (std::rename(tmp.c_str(), path) != 0) std::remove(tmp.c_str());
 }
 
 }  // namespace
