@@ -76,6 +76,7 @@ PROTOTYPES = {
     "cfdb_kernel_build_many": (_I, [_P, _I, C.POINTER(C.c_char_p), C.POINTER(C.c_char_p), _PP]),
     "cfdb_kernel_launch": (_I, [_P, _I64, _I, _P]),
     "cfdb_kernel_destroy": (_I, [_P]),
+    "cfdb_kernel_info": (_I, [_P, _PI, _PI64, _PI]),
     "cfdb_mesh_plain_geometry": (_I, [_P, _P]),
     "cfdb_mesh_lattice_geometry": (_I, [_P, _P]),
     "cfdb_write_vti": (_I, [C.c_char_p, C.c_char_p, _I64, _I64, _I64, _P]),

@@ -40,6 +40,7 @@ bool CFDArcoGlobalInit::cuda_enabled = false;
 bool CFDArcoGlobalInit::store_stepping = false;
 bool CFDArcoGlobalInit::jit_lattice = true;
 bool CFDArcoGlobalInit::jit_all = true;
+bool CFDArcoGlobalInit::jit_report = false;
 std::string CFDArcoGlobalInit::store_dir;
 
 void CFDArcoGlobalInit::initialize(int, char**, bool skip_hist, const std::string& store_path) {
@@ -686,7 +687,16 @@ void jit_compile(const std::vector<std::unique_ptr<JitPlan>*>& plans) {
   std::vector<cfdb_kernel*> ks(passes.size(), nullptr);
   check(cfdb_kernel_build_many(CFDArcoGlobalInit::ctx(), int(passes.size()), srcs.data(), names.data(), ks.data()),
         "cfdb_kernel_build_many");
-  for (size_t k = 0; k < passes.size(); ++k) passes[k]->k = ks[k];
+  for (size_t k = 0; k < passes.size(); ++k) {
+    passes[k]->k = ks[k];
+    if (CFDArcoGlobalInit::jit_report) {
+      int regs = 0, maxt = 0;
+      int64_t local = 0;
+      check(cfdb_kernel_info(ks[k], &regs, &local, &maxt), "cfdb_kernel_info");
+      std::fprintf(stderr, "jit kernel %zu: %s, %d registers, %lld local bytes, %d cells per thread\n", k,
+                   passes[k]->entry.c_str(), regs, (long long)local, passes[k]->cpt);
+    }
+  }
 }
 
 // KernelBuilder::run: the plan's passes in order; the last one writes the

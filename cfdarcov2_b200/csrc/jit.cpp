@@ -481,6 +481,16 @@ extern "C" int cfdb_kernel_launch(cfdb_kernel* k, int64_t n_threads, int block, 
   return CFDB_OK;
 }
 
+extern "C" int cfdb_kernel_info(const cfdb_kernel* k, int* registers, int64_t* local_bytes, int* max_threads) {
+  if (!k || !k->ctx) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_kernel_info: kernel is NULL or its context was destroyed");
+  cudaFuncAttributes fa{};
+  CFDB_CUDA(k->ctx, cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(k->kern)));
+  if (registers) *registers = fa.numRegs;
+  if (local_bytes) *local_bytes = int64_t(fa.localSizeBytes);
+  if (max_threads) *max_threads = fa.maxThreadsPerBlock;
+  return CFDB_OK;
+}
+
 extern "C" int cfdb_kernel_destroy(cfdb_kernel* k) {
   if (!k) return CFDB_OK;
   if (k->ctx) cfdb_release(k->ctx, k);

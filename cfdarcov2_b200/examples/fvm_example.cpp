@@ -17,6 +17,7 @@
 //   fvm_example ref_wave out.bin nx ny nz steps   the reference's wave benchmark (main_3d_wave.cu)
 //   fvm_example <mode>_twice ...                  evaluate twice, print evaluate_us and steady_us
 //   fvm_example <mode>_arrays ...                 generated kernels read the face arrays on exact lattices too
+//   fvm_example <mode>_report ...                 print each generated kernel's registers and local bytes
 //   fvm_example heat_store out.bin nx ny nz steps dir
 //                                                 heat with history kept, then the reference's output
 //                                                 calls: store_history (.vti per step), mesh.json and
@@ -81,6 +82,7 @@ int main(int argc, char** argv) {
     mode.resize(mode.size() - k);
     return true;
   };
+  const bool report = suffix("_report");
   const bool twice = suffix("_twice");
   const bool arrays = suffix("_arrays");
   const bool jit = !suffix("_nojit");
@@ -98,6 +100,7 @@ int main(int argc, char** argv) {
     CFDArcoGlobalInit::enable_cuda(0);
     CFDArcoGlobalInit::jit_lattice = !arrays;
     CFDArcoGlobalInit::jit_all = jit;
+    CFDArcoGlobalInit::jit_report = report;
     Mesh3D mesh(nx, ny, nz, 1.f / float(nx), 1.f / float(ny), 1.f / float(nz));
     mesh.init_basic_internals();
     mesh.compute();
@@ -118,7 +121,6 @@ int main(int argc, char** argv) {
       jitted = eq.jit_equations;
       g_lattice = eq.lattice_equations;
       g_groups = eq.jit_groups;
-    g_groups = eq.jit_groups;
       result.push_back(T.host());
       if (storing) {
         store_history({&T}, &mesh);
@@ -138,7 +140,6 @@ int main(int argc, char** argv) {
       jitted = eq.jit_equations;
       g_lattice = eq.lattice_equations;
       g_groups = eq.jit_groups;
-    g_groups = eq.jit_groups;
       result.push_back(u.host());
     } else if (mode == "advect") {
       HostVec Q0 = gaussian(mesh, 0.4f, 0.5f, 0.5f, 0.15f), Uv(mesh._num_nodes, 0.3f), Vv(mesh._num_nodes, -0.2f),
@@ -156,7 +157,6 @@ int main(int argc, char** argv) {
       jitted = eq.jit_equations;
       g_lattice = eq.lattice_equations;
       g_groups = eq.jit_groups;
-    g_groups = eq.jit_groups;
       result.push_back(q.host());
       result.push_back(r.host());
     } else if (mode == "nested") {
@@ -174,7 +174,6 @@ int main(int argc, char** argv) {
       jitted = eq.jit_equations;
       g_lattice = eq.lattice_equations;
       g_groups = eq.jit_groups;
-    g_groups = eq.jit_groups;
       result.push_back(q.host());
     } else if (mode == "euler3d") {
       // The reference's "euler" benchmark system (examples/main_3d.cpp): primitive

@@ -413,6 +413,10 @@ int cfdb_kernel_build_many(cfdb_ctx* ctx, int count, const char* const* sources,
  * (the cudaLaunchKernel convention).  Asynchronous. */
 int cfdb_kernel_launch(cfdb_kernel* k, int64_t n_threads, int block, void** args);
 int cfdb_kernel_destroy(cfdb_kernel* k);
+/* Resources of a built kernel as the device reports them: registers per
+ * thread, local (spill and stack) bytes per thread, the largest CTA it can
+ * be launched with.  No reference counterpart (OCCA reports nothing). */
+int cfdb_kernel_info(const cfdb_kernel* k, int* registers, int64_t* local_bytes, int* max_threads);
 
 /* The plain FP32 geometry of a mesh as device pointers (uploaded on first
  * use, owned by the mesh): the inputs KernelBuilder wires into generated

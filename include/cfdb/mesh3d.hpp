@@ -38,6 +38,9 @@ class CFDArcoGlobalInit {
   // generated kernels give the operator path's bits); false keeps them on
   // the operator-by-operator path as the reference runs them
   static bool jit_all;
+  // print each generated kernel's entry, registers and local bytes to stderr
+  // when it is built (a diagnostic, off by default)
+  static bool jit_report;
 };
 
 class Mesh3D {

@@ -129,3 +129,15 @@ def test_disk_cache_serves_a_new_context_and_survives_damage(cfdb, tmp_path, mon
     build_many(ctx4, [src.replace("axpy_cached", "axpy_uncached")], ["axpy_uncached"])
     assert len(list(tmp_path.glob("*.cubin"))) == 1
     assert os.environ["CFDB_KERNEL_CACHE"] == "off"
+
+
+def test_kernel_info_reports_the_built_kernel(cfdb):
+    ctx = cfdb.Context(0)
+    (k,) = build_many(ctx, [AXPY.replace("axpy", "axpy_info")], ["axpy_info"])
+    regs, local, maxt = C.c_int(0), C.c_int64(-1), C.c_int(0)
+    capi.call("cfdb_kernel_info", k, C.byref(regs), C.byref(local), C.byref(maxt), ctx=ctx.h)
+    assert 0 < regs.value <= 255 and local.value == 0 and maxt.value >= 128
+    capi.call("cfdb_kernel_destroy", k)
+    with pytest.raises(capi.CfdbError) as e:
+        capi.call("cfdb_kernel_info", None, None, None, None)
+    assert e.value.code == capi.EINVAL
