@@ -230,15 +230,16 @@ def test_operator_tree_with_grad_stab_and_sequential_equations(oracle, tmp_path)
 
 def test_generated_kernels_report_no_spills(tmp_path):
     """_report prints each generated kernel's resources (cfdb_kernel_info):
-    the reference's Euler system builds as 4 fused kernels, none spilling to
-    local memory, and the report changes no result."""
+    the reference's Euler system builds its fused groups (4, plus any
+    materialised operand passes), none spilling to local memory, and the
+    report changes no result."""
     n, steps = 16, 4
     out = tmp_path / "report.bin"
     r = subprocess.run([EXE, "euler3d_report", str(out), str(n), str(n), str(n), str(steps)], capture_output=True,
                        text=True, timeout=300)
     assert r.returncode == 0, r.stderr
     lines = [ln for ln in r.stderr.splitlines() if ln.startswith("jit kernel ")]
-    assert len(lines) == 4, r.stderr
+    assert len(lines) >= 4, r.stderr
     for ln in lines:
         regs = int(ln.split(", ")[1].split()[0])
         local = int(ln.split(", ")[2].split()[0])
