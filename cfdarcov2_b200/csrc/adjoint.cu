@@ -9,6 +9,8 @@
 #include "f32x2.cuh"
 #include "tma_host.hpp"
 
+CFDB_MODULE_ANCHOR
+
 namespace {
 
 constexpr int kThreads = 256;

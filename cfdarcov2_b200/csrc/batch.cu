@@ -23,6 +23,8 @@
 
 #include "cfdb_internal.hpp"
 
+CFDB_MODULE_ANCHOR
+
 namespace {
 
 struct ProbDev {

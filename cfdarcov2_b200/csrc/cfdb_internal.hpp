@@ -179,6 +179,18 @@ void cfdb_dev_free(cfdb_ctx* ctx, void* p);
 int cfdb_ws_alloc(cfdb_ctx* ctx, int64_t bytes, void** out);
 void cfdb_ws_free(cfdb_ctx* ctx, void* p);
 
+// ---- module loading ---------------------------------------------------------
+// CUDA loads a kernel at its first launch by default (lazy loading), which
+// puts 0.1-1.5 ms of module work inside a caller's first step.  Each
+// translation unit with kernels registers an empty anchor kernel at library
+// load; context creation loads every kernel of the anchors' modules.
+int cfdb_register_module(const void* anchor_kernel);
+#define CFDB_MODULE_ANCHOR                                                                      \
+  namespace {                                                                                   \
+  __global__ void cfdb_module_anchor_k() {}                                                     \
+  const int cfdb_module_anchor_reg_ = cfdb_register_module(reinterpret_cast<const void*>(&cfdb_module_anchor_k)); \
+  }
+
 // ---- geometry helpers ------------------------------------------------------
 int cfdb_mesh_need_host_geom(cfdb_mesh* m);
 int cfdb_mesh_need_plain(cfdb_mesh* m, int dtype);

@@ -8,6 +8,8 @@
 // row segment.
 #include "tma_host.hpp"
 
+CFDB_MODULE_ANCHOR
+
 namespace {
 
 constexpr int kThreads = 256;

@@ -9,6 +9,8 @@
 #include "euler_internal.hpp"
 #include "tma_host.hpp"
 
+CFDB_MODULE_ANCHOR
+
 namespace {
 
 __device__ __forceinline__ double bits_to_double(unsigned long long b) { return __longlong_as_double((long long)b); }

@@ -12,6 +12,8 @@
 
 #include "euler_internal.hpp"
 
+CFDB_MODULE_ANCHOR
+
 namespace {
 
 constexpr int kThreads = 256;

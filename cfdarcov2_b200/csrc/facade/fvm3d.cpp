@@ -3,6 +3,7 @@
 // expression node evaluates through a cfdb_op_* kernel into a buffer it
 // allocates once.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstddef>
 #include <cstdint>
@@ -14,7 +15,9 @@
 #include <map>
 #include <set>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
+#include <unordered_map>
 #include <utility>
 
 #include "cfdb/fvm3d.hpp"
@@ -62,8 +65,70 @@ void CFDArcoGlobalInit::enable_cuda(int device) {
   cuda_enabled = true;
 }
 
+namespace {
+// Device buffers of the facade: freed ones are kept by size and handed out
+// again instead of going back to the driver (cudaMalloc of a 100 MB buffer
+// costs ~0.7 ms, cudaFree ~0.35 ms), as the reference allocates from an RMM
+// pool it reserves at start-up (src/cfdarcho_main_3d.cpp:333-344).  All
+// facade work runs on the context's one stream, so a reused buffer is only
+// touched after the work that used it before.  The kept buffers go back to
+// the device in finalize() and when an allocation fails.
+struct BlockCache {
+  std::mutex mu;
+  std::unordered_map<float*, size_t> live;  // buffer -> floats
+  std::multimap<size_t, float*> kept;       // floats -> freed buffer
+};
+BlockCache& blocks() {
+  static BlockCache c;
+  return c;
+}
+void release_kept(cfdb_ctx* ctx) {  // with the cache's lock held
+  for (auto& kv : blocks().kept) cfdb_free(ctx, kv.second);
+  blocks().kept.clear();
+}
+
+float* device_alloc(size_t n) {
+  cfdb_ctx* ctx = CFDArcoGlobalInit::ctx();
+  BlockCache& c = blocks();
+  std::lock_guard<std::mutex> lock(c.mu);
+  auto it = c.kept.find(n);
+  if (it != c.kept.end()) {
+    float* p = it->second;
+    c.kept.erase(it);
+    c.live[p] = n;
+    return p;
+  }
+  void* p = nullptr;
+  int rc = cfdb_alloc(ctx, int64_t(n * sizeof(float)), &p);
+  if (rc == CFDB_ENOMEM && !c.kept.empty()) {
+    release_kept(ctx);
+    rc = cfdb_alloc(ctx, int64_t(n * sizeof(float)), &p);
+  }
+  check(rc, "cfdb_alloc");
+  c.live[static_cast<float*>(p)] = n;
+  return static_cast<float*>(p);
+}
+void device_free(float* p) {
+  if (!p || !CFDArcoGlobalInit::cuda_enabled) return;
+  BlockCache& c = blocks();
+  std::lock_guard<std::mutex> lock(c.mu);
+  auto it = c.live.find(p);
+  if (it == c.live.end()) {
+    cfdb_free(CFDArcoGlobalInit::ctx(), p);
+    return;
+  }
+  c.kept.emplace(it->second, p);
+  c.live.erase(it);
+}
+}  // namespace
+
 void CFDArcoGlobalInit::finalize() {
-  if (g_ctx) cfdb_ctx_destroy(g_ctx);
+  if (g_ctx) {
+    std::lock_guard<std::mutex> lock(blocks().mu);
+    release_kept(g_ctx);
+    blocks().live.clear();  // the context frees what is still live
+    cfdb_ctx_destroy(g_ctx);
+  }
   g_ctx = nullptr;
   cuda_enabled = false;
 }
@@ -72,17 +137,6 @@ cfdb_ctx* CFDArcoGlobalInit::ctx() {
   if (!g_ctx) enable_cuda(0);
   return g_ctx;
 }
-
-namespace {
-float* device_alloc(size_t n) {
-  void* p = nullptr;
-  check(cfdb_alloc(CFDArcoGlobalInit::ctx(), int64_t(n * sizeof(float)), &p), "cfdb_alloc");
-  return static_cast<float*>(p);
-}
-void device_free(float* p) {
-  if (p && CFDArcoGlobalInit::cuda_enabled) cfdb_free(CFDArcoGlobalInit::ctx(), p);
-}
-}  // namespace
 
 // ---------------------------------------------------------------------------
 // Mesh3D
@@ -305,16 +359,29 @@ struct JitPlan {
     return s;
   }
   std::vector<std::unique_ptr<JitPass>> passes;  // run order; the last computes the equation
+  // scratch buffers: sizes while planning; placed in one block that the
+  // caller allocates for all plans of a system (place_scratch)
+  std::vector<size_t> scratch_floats;
   std::vector<float*> scratch;
   std::map<const Node*, int> materialised;
   std::map<const void*, int> stab_grads;  // by field, or by operand node
   bool ok = true;
-  ~JitPlan() {
-    for (float* p : scratch) device_free(p);
-  }
   int new_scratch(size_t floats) {
-    scratch.push_back(device_alloc(floats));
+    scratch_floats.push_back(floats);
+    scratch.push_back(nullptr);
     return int(scratch.size() - 1);
+  }
+  static size_t slot(size_t floats) { return (floats + 63) / 64 * 64; }  // 256-byte aligned slots
+  size_t scratch_total() const {
+    size_t t = 0;
+    for (size_t f : scratch_floats) t += slot(f);
+    return t;
+  }
+  void place_scratch(float* base) {
+    for (size_t k = 0; k < scratch.size(); ++k) {
+      scratch[k] = base;
+      base += slot(scratch_floats[k]);
+    }
   }
   int materialise(const Node* n);
   int stab_grad(const Node* operand);
@@ -951,6 +1018,11 @@ Equation::Equation(size_t t) : timesteps(t) {}
 void Equation::evaluate(std::vector<Variable*>& all_vars, EquationTemplate& eqs, DT* dt, bool visualize,
                         std::vector<Variable*> store_vars) const {
   cfdb_ctx* ctx = CFDArcoGlobalInit::ctx();
+  // phase times on the host clock, printed with jit_report
+  using Clock = std::chrono::steady_clock;
+  const auto t_start = Clock::now();
+  auto ms_since = [](Clock::time_point a) { return std::chrono::duration<double, std::milli>(Clock::now() - a).count(); };
+  double ms_plan = 0, ms_compile = 0, ms_first = 0;
   fused_equations = 0;
   jit_equations = 0;
   lattice_equations = 0;
@@ -1026,12 +1098,33 @@ void Equation::evaluate(std::vector<Variable*>& all_vars, EquationTemplate& eqs,
     open_written.insert(target);
   }
   close_group();
+  // every plan's scratch in one block, returned when evaluate ends
+  struct Block {
+    float* p = nullptr;
+    ~Block() { device_free(p); }
+  } scratch;
+  {
+    size_t total = 0;
+    for (Unit& u : units) total += u.plan->scratch_total();
+    if (total) scratch.p = device_alloc(total);
+    float* at = scratch.p;
+    for (Unit& u : units) {
+      u.plan->place_scratch(at);
+      at += u.plan->scratch_total();
+    }
+  }
+  ms_plan = ms_since(t_start);
   {
     std::vector<std::unique_ptr<JitPlan>*> plans;
     for (Unit& u : units) plans.push_back(&u.plan);
     jit_compile(plans);
   }
+  ms_compile = ms_since(t_start) - ms_plan;
   for (size_t t = 0; t < timesteps; ++t) {
+    if (t == 1 && CFDArcoGlobalInit::jit_report) {
+      check(cfdb_sync(ctx), "cfdb_sync");
+      ms_first = ms_since(t_start) - ms_plan - ms_compile;
+    }
     dt->update();
     const float dtv = dt->_dt;
     for (size_t e = 0; e < eqs.size(); ++e) {
@@ -1102,6 +1195,17 @@ void Equation::evaluate(std::vector<Variable*>& all_vars, EquationTemplate& eqs,
   }
   check(cfdb_sync(ctx), "cfdb_sync");
   if (visualize) std::printf("\n");
+  if (CFDArcoGlobalInit::jit_report) {
+    const double ms_steps = ms_since(t_start) - ms_plan - ms_compile - ms_first;
+    const auto t_free = Clock::now();
+    units.clear();  // the plans' kernels and the scratch block, as the return would
+    device_free(scratch.p);
+    scratch.p = nullptr;
+    std::fprintf(stderr,
+                 "evaluate phases (ms): plan %.3f, kernel builds %.3f, first step %.3f, other steps %.3f, "
+                 "release %.3f\n",
+                 ms_plan, ms_compile, ms_first, ms_steps, ms_since(t_free));
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -10,6 +10,8 @@
 #include "heat_cell.cuh"
 #include "tma_host.hpp"
 
+CFDB_MODULE_ANCHOR
+
 namespace {
 
 // Heat: T' = T + dt k sum_d ((T_d+ - T) + (T_d- - T)) / h_d^2.  Boundary faces

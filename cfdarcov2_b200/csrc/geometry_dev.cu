@@ -8,6 +8,8 @@
 #include "cfdb_internal.hpp"
 #include "geometry_cell.hpp"
 
+CFDB_MODULE_ANCHOR
+
 namespace {
 
 using cfdb_geom::CellFace;

@@ -10,6 +10,8 @@
 
 #include "cfdb_internal.hpp"
 
+CFDB_MODULE_ANCHOR
+
 int cfdb_revolve_build(int32_t steps, int32_t snapshots, std::vector<int32_t>& act, std::vector<int32_t>& arg,
                        std::vector<int32_t>& at, int64_t* forward);
 

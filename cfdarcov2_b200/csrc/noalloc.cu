@@ -27,6 +27,8 @@
 
 #include "cfdb_internal.hpp"
 
+CFDB_MODULE_ANCHOR
+
 namespace {
 
 constexpr int kChunk = 4096;             // cells reduced by one CTA

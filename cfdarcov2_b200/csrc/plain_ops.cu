@@ -11,6 +11,8 @@
 
 #include "cfdb_internal.hpp"
 
+CFDB_MODULE_ANCHOR
+
 namespace {
 
 constexpr int kThreads = 256;

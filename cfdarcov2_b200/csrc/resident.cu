@@ -18,6 +18,8 @@
 #include "cfdb_internal.hpp"
 #include "heat_cell.cuh"
 
+CFDB_MODULE_ANCHOR
+
 namespace cg = cooperative_groups;
 
 namespace {

@@ -9,7 +9,11 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
+#include <vector>
+
+#include <cuda.h>
 
 #include "cfdb_internal.hpp"
 
@@ -63,21 +67,86 @@ void cfdb_dev_free(cfdb_ctx* ctx, void* p) {
   cudaFree(p);
 }
 
+// ---- module loading -----------------------------------------------------------
+namespace {
+std::vector<const void*>& module_anchors() {
+  static std::vector<const void*> v;
+  return v;
+}
+
+template <class F> F driver_fn(const char* name) {
+  void* p = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess)
+    return nullptr;
+  return reinterpret_cast<F>(p);
+}
+
+// Loads every kernel of the registered modules on the current device, once
+// per device and process.  Best effort: a driver without the enumeration
+// calls (before CUDA 12.4) leaves loading to the first launches.
+void load_modules(int device) {
+  static std::mutex mu;
+  static bool done[kMaxDevices] = {};
+  std::lock_guard<std::mutex> lock(mu);
+  if (device < 0 || device >= kMaxDevices || done[device]) return;
+  done[device] = true;
+  using GetModule = CUresult (*)(CUmodule*, CUfunction);
+  using Count = CUresult (*)(unsigned int*, CUmodule);
+  using Enumerate = CUresult (*)(CUfunction*, unsigned int, CUmodule);
+  using Load = CUresult (*)(CUfunction);
+  auto get_module = driver_fn<GetModule>("cuFuncGetModule");
+  auto count = driver_fn<Count>("cuModuleGetFunctionCount");
+  auto enumerate = driver_fn<Enumerate>("cuModuleEnumerateFunctions");
+  auto load = driver_fn<Load>("cuFuncLoad");
+  if (!get_module || !count || !enumerate || !load) return;
+  for (const void* anchor : module_anchors()) {
+    cudaFunction_t f = nullptr;
+    if (cudaGetFuncBySymbol(&f, anchor) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    CUmodule mod = nullptr;
+    unsigned int n = 0;
+    if (get_module(&mod, reinterpret_cast<CUfunction>(f)) != CUDA_SUCCESS || count(&n, mod) != CUDA_SUCCESS || n == 0)
+      continue;
+    std::vector<CUfunction> fns(n);
+    if (enumerate(fns.data(), n, mod) != CUDA_SUCCESS) continue;
+    for (CUfunction fn : fns) load(fn);
+  }
+}
+
+// The context's stream-ordered pool, created with the context and grown by
+// one small block so that the first workspace of a step does not create it.
+int make_pool(cfdb_ctx* ctx) {
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = ctx->device;
+  CFDB_CUDA(ctx, cudaMemPoolCreate(&ctx->pool, &props));
+  uint64_t keep = UINT64_MAX;  // never hand freed blocks back on synchronisation
+  CFDB_CUDA(ctx, cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  void* p = nullptr;
+  CFDB_CUDA(ctx, cudaMallocFromPoolAsync(&p, 1 << 20, ctx->pool, ctx->stream));
+  CFDB_CUDA(ctx, cudaFreeAsync(p, ctx->stream));
+  CFDB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return CFDB_OK;
+}
+}  // namespace
+
+int cfdb_register_module(const void* anchor_kernel) {
+  module_anchors().push_back(anchor_kernel);
+  return 0;
+}
+
 int cfdb_ws_alloc(cfdb_ctx* ctx, int64_t bytes, void** out) {
   *out = nullptr;
   if (bytes <= 0) bytes = 16;
   if (ctx->budget > 0 && ctx->allocated + bytes > ctx->budget)
     return cfdb_fail(ctx, CFDB_ENOMEM, "workspace of %lld bytes exceeds the context budget (%lld of %lld used)",
                      (long long)bytes, (long long)ctx->allocated, (long long)ctx->budget);
-  if (!ctx->pool) {
-    cudaMemPoolProps props{};
-    props.allocType = cudaMemAllocationTypePinned;
-    props.location.type = cudaMemLocationTypeDevice;
-    props.location.id = ctx->device;
-    CFDB_CUDA(ctx, cudaMemPoolCreate(&ctx->pool, &props));
-    uint64_t keep = UINT64_MAX;  // never hand freed blocks back on synchronisation
-    CFDB_CUDA(ctx, cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep));
-  }
+  if (!ctx->pool)
+    if (int rc = make_pool(ctx)) return rc;
   void* p = nullptr;
   cudaError_t e = cudaMallocFromPoolAsync(&p, size_t(bytes), ctx->pool, ctx->stream);
   if (e != cudaSuccess) {
@@ -143,9 +212,18 @@ extern "C" int cfdb_ctx_create(int device, cfdb_ctx** out) {
   e = cudaMemset(ctx->d_error, 0, sizeof(int) * 4);
   if (e != cudaSuccess) {
     int r = cfdb_cuda_fail(nullptr, e, "cudaMemset");
+    cfdb_dev_free(ctx, ctx->d_error);
     delete ctx;
     return r;
   }
+  if ((rc = make_pool(ctx))) {
+    g_err_noctx = ctx->err;
+    if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
+    cfdb_dev_free(ctx, ctx->d_error);
+    delete ctx;
+    return rc;
+  }
+  load_modules(device);
   *out = ctx;
   return CFDB_OK;
 }
