@@ -165,6 +165,14 @@ class Context:
         call("cfdb_heat_step", self.h, mesh.h, _dtype_code(T), int(path), _ptr(T), _ptr(Tn), float(k), float(dt),
              ctx=self.h)
 
+    def d2t_step(self, mesh, u, u_prev, u_next, k, masks, dt, first_step=False):
+        """One leapfrog step of d2t(u) = k * sum_j L_{masks[j]}(u), fused
+        (cfdb_d2t_step): u_next = (dt dt R + 2 u) - u_prev, or dt R + u on
+        the first step (u_prev unused)."""
+        arr = (C.c_int32 * len(masks))(*[int(v) for v in masks])
+        call("cfdb_d2t_step", self.h, mesh.h, _dtype_code(u), _ptr(u), _ptr(u_prev), _ptr(u_next), float(k), arr,
+             len(masks), float(dt), int(bool(first_step)), ctx=self.h)
+
     def wave_step(self, mesh, q, qn, dt, c=None, c_const=1.0, speed_mode=0, path=FUSED):
         call("cfdb_wave_step", self.h, mesh.h, _dtype_code(q), int(path), _ptr(q), _ptr(qn), _ptr(c), float(c_const),
              int(speed_mode), float(dt), ctx=self.h)

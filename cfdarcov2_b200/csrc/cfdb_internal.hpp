@@ -217,6 +217,8 @@ int plain_wave_adjoint(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* q, co
                        const void* c, void* gc, double dt);
 // fused_tma.cu
 int fused_heat_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* T, void* Tn, double k, double dt);
+int fused_d2t_step(cfdb_ctx* ctx, cfdb_mesh* m, const void* u, const void* u_prev, void* u_next, double k,
+                   const int32_t* masks, int32_t n_terms, double dt, int first_step);
 // All `steps` FP32 heat steps in one thread-block-cluster launch with the
 // field resident in distributed shared memory (resident.cu); CFDB_EUNSUPPORTED
 // when the mesh does not fit (nothing launched).

@@ -857,6 +857,53 @@ bool match_heat(const Node* rhs, const Variable* T, float* k) {
   return false;
 }
 
+// d2t(u) = k * S, S * k or S, with S Laplacians of u (d2dx, d2dy, d2dz,
+// lapl, ...) summed left to right, at most three: the wave template that
+// cfdb_d2t_step runs as one fused pass with the generated kernel's rounding.
+struct D2tForm {
+  float k = 1.f;
+  int32_t masks[3] = {0, 0, 0};
+  int32_t n = 0;
+};
+bool match_d2t(const Node* rhs, const Variable* u, D2tForm* out) {
+  D2tForm f;
+  const Node* sum = rhs;
+  if (rhs->kind == Node::kBinary && rhs->op == CFDB_OP_MUL) {
+    if (rhs->a->kind == Node::kConst) {
+      f.k = rhs->a->value;
+      sum = rhs->b.get();
+    } else if (rhs->b->kind == Node::kConst) {
+      f.k = rhs->b->value;
+      sum = rhs->a.get();
+    }
+  }
+  auto lapl_u = [&](const Node* n) {
+    return n->kind == Node::kLapl && n->mask >= 1 && n->mask <= 7 && n->a->kind == Node::kField && n->a->field == u;
+  };
+  std::vector<int32_t> masks;
+  const Node* n = sum;
+  while (n->kind == Node::kBinary && n->op == CFDB_OP_ADD && lapl_u(n->b.get())) {
+    masks.insert(masks.begin(), n->b->mask);
+    n = n->a.get();
+  }
+  if (!lapl_u(n)) return false;
+  masks.insert(masks.begin(), n->mask);
+  if (masks.size() > 3) return false;
+  for (size_t j = 0; j < masks.size(); ++j) f.masks[j] = masks[j];
+  f.n = int32_t(masks.size());
+  *out = f;
+  return true;
+}
+
+// The mesh is an exact lattice (per-slot geometry constants, all finite).
+bool lattice_exact(Mesh3D* mesh) {
+  cfdb_lattice_geometry lat{};
+  check(cfdb_mesh_lattice_geometry(mesh->handle(), &lat), "cfdb_mesh_lattice_geometry");
+  bool ok = lat.exact != 0;
+  for (const float* v = lat.normal; v <= &lat.volume; ++v) ok = ok && std::isfinite(*v);
+  return ok;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -1040,6 +1087,7 @@ void Equation::evaluate(std::vector<Variable*>& all_vars, EquationTemplate& eqs,
   };
   std::vector<Unit> units;
   std::vector<int> unit_at(eqs.size(), -1);  // unit starting at this equation
+  std::map<size_t, D2tForm> fused_d2t;       // d2t equations run by cfdb_d2t_step
   std::vector<GroupMember> open;
   size_t open_first = 0;
   Mesh3D* open_mesh = nullptr;
@@ -1075,6 +1123,14 @@ void Equation::evaluate(std::vector<Variable*>& all_vars, EquationTemplate& eqs,
     }
     if (d2) {
       close_group();
+      // the wave template on an exact lattice: one fused pass instead of a
+      // generated kernel (the face-array form, jit_lattice off, keeps the latter)
+      D2tForm form;
+      if (CFDArcoGlobalInit::jit_lattice && match_d2t(rhs, d2->var, &form) && stencil_fusable(mesh) &&
+          lattice_exact(mesh)) {
+        fused_d2t[e] = form;
+        continue;
+      }
       auto plan = jit_build(rhs, mesh);
       if (plan) {
         ++jit_equations;
@@ -1156,7 +1212,14 @@ void Equation::evaluate(std::vector<Variable*>& all_vars, EquationTemplate& eqs,
         Variable* Uv = d2->var;
         const int64_t N = int64_t(Uv->mesh->_num_nodes);
         if (!Uv->prev_cu) Uv->prev_cu = device_alloc(Uv->mesh->_num_nodes);
-        if (J) {
+        auto fz = fused_d2t.find(e);
+        if (fz != fused_d2t.end()) {
+          const D2tForm& f = fz->second;
+          check(cfdb_d2t_step(ctx, Uv->mesh->handle(), CFDB_F32, Uv->current_cu, Uv->has_prev ? Uv->prev_cu : nullptr,
+                              Uv->next_cu, f.k, f.masks, f.n, dtv, Uv->has_prev ? 0 : 1),
+                "cfdb_d2t_step");
+          if (t == 0) ++fused_equations;
+        } else if (J) {
           jit_run(*J, dtv, Uv->next_cu, Uv->current_cu, Uv->prev_cu, Uv->has_prev ? 2 : 1);
         } else {
           const float* R = eval_node(rhs.node.get());

@@ -4,6 +4,7 @@
 // Replaces the reference's per-equation JIT kernel (src/fvm3d.cpp:1219-1394),
 // which streamed ~180 B/cell of geometry per step; on a uniform mesh the
 // geometry reduces to three spacings.
+#include <cmath>
 #include <cstdlib>
 #include <string>
 
@@ -29,6 +30,95 @@ struct HeatPhys {
   __device__ static void cell(const stencil::CellIn<1>& in, const Params& a, float o[NF]) {
     o[0] = heat_update(in.P[0], in.nb[0][0], in.nb[1][0], in.nb[2][0], in.nb[3][0], in.nb[4][0], in.nb[5][0], a.cx,
                        a.cy, a.cz);
+  }
+  __device__ static void acc_init(Acc&) {}
+  __device__ static void acc_cell(Acc&, const float*, const Params&) {}
+  __device__ static void finish(Acc&, const Params&, bool) {}
+};
+
+// Leapfrog of d2t(u) = k sum_j L_{m_j}(u) on an exact lattice, the equation
+// the reference's wave example builds (examples/main_3d_wave.cu:
+// d2t(u) = c^2 (d2dx(u) + d2dy(u))), with the operands in the order of the
+// operator kernels and the generated ones (Grad2Var, src/fvm3d.cpp:831-906;
+// update, src/fvm3d.cpp:710-765), every operation rounded on its own:
+//   sn_f  = (u_N(f) - u) alpha_f                      face slots f = 0..5
+//   acc_d = 0 + sum_{f: n_{f,d} != 0} (sn_f n_{f,d}) A_f,   L_m = 0 + sum_{d in m} acc_d / V
+//   R = k ((L_m1 + L_m2) + L_m3)
+//   first step: u' = dt R + u;  later: u' = (dt dt R + 2 u) - u_prev
+// A boundary face has u_N = u: its sn is +0 whatever alpha the wall has, so
+// the interior alphas serve every face.  u_prev comes one plane ahead from
+// global memory (HAS_PRE); only u is staged with its halo.  Each direction's
+// nonzero normals are its own two faces (the uniform meshes the sweep serves
+// are axis-aligned).  GEOM says how the face factors round: D2T_DIVIDE
+// divides by V; D2T_RECIP multiplies by 1/V where that is exact (V a power of
+// two: acc / V == acc * (1/V) bit for bit); D2T_UNIT has alpha, the normals on
+// their own faces, the areas and V all exactly 1 (unit cells), where every
+// product by them returns its operand, so they are left out.  FORM >= 0 packs the term masks at compile time (3 bits
+// each: 7 = lapl, 1 | 2 << 3 = d2dx + d2dy, ...), so the sum has no branches;
+// FORM < 0 reads them from the parameters.  Directions no term uses are
+// skipped.
+struct D2tParams {
+  float* prev;      // u at the previous step (the first step reads u again: no subtraction)
+  float alpha[6];   // interior alpha per face slot
+  float nrm[3][6];  // normal component d of face slot f
+  float area[6];
+  float volume, vinv, k, dt;
+  int masks[3];     // direction mask of each term
+  int n_terms;
+  int used;         // union of the masks
+  int first;
+};
+enum { D2T_DIVIDE = 0, D2T_RECIP = 1, D2T_UNIT = 2 };
+template <int GEOM, int FORM> struct D2tPhys {
+  static constexpr int NF = 1;
+  static constexpr int NA = 0;
+  static constexpr bool HAS_C = false;
+  static constexpr bool HAS_PRE = true;
+  static constexpr int MIN_BLOCKS = 4;
+  using Params = D2tParams;
+  struct Acc {};
+  static constexpr int form_mask(int j) { return (FORM >> (3 * j)) & 7; }
+  __device__ static int term_mask(const Params& a, int j) { return FORM >= 0 ? form_mask(j) : a.masks[j]; }
+  __device__ static int terms(const Params& a) {
+    return FORM >= 0 ? (form_mask(0) != 0) + (form_mask(1) != 0) + (form_mask(2) != 0) : a.n_terms;
+  }
+  __device__ static int used(const Params& a) {
+    return FORM >= 0 ? (form_mask(0) | form_mask(1) | form_mask(2)) : a.used;
+  }
+  __device__ static float* pre_ptr(const Params& a) { return a.prev; }
+  __device__ static bool begin(Params&) { return true; }
+  __device__ static void ghost(float g[NF], const float p[NF], int) { g[0] = p[0]; }
+  __device__ static void cell(const stencil::CellIn<1>& in, const Params& a, float o[NF]) {
+    const float u = in.P[0];
+    // sweep neighbour order x-, x+, y-, y+, z-, z+ by face slot (0/1 z, 2/3 y, 4/5 x)
+    constexpr int nb_of_slot[6] = {4, 5, 2, 3, 0, 1};
+    float L[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      if (!((used(a) >> d) & 1)) continue;
+      float acc = 0.f;
+      const int f0 = 4 - 2 * d;  // the direction's - and + faces, in slot order
+#pragma unroll
+      for (int f = f0; f < f0 + 2; ++f) {
+        const float diff = __fsub_rn(in.nb[nb_of_slot[f]][0], u);
+        if (GEOM == D2T_UNIT) acc = __fadd_rn(acc, diff);
+        else acc = __fadd_rn(acc, __fmul_rn(__fmul_rn(__fmul_rn(diff, a.alpha[f]), a.nrm[d][f]), a.area[f]));
+      }
+      L[d] = GEOM == D2T_UNIT ? acc : GEOM == D2T_RECIP ? __fmul_rn(acc, a.vinv) : __fdiv_rn(acc, a.volume);
+    }
+    float S = 0.f;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      if (j >= terms(a)) break;
+      float t = 0.f;
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+        if ((term_mask(a, j) >> d) & 1) t = __fadd_rn(t, L[d]);
+      S = j == 0 ? t : __fadd_rn(S, t);
+    }
+    const float R = __fmul_rn(a.k, S);
+    o[0] = a.first ? __fadd_rn(__fmul_rn(a.dt, R), u)
+                   : __fsub_rn(__fadd_rn(__fmul_rn(__fmul_rn(a.dt, a.dt), R), __fmul_rn(2.0f, u)), in.pre);
   }
   __device__ static void acc_init(Acc&) {}
   __device__ static void acc_cell(Acc&, const float*, const Params&) {}
@@ -145,6 +235,61 @@ int fused_heat_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* T, void*
   p.cy = float(dt * k / (m->dy * m->dy));
   p.cz = float(dt * k / (m->dz * m->dz));
   return dispatch_tz<HeatPhys, 6>(ctx, m, T, Tn, nullptr, p, 0);
+}
+
+int fused_d2t_step(cfdb_ctx* ctx, cfdb_mesh* m, const void* u, const void* u_prev, void* u_next, double k,
+                   const int32_t* masks, int32_t n_terms, double dt, int first_step) {
+  if (int rc = stencil::check_sweep(ctx, m, {u, u_prev, u_next})) return rc;
+  cfdb_lattice_geometry lat{};
+  if (int rc = cfdb_mesh_lattice_geometry(m, &lat)) return rc;
+  if (!lat.exact)
+    return cfdb_fail(ctx, CFDB_EUNSUPPORTED,
+                     "cfdb_d2t_step: the mesh is not an exact lattice (its FP32 face values differ between cells)");
+  D2tParams p{};
+  p.prev = const_cast<float*>(static_cast<const float*>(first_step ? u : u_prev));
+  for (int f = 0; f < 6; ++f) {
+    p.alpha[f] = lat.alpha[f];
+    p.area[f] = lat.area[f];
+  }
+  for (int d = 0; d < 3; ++d) {
+    int faces = 0;  // bit f: n_{f,d} != 0
+    for (int f = 0; f < 6; ++f) {
+      p.nrm[d][f] = lat.normal[d * 6 + f];
+      if (lat.normal[d * 6 + f] != 0.f) faces |= 1 << f;
+    }
+    if (faces != (3 << (4 - 2 * d)))
+      return cfdb_fail(ctx, CFDB_EUNSUPPORTED, "cfdb_d2t_step: direction %d has normals off its own two faces", d);
+  }
+  p.volume = lat.volume;
+  int e2 = 0;
+  const bool recip = lat.volume > 0.f && std::frexp(double(lat.volume), &e2) == 0.5 && std::isnormal(1.0f / lat.volume);
+  p.vinv = recip ? 1.0f / lat.volume : 0.f;
+  p.k = float(k);
+  p.dt = float(dt);
+  p.n_terms = n_terms;
+  for (int j = 0; j < 3; ++j) {
+    p.masks[j] = j < n_terms ? masks[j] : 0;
+    p.used |= p.masks[j];
+  }
+  p.first = first_step ? 1 : 0;
+  bool unit = lat.volume == 1.f;
+  for (int f = 0; f < 6; ++f) unit = unit && lat.alpha[f] == 1.f && lat.area[f] == 1.f && lat.normal[(f < 2 ? 2 : f < 4 ? 1 : 0) * 6 + f] == 1.f;
+  const int form = p.masks[0] | p.masks[1] << 3 | p.masks[2] << 6;
+  // the reference's wave equation (d2dx + d2dy), lapl, and d2dx + d2dy + d2dz
+  // compiled with their masks
+  constexpr int XY = 1 | 2 << 3, LAPL = 7, XYZ = 1 | 2 << 3 | 4 << 6;
+  if (unit) {
+    if (form == XY) return dispatch_tz<D2tPhys<D2T_UNIT, XY>, 6>(ctx, m, u, u_next, nullptr, p, 0);
+    if (form == LAPL) return dispatch_tz<D2tPhys<D2T_UNIT, LAPL>, 6>(ctx, m, u, u_next, nullptr, p, 0);
+    if (form == XYZ) return dispatch_tz<D2tPhys<D2T_UNIT, XYZ>, 6>(ctx, m, u, u_next, nullptr, p, 0);
+    return dispatch_tz<D2tPhys<D2T_UNIT, -1>, 6>(ctx, m, u, u_next, nullptr, p, 0);
+  }
+  if (recip) {
+    if (form == XY) return dispatch_tz<D2tPhys<D2T_RECIP, XY>, 6>(ctx, m, u, u_next, nullptr, p, 0);
+    if (form == LAPL) return dispatch_tz<D2tPhys<D2T_RECIP, LAPL>, 6>(ctx, m, u, u_next, nullptr, p, 0);
+    return dispatch_tz<D2tPhys<D2T_RECIP, -1>, 6>(ctx, m, u, u_next, nullptr, p, 0);
+  }
+  return dispatch_tz<D2tPhys<D2T_DIVIDE, -1>, 6>(ctx, m, u, u_next, nullptr, p, 0);
 }
 
 int fused_wave_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* q, void* qn, const void* c, double cconst,

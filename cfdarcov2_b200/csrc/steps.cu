@@ -29,6 +29,21 @@ extern "C" int cfdb_heat_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, int path, 
   return plain_heat_update(ctx, dtype, p.stab_tmp, T, k, dt, Tn, m->n);
 }
 
+extern "C" int cfdb_d2t_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* u, const void* u_prev, void* u_next,
+                             double k, const int32_t* masks, int32_t n_terms, double dt, int first_step) {
+  if (int rc = check_step(ctx, m, dtype, CFDB_PATH_FUSED, "cfdb_d2t_step")) return rc;
+  if (dtype != CFDB_F32) return cfdb_fail(ctx, CFDB_EUNSUPPORTED, "cfdb_d2t_step computes in float32 only");
+  if (!u || !u_next || (!first_step && !u_prev)) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_d2t_step: NULL field pointer");
+  if (u == u_next || (!first_step && u_prev == u_next))
+    return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_d2t_step: u_next must differ from u and u_prev (no in-place stencil writes)");
+  if (!masks || n_terms < 1 || n_terms > 3) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_d2t_step: need 1 to 3 terms");
+  for (int j = 0; j < n_terms; ++j)
+    if (masks[j] < 1 || masks[j] > 7)
+      return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_d2t_step: term %d has mask %d (1..7)", j, masks[j]);
+  if (!std::isfinite(k) || !std::isfinite(dt)) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_d2t_step: k and dt must be finite");
+  return fused_d2t_step(ctx, m, u, first_step ? nullptr : u_prev, u_next, k, masks, n_terms, dt, first_step);
+}
+
 extern "C" int cfdb_wave_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, int path, const void* q, void* qn,
                               const void* c, double cconst, int mode, double dt) {
   if (int rc = check_step(ctx, m, dtype, path, "cfdb_wave_step")) return rc;

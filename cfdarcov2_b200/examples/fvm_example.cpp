@@ -138,6 +138,7 @@ int main(int argc, char** argv) {
       Equation eq(steps);
       eq.evaluate(vars, eqs, &dt, false);
       jitted = eq.jit_equations;
+      fused = eq.fused_equations;
       g_lattice = eq.lattice_equations;
       g_groups = eq.jit_groups;
       result.push_back(u.host());
@@ -282,7 +283,7 @@ int main(int argc, char** argv) {
       DT dt(&cube, UpdatePolicies::constant_dt, 0.1f, vars);
       const float c = 0.3f;
       EquationTemplate eqs = {{d2t(u), '=', c * c * (d2dx(u) + d2dy(u)), jit}};
-      jitted = timed_evaluate(steps, vars, eqs, dt, twice);
+      jitted = timed_evaluate(steps, vars, eqs, dt, twice, &fused);
       result.push_back(u.host());
     } else {
       std::fprintf(stderr, "unknown mode %s\n", mode.c_str());

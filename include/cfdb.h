@@ -251,6 +251,19 @@ int cfdb_total_fp64_noalloc(int dtype, const void* field, const void* volumes, d
 int cfdb_heat_step(cfdb_ctx* ctx, cfdb_mesh* mesh, int dtype, int path, const void* T, void* T_next, double k,
                    double dt);
 
+/* Leapfrog step of d2t(u) = k * (L_m1(u) + L_m2(u) + ...) with L_m the
+ * Laplacian over the directions of mask m (1 = d2dx, 2 = d2dy, 4 = d2dz,
+ * 7 = lapl) -- the equation examples/main_3d_wave.cu builds, whose
+ * KernelBuilder kernel (src/fvm3d.cpp:1219-1394, update src/fvm3d.cpp:710-765)
+ * this replaces with one TMA-tiled pass.  first_step != 0: u_next = dt R + u
+ * (u_prev unused, may be NULL); else u_next = (dt dt R + 2 u) - u_prev.
+ * Rounds like the operator kernels and the generated ones, operation by
+ * operation, so all give the same bits.  CFDB_F32 on an exact lattice
+ * (cfdb_mesh_lattice_geometry) with nz % 4 == 0 and 16-byte aligned fields;
+ * CFDB_EUNSUPPORTED otherwise. */
+int cfdb_d2t_step(cfdb_ctx* ctx, cfdb_mesh* mesh, int dtype, const void* u, const void* u_prev, void* u_next,
+                  double k, const int32_t* masks, int32_t n_terms, double dt, int first_step);
+
 /* First-order acoustic system (p,u,v,w), rho = 1: p_t = -c^2 div u,
  * u_t = -grad p, Rusanov face flux, reflective walls, forward Euler.
  * c_field (n values, same dtype) may be NULL for the constant c_const.

@@ -248,6 +248,68 @@ def test_fused_requires_nz_multiple_of_4(cfdb, ctx):
     ctx.heat_step(m, a, b, 1.0, 0.001, path=cfdb.PLAIN)  # the plain path serves any shape
 
 
+@pytest.mark.parametrize("shape,spacing,masks,k", [((16, 12, 8), (1.0, 1.0, 1.0), [1, 2], 0.09),
+                                                   ((10, 9, 12), (0.5, 0.25, 0.125), [7], 1.0),
+                                                   ((8, 8, 16), (1 / 8, 1 / 8, 1 / 16), [4, 1, 2], 0.3),
+                                                   ((5, 7, 4), (1.0, 2.0, 0.5), [3, 6], -1.5),
+                                                   ((8, 6, 8), (1.0, 1.0, 3.0), [7], 0.5),
+                                                   ((9, 4, 8), (1.0, 1.0, 1.0), [1, 2, 4], 0.25),
+                                                   ((12, 8, 8), (1.0, 1.0, 1.0), [7], 0.7),
+                                                   ((8, 8, 8), (1.0, 1.0, 1.0), [2, 1], 1.3),
+                                                   ((16, 8, 8), (0.5, 0.5, 0.5), [1, 2], 0.2)])
+def test_d2t_fused_equals_operator_composition_bitwise(cfdb, ctx, shape, spacing, masks, k):
+    """cfdb_d2t_step (one TMA pass) gives the bits of the operator kernels
+    composed as the generated kernel of d2t(u) = k (L_m1(u) + L_m2(u) + ...)
+    computes: Laplacians by direction mask, their sum left to right, times k,
+    then the leapfrog update (first step: the d1t form).  Covers unit cells
+    (products by one left out), power-of-two volumes (an exact 1/V) and
+    V = 3 (a true division), each with the masks compiled in ([1, 2], [7],
+    [1, 2, 4]) and read at run time."""
+    m = cfdb.Mesh.structured(ctx, *shape, *spacing)
+    assert m.lattice_geometry()[0]
+    g = torch.Generator(device="cpu").manual_seed(5)
+    u = torch.rand(m.n, generator=g).to(DEV)
+    prev = torch.rand(m.n, generator=g).to(DEV)
+    dt = torch.tensor(0.05, dtype=torch.float32, device=DEV)
+    S = None
+    for mk in masks:
+        L = ctx.lapl(m, u, mask=mk)
+        S = L if S is None else S + L
+    R = torch.tensor(k, dtype=torch.float32, device=DEV) * S
+    nxt = torch.empty_like(u)
+    ctx.d2t_step(m, u, prev, nxt, k, masks, 0.05)
+    assert torch.equal(nxt, (dt * dt * R + 2.0 * u) - prev)
+    ctx.d2t_step(m, u, None, nxt, k, masks, 0.05, first_step=True)
+    assert torch.equal(nxt, dt * R + u)
+
+
+def test_d2t_fused_rejects_what_it_cannot_run(cfdb, ctx):
+    m = cfdb.Mesh.structured(ctx, 8, 8, 8, 1.0, 1.0, 1.0)
+    u, p, o = (torch.zeros(m.n, device=DEV) for _ in range(3))
+    for masks in ([], [8], [1, 2, 4, 7]):
+        with pytest.raises(cfdb.CfdbError) as e:
+            ctx.d2t_step(m, u, p, o, 1.0, masks, 0.1)
+        assert e.value.code == cfdb.capi.EINVAL
+    with pytest.raises(cfdb.CfdbError) as e:
+        ctx.d2t_step(m, u, p, u, 1.0, [7], 0.1)  # in place
+    assert e.value.code == cfdb.capi.EINVAL
+    with pytest.raises(cfdb.CfdbError) as e:
+        ctx.d2t_step(m, u.double(), p.double(), o.double(), 1.0, [7], 0.1)
+    assert e.value.code == cfdb.capi.EUNSUPPORTED
+    m6 = cfdb.Mesh.structured(ctx, 4, 4, 6, 1.0, 1.0, 1.0)  # rows of 6 floats: no TMA sweep
+    a, b = torch.zeros(m6.n, device=DEV), torch.zeros(m6.n, device=DEV)
+    with pytest.raises(cfdb.CfdbError) as e:
+        ctx.d2t_step(m6, a, None, b, 1.0, [7], 0.1, first_step=True)
+    assert e.value.code == cfdb.capi.EUNSUPPORTED
+    mr = cfdb.Mesh.structured(ctx, 7, 5, 8, 1 / 13, 0.3, 1 / 7)
+    a, b = torch.zeros(mr.n, device=DEV), torch.zeros(mr.n, device=DEV)
+    if not mr.lattice_geometry()[0]:  # geometry constants that differ between cells
+        with pytest.raises(cfdb.CfdbError) as e:
+            ctx.d2t_step(mr, a, None, b, 1.0, [7], 0.1, first_step=True)
+        assert e.value.code == cfdb.capi.EUNSUPPORTED and "exact lattice" in str(e.value)
+    ctx.sync()
+
+
 @pytest.mark.parametrize("spec", MESHES, ids=["aniso", "cube8", "jitter6"])
 @pytest.mark.parametrize("mode", [0, 1])
 def test_wave_plain_fp64_bitwise(cfdb, oracle, ctx, spec, mode):
