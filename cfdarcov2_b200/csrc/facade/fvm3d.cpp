@@ -295,7 +295,8 @@ const float* eval_node(Node* n) {
 // Cell indices stay 64-bit: 32-bit indices (an int index type in the
 // operator header for meshes below 2^31 / 18 cells) cut the largest group's
 // registers from 80 to 72 but slowed the Euler system from 214 to 229 ms per
-// 200 steps at 200^3.
+// 200 steps at 200^3; __launch_bounds__(256, 4) on the group kernels (64
+// registers, 40 bytes of spills in the largest) ran 220 ms.
 constexpr int kCptEquation = 4;
 constexpr int kCptGroup = 1;
 constexpr int kCptStab = 1;
