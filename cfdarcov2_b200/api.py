@@ -165,6 +165,12 @@ class Context:
         call("cfdb_heat_step", self.h, mesh.h, _dtype_code(T), int(path), _ptr(T), _ptr(Tn), float(k), float(dt),
              ctx=self.h)
 
+    def heat_step_fixed(self, mesh, T, Tn, k, dt, fixed):
+        """The fused heat step with the box-surface cells set to `fixed` in
+        the same pass (cfdb_heat_step_fixed)."""
+        call("cfdb_heat_step_fixed", self.h, mesh.h, _dtype_code(T), _ptr(T), _ptr(Tn), float(k), float(dt),
+             _ptr(fixed), ctx=self.h)
+
     def d2t_step(self, mesh, u, u_prev, u_next, k, masks, dt, first_step=False):
         """One leapfrog step of d2t(u) = k * sum_j L_{masks[j]}(u), fused
         (cfdb_d2t_step): u_next = (dt dt R + 2 u) - u_prev, or dt R + u on

@@ -109,6 +109,7 @@ PROTOTYPES = {
     "cfdb_total_fp64_noalloc": (_I, [_I, _P, _P, _D, _I64, _P, _P]),
     "cfdb_heat_step": (_I, [_P, _P, _I, _I, _P, _P, _D, _D]),
     "cfdb_d2t_step": (_I, [_P, _P, _I, _P, _P, _P, _D, _P, _I32, _D, _I]),
+    "cfdb_heat_step_fixed": (_I, [_P, _P, _I, _P, _P, _D, _D, _P]),
     "cfdb_wave_step": (_I, [_P, _P, _I, _I, _P, _P, _P, _D, _I, _D]),
     "cfdb_wave_dt": (_I, [_P, _P, _D, _D, _PD]),
     "cfdb_heat_run": (_I, [_P, _P, _I, _I, _P, _P, _D, _D, _I32, _I, _PI]),

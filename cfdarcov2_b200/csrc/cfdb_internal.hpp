@@ -216,7 +216,8 @@ int plain_wave_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* q, void*
 int plain_wave_adjoint(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* q, const void* lam1, void* lam0,
                        const void* c, void* gc, double dt);
 // fused_tma.cu
-int fused_heat_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* T, void* Tn, double k, double dt);
+int fused_heat_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* T, void* Tn, double k, double dt,
+                    const void* fixed = nullptr);
 int fused_d2t_step(cfdb_ctx* ctx, cfdb_mesh* m, const void* u, const void* u_prev, void* u_next, double k,
                    const int32_t* masks, int32_t n_terms, double dt, int first_step);
 // All `steps` FP32 heat steps in one thread-block-cluster launch with the

@@ -1017,16 +1017,26 @@ Variable stabz(const Variable& v) { return mesh_op(v, Node::kStab, 4); }
 
 HostVec boundary_none(Mesh3D*, HostVec& arr, const DT*) { return arr; }
 
+namespace {
+// The boundary copy as a callable the time loop can recognise: a heat
+// equation whose field has it runs the copy inside its fused step.
+struct BoundaryCopyCu {
+  std::shared_ptr<float> buf;
+  size_t count = 0;
+  // in place over the boundary cells only (the reference's blend
+  // arr * (1 - b) + copy * b leaves the interior as it is for finite states)
+  void operator()(Mesh3D* m, float* field, const DT*) const {
+    check(cfdb_op_boundary_set(CFDArcoGlobalInit::ctx(), m->handle(), CFDB_F32, field, buf.get()),
+          "cfdb_op_boundary_set");
+  }
+};
+}  // namespace
+
 BoundaryFNCU boundary_copy_cu(Mesh3D* mesh, const HostVec& values) {
   auto buf = std::shared_ptr<float>(device_alloc(values.size()), [](float* p) { device_free(p); });
   check(cfdb_upload(CFDArcoGlobalInit::ctx(), buf.get(), values.data(), int64_t(values.size() * sizeof(float))),
         "cfdb_upload");
-  // in place over the boundary cells only (the reference's blend
-  // arr * (1 - b) + copy * b leaves the interior as it is for finite states)
-  return [buf](Mesh3D* m, float* field, const DT*) {
-    check(cfdb_op_boundary_set(CFDArcoGlobalInit::ctx(), m->handle(), CFDB_F32, field, buf.get()),
-          "cfdb_op_boundary_set");
-  };
+  return BoundaryCopyCu{buf, values.size()};
 }
 
 // ---------------------------------------------------------------------------
@@ -1182,6 +1192,7 @@ void Equation::evaluate(std::vector<Variable*>& all_vars, EquationTemplate& eqs,
   }
   ms_compile = ms_since(t_start) - ms_plan;
   for (size_t t = 0; t < timesteps; ++t) {
+    Variable* bc_done = nullptr;  // a field whose boundary copy ran inside its fused step
     if (t == 1 && CFDArcoGlobalInit::jit_report) {
       check(cfdb_sync(ctx), "cfdb_sync");
       ms_first = ms_since(t_start) - ms_plan - ms_compile;
@@ -1204,9 +1215,22 @@ void Equation::evaluate(std::vector<Variable*>& all_vars, EquationTemplate& eqs,
         Variable* T = d->var;
         const int64_t N = int64_t(T->mesh->_num_nodes);
         float k = 0.f;
-        if (match_heat(rhs.node.get(), T, &k) &&
-            cfdb_heat_step(ctx, T->mesh->handle(), CFDB_F32, CFDB_PATH_FUSED, T->current_cu, T->next_cu, k,
-                           dtv) == CFDB_OK) {
+        // a one-equation, one-field system whose field resets its surface
+        // cells to a copy after each step: the copy runs inside the fused
+        // step (no other boundary function can observe the difference)
+        const BoundaryCopyCu* copy = nullptr;
+        if (eqs.size() == 1 && all_vars.size() == 1 && all_vars[0] == T && T->has_boundary_conditions_cu) {
+          copy = T->boundary_conditions_cu.target<BoundaryCopyCu>();
+          if (copy && copy->count != size_t(N)) copy = nullptr;
+        }
+        if (copy && match_heat(rhs.node.get(), T, &k) &&
+            cfdb_heat_step_fixed(ctx, T->mesh->handle(), CFDB_F32, T->current_cu, T->next_cu, k, dtv,
+                                 copy->buf.get()) == CFDB_OK) {
+          if (t == 0) ++fused_equations;
+          bc_done = T;
+        } else if (match_heat(rhs.node.get(), T, &k) &&
+                   cfdb_heat_step(ctx, T->mesh->handle(), CFDB_F32, CFDB_PATH_FUSED, T->current_cu, T->next_cu, k,
+                                  dtv) == CFDB_OK) {
           if (t == 0) ++fused_equations;
         } else {
           const float* R = eval_node(rhs.node.get());
@@ -1245,7 +1269,9 @@ void Equation::evaluate(std::vector<Variable*>& all_vars, EquationTemplate& eqs,
       }
     }
     for (Variable* v : all_vars) {
-      if (v->has_boundary_conditions_cu) {
+      if (v == bc_done) {
+        // applied inside the fused step
+      } else if (v->has_boundary_conditions_cu) {
         v->boundary_conditions_cu(v->mesh, v->current_cu, dt);
       } else if (v->boundary_conditions) {
         using Plain = HostVec (*)(Mesh3D*, HostVec&, const DT*);

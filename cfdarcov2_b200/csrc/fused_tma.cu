@@ -17,19 +17,26 @@ namespace {
 
 // Heat: T' = T + dt k sum_d ((T_d+ - T) + (T_d- - T)) / h_d^2.  Boundary faces
 // see T_N = T_P (zero gradient, intrinsic to Grad2Var: the reference's _ids
-// point to the cell itself, src/mesh3d.cpp:273-276).
-struct HeatPhys {
+// point to the cell itself, src/mesh3d.cpp:273-276).  FIXED: the cells of
+// the box surface then take fixed values (the examples' boundary copy,
+// examples/main_3d_heat.cpp:41-60, applied after the step) in the same pass.
+struct HeatParams {
+  float cx, cy, cz;     // dt k / h_d^2
+  const float* fixed;   // surface values (FIXED)
+};
+template <bool FIXED> struct HeatPhys {
   static constexpr int NF = 1;
   static constexpr int NA = 0;
   static constexpr bool HAS_C = false;
   static constexpr int MIN_BLOCKS = 4;
-  struct Params { float cx, cy, cz; };  // dt k / h_d^2
+  using Params = HeatParams;
   struct Acc {};
   __device__ static bool begin(Params&) { return true; }
   __device__ static void ghost(float g[NF], const float p[NF], int) { g[0] = p[0]; }
   __device__ static void cell(const stencil::CellIn<1>& in, const Params& a, float o[NF]) {
     o[0] = heat_update(in.P[0], in.nb[0][0], in.nb[1][0], in.nb[2][0], in.nb[3][0], in.nb[4][0], in.nb[5][0], a.cx,
                        a.cy, a.cz);
+    if (FIXED && in.walls) o[0] = a.fixed[in.idx];
   }
   __device__ static void acc_init(Acc&) {}
   __device__ static void acc_cell(Acc&, const float*, const Params&) {}
@@ -227,14 +234,17 @@ int dispatch_wave_tiles(cfdb_ctx* ctx, const cfdb_mesh* m, const void* q, void* 
 
 }  // namespace
 
-int fused_heat_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* T, void* Tn, double k, double dt) {
+int fused_heat_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* T, void* Tn, double k, double dt,
+                    const void* fixed) {
   if (dtype != CFDB_F32) return cfdb_fail(ctx, CFDB_EUNSUPPORTED, "the fused heat step computes in float32 only");
   if (int rc = stencil::check_sweep(ctx, m, {T, Tn})) return rc;
-  HeatPhys::Params p;
+  HeatParams p;
   p.cx = float(dt * k / (m->dx * m->dx));
   p.cy = float(dt * k / (m->dy * m->dy));
   p.cz = float(dt * k / (m->dz * m->dz));
-  return dispatch_tz<HeatPhys, 6>(ctx, m, T, Tn, nullptr, p, 0);
+  p.fixed = static_cast<const float*>(fixed);
+  if (fixed) return dispatch_tz<HeatPhys<true>, 6>(ctx, m, T, Tn, nullptr, p, 0);
+  return dispatch_tz<HeatPhys<false>, 6>(ctx, m, T, Tn, nullptr, p, 0);
 }
 
 int fused_d2t_step(cfdb_ctx* ctx, cfdb_mesh* m, const void* u, const void* u_prev, void* u_next, double k,

@@ -29,6 +29,17 @@ extern "C" int cfdb_heat_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, int path, 
   return plain_heat_update(ctx, dtype, p.stab_tmp, T, k, dt, Tn, m->n);
 }
 
+extern "C" int cfdb_heat_step_fixed(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* T, void* Tn, double k,
+                                    double dt, const void* fixed) {
+  if (int rc = check_step(ctx, m, dtype, CFDB_PATH_FUSED, "cfdb_heat_step_fixed")) return rc;
+  if (!T || !Tn || !fixed) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_heat_step_fixed: NULL field pointer");
+  if (T == Tn || fixed == Tn)
+    return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_heat_step_fixed: T_next must differ from T and the fixed values");
+  if (!std::isfinite(k) || !std::isfinite(dt))
+    return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_heat_step_fixed: k and dt must be finite");
+  return fused_heat_step(ctx, m, dtype, T, Tn, k, dt, fixed);
+}
+
 extern "C" int cfdb_d2t_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* u, const void* u_prev, void* u_next,
                              double k, const int32_t* masks, int32_t n_terms, double dt, int first_step) {
   if (int rc = check_step(ctx, m, dtype, CFDB_PATH_FUSED, "cfdb_d2t_step")) return rc;

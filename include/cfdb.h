@@ -251,6 +251,15 @@ int cfdb_total_fp64_noalloc(int dtype, const void* field, const void* volumes, d
 int cfdb_heat_step(cfdb_ctx* ctx, cfdb_mesh* mesh, int dtype, int path, const void* T, void* T_next, double k,
                    double dt);
 
+/* The fused heat step followed by the examples' boundary copy
+ * (examples/main_3d_heat.cpp:41-60: the cells of the box surface reset to
+ * fixed values after each step) in the same pass: T_next = the heat update
+ * inside, fixed[i] on the surface cells.  The same values as cfdb_heat_step
+ * followed by cfdb_op_boundary_set.  CFDB_F32, uniform meshes with
+ * nz % 4 == 0, 16-byte aligned T and T_next. */
+int cfdb_heat_step_fixed(cfdb_ctx* ctx, cfdb_mesh* mesh, int dtype, const void* T, void* T_next, double k, double dt,
+                         const void* fixed);
+
 /* Leapfrog step of d2t(u) = k * (L_m1(u) + L_m2(u) + ...) with L_m the
  * Laplacian over the directions of mask m (1 = d2dx, 2 = d2dy, 4 = d2dz,
  * 7 = lapl) -- the equation examples/main_3d_wave.cu builds, whose

@@ -238,6 +238,44 @@ def test_heat_fused_edge_shapes(cfdb, oracle, ctx, shape):
     assert rel_linf(host(out), ref) <= 3e-6
 
 
+@pytest.mark.parametrize("shape", [(16, 12, 8), (9, 5, 4), (3, 7, 132), (1, 1, 8)])
+def test_heat_step_fixed_equals_step_then_boundary_set(cfdb, ctx, shape):
+    """cfdb_heat_step_fixed (the boundary copy inside the fused step) gives
+    the bits of cfdb_heat_step followed by cfdb_op_boundary_set; the surface
+    cells hold the fixed values, the interior the heat update."""
+    nx, ny, nz = shape
+    m = cfdb.Mesh.structured(ctx, nx, ny, nz, 1 / nx, 1 / ny, 1 / nz)
+    g = torch.Generator(device="cpu").manual_seed(11)
+    T = torch.rand(m.n, generator=g).to(DEV)
+    fixed = torch.rand(m.n, generator=g).to(DEV) + 2.0
+    a, b = torch.empty_like(T), torch.empty_like(T)
+    ctx.heat_step(m, T, a, 0.7, 1e-6, path=cfdb.FUSED)  # stable for every shape here (k dt / h^2 < 1/6)
+    ctx.boundary_set(m, a, fixed)
+    ctx.heat_step_fixed(m, T, b, 0.7, 1e-6, fixed)
+    assert torch.equal(a, b)
+    x, y, z = torch.meshgrid(torch.arange(nx), torch.arange(ny), torch.arange(nz), indexing="ij")
+    surf = ((x == 0) | (x == nx - 1) | (y == 0) | (y == ny - 1) | (z == 0) | (z == nz - 1)).reshape(-1).to(DEV)
+    assert torch.equal(b[surf], fixed[surf])
+    assert not torch.any(b[~surf] >= 2.0)
+
+
+def test_heat_step_fixed_rejects_bad_arguments(cfdb, ctx):
+    m = cfdb.Mesh.structured(ctx, 8, 8, 8, 1 / 8, 1 / 8, 1 / 8)
+    T, Tn, fx = (torch.zeros(m.n, device=DEV) for _ in range(3))
+    for args, code in (((T, Tn, None), cfdb.capi.EINVAL), ((T, Tn, Tn), cfdb.capi.EINVAL),
+                       ((T, T, fx), cfdb.capi.EINVAL),
+                       ((T.double(), Tn.double(), fx.double()), cfdb.capi.EUNSUPPORTED)):
+        with pytest.raises(cfdb.CfdbError) as e:
+            ctx.heat_step_fixed(m, args[0], args[1], 1.0, 1e-4, args[2])
+        assert e.value.code == code
+    m6 = cfdb.Mesh.structured(ctx, 4, 4, 6, 0.25, 0.25, 1 / 6)
+    a, b, c = (torch.zeros(m6.n, device=DEV) for _ in range(3))
+    with pytest.raises(cfdb.CfdbError) as e:
+        ctx.heat_step_fixed(m6, a, b, 1.0, 1e-4, c)
+    assert e.value.code == cfdb.capi.EUNSUPPORTED
+    ctx.sync()
+
+
 def test_fused_requires_nz_multiple_of_4(cfdb, ctx):
     m = cfdb.Mesh.structured(ctx, 4, 4, 6, 0.25, 0.25, 1 / 6)
     a = torch.zeros(m.n, device=DEV)
