@@ -36,6 +36,8 @@ template <bool FIXED> struct HeatPhys {
   __device__ static void cell(const stencil::CellIn<1>& in, const Params& a, float o[NF]) {
     o[0] = heat_update(in.P[0], in.nb[0][0], in.nb[1][0], in.nb[2][0], in.nb[3][0], in.nb[4][0], in.nb[5][0], a.cx,
                        a.cy, a.cz);
+    // (loading the wall values one plane ahead instead, only where walls
+    // are, measured 3.88 against 3.83 ms per 200 steps at 200^3)
     if (FIXED && in.walls) o[0] = a.fixed[in.idx];
   }
   __device__ static void acc_init(Acc&) {}
