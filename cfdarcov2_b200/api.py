@@ -144,6 +144,13 @@ class Context:
         call("cfdb_op_boundary_copy", self.h, mesh.h, _dtype_code(arr), _ptr(arr), _ptr(copy), _ptr(out), ctx=self.h)
         return out
 
+    def boundary_set_many(self, mesh, fields, values):
+        """cfdb_op_boundary_set for several fields in one launch."""
+        n = len(fields)
+        fp = (C.c_void_p * max(n, 1))(*[t.data_ptr() for t in fields])
+        vp = (C.c_void_p * max(n, 1))(*[t.data_ptr() for t in values])
+        call("cfdb_op_boundary_set_many", self.h, mesh.h, _dtype_code(fields[0]) if n else F32, n, fp, vp, ctx=self.h)
+
     def boundary_set(self, mesh, field, values):
         """field[i] = values[i] on the boundary cells, in place."""
         call("cfdb_op_boundary_set", self.h, mesh.h, _dtype_code(field), _ptr(field), _ptr(values), ctx=self.h)

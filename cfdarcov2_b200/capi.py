@@ -104,6 +104,7 @@ PROTOTYPES = {
     "cfdb_op_d2t": (_I, [_P, _I, _P, _P, _P, _D, _I, _P, _I64]),
     "cfdb_op_boundary_copy": (_I, [_P, _P, _I, _P, _P, _P]),
     "cfdb_op_boundary_set": (_I, [_P, _P, _I, _P, _P]),
+    "cfdb_op_boundary_set_many": (_I, [_P, _P, _I, _I32, _P, _P]),
     "cfdb_cfl_dt": (_I, [_P, _P, _I, _D, _D, _P, _P, _P, _P, _P, _PD]),
     "cfdb_total_fp64": (_I, [_P, _P, _I, _P, _PD]),
     "cfdb_total_fp64_noalloc": (_I, [_I, _P, _P, _D, _I64, _P, _P]),

@@ -1268,8 +1268,34 @@ void Equation::evaluate(std::vector<Variable*>& all_vars, EquationTemplate& eqs,
         throw std::runtime_error("Equation: left-hand side must be a field, d1t(field) or d2t(field)");
       }
     }
+    // boundary functions in variable order; a run of consecutive boundary
+    // copies on one mesh goes out as one launch (each writes only its own
+    // field from its own buffer, so the run's order cannot matter)
+    std::vector<void*> set_fields;
+    std::vector<const void*> set_values;
+    Mesh3D* set_mesh = nullptr;
+    auto flush_sets = [&] {
+      if (set_fields.empty()) return;
+      check(cfdb_op_boundary_set_many(ctx, set_mesh->handle(), CFDB_F32, int32_t(set_fields.size()), set_fields.data(),
+                                      set_values.data()),
+            "cfdb_op_boundary_set_many");
+      set_fields.clear();
+      set_values.clear();
+    };
     for (Variable* v : all_vars) {
-      if (v == bc_done) {
+      const BoundaryCopyCu* copy =
+          v != bc_done && v->has_boundary_conditions_cu ? v->boundary_conditions_cu.target<BoundaryCopyCu>() : nullptr;
+      if (copy && copy->count == v->mesh->_num_nodes) {
+        if (set_mesh != v->mesh) flush_sets();
+        set_mesh = v->mesh;
+        set_fields.push_back(v->current_cu);
+        set_values.push_back(copy->buf.get());
+      } else {
+        flush_sets();
+      }
+      if (copy && copy->count == v->mesh->_num_nodes) {
+        // queued above
+      } else if (v == bc_done) {
         // applied inside the fused step
       } else if (v->has_boundary_conditions_cu) {
         v->boundary_conditions_cu(v->mesh, v->current_cu, dt);
@@ -1283,8 +1309,12 @@ void Equation::evaluate(std::vector<Variable*>& all_vars, EquationTemplate& eqs,
       }
       bool store = !CFDArcoGlobalInit::skip_history;
       for (Variable* s : store_vars) store = store || (s == v && !CFDArcoGlobalInit::skip_history);
-      if (store) v->history.push_back(v->host());
+      if (store) {
+        flush_sets();  // the stored state has its boundary copy
+        v->history.push_back(v->host());
+      }
     }
+    flush_sets();
     if (visualize) std::printf("\rstep %zu / %zu", t + 1, timesteps);
   }
   check(cfdb_sync(ctx), "cfdb_sync");

@@ -233,6 +233,34 @@ __global__ void bset_k(R* __restrict__ field, const R* __restrict__ values, int6
   }
 }
 
+// bset_k for up to kSetBatch fields in one launch: field k = blockIdx.y
+constexpr int kSetBatch = 16;
+template <class R> struct SetBatch {
+  R* field[kSetBatch];
+  const R* values[kSetBatch];
+};
+template <class R>
+__global__ void bset_many_k(SetBatch<R> b, int64_t nx, int64_t ny, int64_t nz) {
+  R* __restrict__ field = b.field[blockIdx.y];
+  const R* __restrict__ values = b.values[blockIdx.y];
+  const int64_t px = ny * nz, py = nx * nz, pz = nx * ny, total = 2 * (px + py + pz);
+  GRID_STRIDE(t, total) {
+    int64_t x, y, z;
+    if (t < 2 * px) {
+      const int64_t r = t % px;
+      x = t < px ? 0 : nx - 1, y = r / nz, z = r % nz;
+    } else if (t < 2 * (px + py)) {
+      const int64_t u = t - 2 * px, r = u % py;
+      y = u < py ? 0 : ny - 1, x = r / nz, z = r % nz;
+    } else {
+      const int64_t u = t - 2 * (px + py), r = u % pz;
+      z = u < pz ? 0 : nz - 1, x = r / ny, y = r % ny;
+    }
+    const int64_t i = (x * ny + y) * nz + z;
+    field[i] = values[i];
+  }
+}
+
 // ---- reductions -------------------------------------------------------------
 __device__ __forceinline__ void atomic_min_pos(float* a, float v) { atomicMin(reinterpret_cast<int*>(a), __float_as_int(v)); }
 __device__ __forceinline__ void atomic_min_pos(double* a, double v) {
@@ -555,6 +583,34 @@ extern "C" int cfdb_op_boundary_set(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, void
   const int64_t total = 2 * (m->ny * m->nz + m->nx * m->nz + m->nx * m->ny);
   DISPATCH(dtype, R, bset_k<R><<<grid_for(ctx, total, kThreads), kThreads, 0, ctx->stream>>>((R*)field, (const R*)values, m->nx, m->ny, m->nz));
   CFDB_LAUNCHED(ctx);
+  return CFDB_OK;
+}
+
+extern "C" int cfdb_op_boundary_set_many(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, int32_t count, void* const* fields,
+                                         const void* const* values) {
+  if (int rc = cfdb_check_mesh(ctx, m)) return rc;
+  if (!dtype_ok(dtype)) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_op_boundary_set_many: unknown dtype %d", dtype);
+  if (count < 0 || (count > 0 && (!fields || !values)))
+    return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_op_boundary_set_many: bad field list");
+  for (int32_t k = 0; k < count; ++k)
+    if (int rc = check_ptrs(ctx, "cfdb_op_boundary_set_many", {fields[k], values[k]})) return rc;
+  if (count == 0) return CFDB_OK;
+  CFDB_CUDA(ctx, cudaSetDevice(ctx->device));
+  const int64_t total = 2 * (m->ny * m->nz + m->nx * m->nz + m->nx * m->ny);
+  for (int32_t k0 = 0; k0 < count; k0 += kSetBatch) {
+    const int nb = std::min<int32_t>(kSetBatch, count - k0);
+    // one CTA row per field; the fields share the launch's x extent
+    const dim3 grid(unsigned(std::max(1, grid_for(ctx, total, kThreads) / nb)), unsigned(nb));
+    DISPATCH(dtype, R, {
+      SetBatch<R> b{};
+      for (int j = 0; j < nb; ++j) {
+        b.field[j] = static_cast<R*>(fields[k0 + j]);
+        b.values[j] = static_cast<const R*>(values[k0 + j]);
+      }
+      bset_many_k<R><<<grid, kThreads, 0, ctx->stream>>>(b, m->nx, m->ny, m->nz);
+    });
+    CFDB_LAUNCHED(ctx);
+  }
   return CFDB_OK;
 }
 

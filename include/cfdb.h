@@ -210,6 +210,12 @@ int cfdb_op_boundary_copy(cfdb_ctx* ctx, cfdb_mesh* mesh, int dtype, const void*
  * writes 2 x 6N^2 cells of an N^3 mesh instead of streaming all N^3 three
  * times. */
 int cfdb_op_boundary_set(cfdb_ctx* ctx, cfdb_mesh* mesh, int dtype, void* field, const void* values);
+/* cfdb_op_boundary_set for `count` fields at once (fields[k] from values[k]),
+ * one launch per 16 fields: the boundary copies of a system's variables
+ * after a step (src/fvm3d.cpp:1008-1049 applies them one variable at a
+ * time). */
+int cfdb_op_boundary_set_many(cfdb_ctx* ctx, cfdb_mesh* mesh, int dtype, int32_t count, void* const* fields,
+                              const void* const* values);
 
 /* UpdatePolicies::CourantFriedrichsLewy3DCu / 1DCu + cfl_cu
  * (src/fvm3d.cpp:528-567; src/cuda_operators.cu:138-235):

@@ -259,6 +259,23 @@ def test_heat_step_fixed_equals_step_then_boundary_set(cfdb, ctx, shape):
     assert not torch.any(b[~surf] >= 2.0)
 
 
+@pytest.mark.parametrize("count,dtype", [(3, torch.float32), (17, torch.float32), (2, torch.float64)])
+def test_boundary_set_many_equals_one_by_one(cfdb, ctx, count, dtype):
+    """cfdb_op_boundary_set_many (one launch per 16 fields) writes what
+    cfdb_op_boundary_set writes field by field, and nothing else."""
+    m = cfdb.Mesh.structured(ctx, 9, 6, 8, 1 / 9, 1 / 6, 1 / 8)
+    g = torch.Generator(device="cpu").manual_seed(2)
+    fields = [torch.rand(m.n, generator=g, dtype=dtype).to(DEV) for _ in range(count)]
+    values = [torch.rand(m.n, generator=g, dtype=dtype).to(DEV) for _ in range(count)]
+    one = [f.clone() for f in fields]
+    for f, v in zip(one, values):
+        ctx.boundary_set(m, f, v)
+    ctx.boundary_set_many(m, fields, values)
+    for a, b in zip(fields, one):
+        assert torch.equal(a, b)
+    ctx.boundary_set_many(m, [], [])  # nothing to do
+
+
 def test_heat_step_fixed_rejects_bad_arguments(cfdb, ctx):
     m = cfdb.Mesh.structured(ctx, 8, 8, 8, 1 / 8, 1 / 8, 1 / 8)
     T, Tn, fx = (torch.zeros(m.n, device=DEV) for _ in range(3))
