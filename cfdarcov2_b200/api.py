@@ -147,6 +147,8 @@ class Context:
     def boundary_set_many(self, mesh, fields, values):
         """cfdb_op_boundary_set for several fields in one launch."""
         n = len(fields)
+        if len(values) != n or any(t.dtype != fields[0].dtype for t in list(fields) + list(values)):
+            raise ValueError("boundary_set_many: one values tensor per field, all of one dtype")
         fp = (C.c_void_p * max(n, 1))(*[t.data_ptr() for t in fields])
         vp = (C.c_void_p * max(n, 1))(*[t.data_ptr() for t in values])
         call("cfdb_op_boundary_set_many", self.h, mesh.h, _dtype_code(fields[0]) if n else F32, n, fp, vp, ctx=self.h)
