@@ -296,7 +296,10 @@ const float* eval_node(Node* n) {
 // operator header for meshes below 2^31 / 18 cells) cut the largest group's
 // registers from 80 to 72 but slowed the Euler system from 214 to 229 ms per
 // 200 steps at 200^3; __launch_bounds__(256, 4) on the group kernels (64
-// registers, 40 bytes of spills in the largest) ran 220 ms.
+// registers, 40 bytes of spills in the largest) ran 220 ms; CTAs tiled as
+// 32 z x 8 y cells of cpt consecutive x planes (y neighbours from the same
+// CTA, x neighbours from the thread's own cells) ran 236 ms against 206 ms
+// for the linear chunks.
 constexpr int kCptEquation = 4;
 constexpr int kCptGroup = 1;
 constexpr int kCptStab = 1;
