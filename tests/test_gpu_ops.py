@@ -311,7 +311,8 @@ def test_fused_requires_nz_multiple_of_4(cfdb, ctx):
                                                    ((9, 4, 8), (1.0, 1.0, 1.0), [1, 2, 4], 0.25),
                                                    ((12, 8, 8), (1.0, 1.0, 1.0), [7], 0.7),
                                                    ((8, 8, 8), (1.0, 1.0, 1.0), [2, 1], 1.3),
-                                                   ((16, 8, 8), (0.5, 0.5, 0.5), [1, 2], 0.2)])
+                                                   ((16, 8, 8), (0.5, 0.5, 0.5), [1, 2], 0.2),
+                                                   ((4, 3, 136), (1.0, 1.0, 1.0), [1, 2], 0.09)])
 def test_d2t_fused_equals_operator_composition_bitwise(cfdb, ctx, shape, spacing, masks, k):
     """cfdb_d2t_step (one TMA pass) gives the bits of the operator kernels
     composed as the generated kernel of d2t(u) = k (L_m1(u) + L_m2(u) + ...)
@@ -319,7 +320,7 @@ def test_d2t_fused_equals_operator_composition_bitwise(cfdb, ctx, shape, spacing
     then the leapfrog update (first step: the d1t form).  Covers unit cells
     (products by one left out), power-of-two volumes (an exact 1/V) and
     V = 3 (a true division), each with the masks compiled in ([1, 2], [7],
-    [1, 2, 4]) and read at run time."""
+    [1, 2, 4]) and read at run time; nz = 136 takes the 64-wide tiles."""
     m = cfdb.Mesh.structured(ctx, *shape, *spacing)
     assert m.lattice_geometry()[0]
     g = torch.Generator(device="cpu").manual_seed(5)
