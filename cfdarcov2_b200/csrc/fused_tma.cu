@@ -215,12 +215,13 @@ int dispatch_tz(cfdb_ctx* ctx, const cfdb_mesh* m, const void* q, void* out, con
   return stencil::launch_sweep<Phys, 32, 8, S>(ctx, m, q, nullptr, c, out, prm, ctas_per_sm);
 }
 
-// Tile width of the wave-template sweeps: 64 where it pads the z rows less
-// than 128 (nz = 400: 448 against 512 cells per row, 126 against 156 us per
-// step), else as dispatch_tz.  The heat sweep keeps 128 at nz = 400 (112 us
-// against 123 us with 64).
+// Tile width of the wave-template sweeps and of the heat sweep with the
+// boundary copy: 64 where it pads the z rows less than 128 (nz = 400: 448
+// against 512 cells per row; 126 against 156 us per d2t step, 158 against
+// 176 us per heat step with the copy), else as dispatch_tz.  The plain heat
+// sweep keeps 128 at nz = 400 (112 us against 123 us with 64).
 template <class Phys>
-int dispatch_d2t(cfdb_ctx* ctx, const cfdb_mesh* m, const void* u, void* u_next, const typename Phys::Params& prm) {
+int dispatch_padded(cfdb_ctx* ctx, const cfdb_mesh* m, const void* u, void* u_next, const typename Phys::Params& prm) {
   const int64_t pad64 = (m->nz + 63) / 64 * 64, pad128 = (m->nz + 127) / 128 * 128;
   if (m->nz >= 128 && pad64 < pad128)
     return stencil::launch_sweep<Phys, 64, 8, 6>(ctx, m, u, nullptr, nullptr, u_next, prm, 0);
@@ -257,7 +258,7 @@ int fused_heat_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* T, void*
   p.cy = float(dt * k / (m->dy * m->dy));
   p.cz = float(dt * k / (m->dz * m->dz));
   p.fixed = static_cast<const float*>(fixed);
-  if (fixed) return dispatch_tz<HeatPhys<true>, 6>(ctx, m, T, Tn, nullptr, p, 0);
+  if (fixed) return dispatch_padded<HeatPhys<true>>(ctx, m, T, Tn, p);
   return dispatch_tz<HeatPhys<false>, 6>(ctx, m, T, Tn, nullptr, p, 0);
 }
 
@@ -303,17 +304,17 @@ int fused_d2t_step(cfdb_ctx* ctx, cfdb_mesh* m, const void* u, const void* u_pre
   // compiled with their masks
   constexpr int XY = 1 | 2 << 3, LAPL = 7, XYZ = 1 | 2 << 3 | 4 << 6;
   if (unit) {
-    if (form == XY) return dispatch_d2t<D2tPhys<D2T_UNIT, XY>>(ctx, m, u, u_next, p);
-    if (form == LAPL) return dispatch_d2t<D2tPhys<D2T_UNIT, LAPL>>(ctx, m, u, u_next, p);
-    if (form == XYZ) return dispatch_d2t<D2tPhys<D2T_UNIT, XYZ>>(ctx, m, u, u_next, p);
-    return dispatch_d2t<D2tPhys<D2T_UNIT, -1>>(ctx, m, u, u_next, p);
+    if (form == XY) return dispatch_padded<D2tPhys<D2T_UNIT, XY>>(ctx, m, u, u_next, p);
+    if (form == LAPL) return dispatch_padded<D2tPhys<D2T_UNIT, LAPL>>(ctx, m, u, u_next, p);
+    if (form == XYZ) return dispatch_padded<D2tPhys<D2T_UNIT, XYZ>>(ctx, m, u, u_next, p);
+    return dispatch_padded<D2tPhys<D2T_UNIT, -1>>(ctx, m, u, u_next, p);
   }
   if (recip) {
-    if (form == XY) return dispatch_d2t<D2tPhys<D2T_RECIP, XY>>(ctx, m, u, u_next, p);
-    if (form == LAPL) return dispatch_d2t<D2tPhys<D2T_RECIP, LAPL>>(ctx, m, u, u_next, p);
-    return dispatch_d2t<D2tPhys<D2T_RECIP, -1>>(ctx, m, u, u_next, p);
+    if (form == XY) return dispatch_padded<D2tPhys<D2T_RECIP, XY>>(ctx, m, u, u_next, p);
+    if (form == LAPL) return dispatch_padded<D2tPhys<D2T_RECIP, LAPL>>(ctx, m, u, u_next, p);
+    return dispatch_padded<D2tPhys<D2T_RECIP, -1>>(ctx, m, u, u_next, p);
   }
-  return dispatch_d2t<D2tPhys<D2T_DIVIDE, -1>>(ctx, m, u, u_next, p);
+  return dispatch_padded<D2tPhys<D2T_DIVIDE, -1>>(ctx, m, u, u_next, p);
 }
 
 int fused_wave_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* q, void* qn, const void* c, double cconst,
