@@ -51,7 +51,7 @@ def parse():
 
 def workload_config(n, tsteps):
     return {"workload": f"wave3d_rusanov_{n}^3_x{tsteps}_steps", "mesh": [n, n, n], "time_steps_per_bench_step": tsteps,
-            "fields": 4, "path": "fused_tma_sweep", "cfl": 0.4, "c": 1.0,
+            "fields": 4, "cfl": 0.4, "c": 1.0,
             "l2": "flushed between bench steps (512 MB write); the 67 MB ping-pong working set stays L2-resident within a solve",
             "parallelism": "replica per GPU"}
 
@@ -174,6 +174,8 @@ def run_reference(args, rank):
             "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": workload_config(n, args.tsteps), "impl": "reference",
+            "path": f"CPU restatement of the reference's operator-by-operator path, FP32, {cores} host threads; "
+                    f"each bench step times a {per_step}-time-step sample of the workload",
             "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": cores, "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -313,6 +315,7 @@ def run_native(args, rank, world, local_rank):
         "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Gaussian pulse)",
         "config": workload_config(n, T),
+        "path": "fused TMA sweep (one sm_100a kernel per time step), CUDA graph replay",
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
                      "kernel": "stencil::sweep_kernel<WavePhys<false>,128,8,3,4>",
