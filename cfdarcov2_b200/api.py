@@ -66,6 +66,10 @@ class Context:
         call("cfdb_ctx_launch_count", self.h, C.byref(v), ctx=self.h)
         return v.value
 
+    def set_wait_limit(self, cycles: int = 4000000000, missing_plane: int = -1) -> None:
+        """Bound of the sweep kernels' device waits; missing_plane >= 0 is the timeout test hook."""
+        call("cfdb_ctx_set_wait_limit", self.h, int(cycles), int(missing_plane), ctx=self.h)
+
     def trim(self) -> None:
         """Returns the workspace cached by earlier calls (checkpoint slots and
         the like) to the device."""

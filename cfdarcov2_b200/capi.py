@@ -72,6 +72,7 @@ PROTOTYPES = {
     "cfdb_ctx_allocated_bytes": (_I, [_P, _PI64]),
     "cfdb_ctx_trim": (_I, [_P]),
     "cfdb_ctx_launch_count": (_I, [_P, _PI64]),
+    "cfdb_ctx_set_wait_limit": (_I, [_P, _I64, _I32]),
     "cfdb_kernel_build": (_I, [_P, C.c_char_p, C.c_char_p, _PP]),
     "cfdb_kernel_build_many": (_I, [_P, _I, C.POINTER(C.c_char_p), C.POINTER(C.c_char_p), _PP]),
     "cfdb_kernel_launch": (_I, [_P, _I64, _I, _P]),

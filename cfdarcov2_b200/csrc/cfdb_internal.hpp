@@ -74,6 +74,10 @@ struct cfdb_ctx {
   cudaMemPool_t pool = nullptr;
   std::unordered_map<void*, int64_t> ws;
   int* d_error = nullptr;  // device error word written by bounded waits
+  // Bound of the sweep kernels' mbarrier waits (SM clock cycles) and the
+  // missing-copy test hook (cfdb_ctx_set_wait_limit).
+  long long wait_cycles = 4000000000LL;
+  int missing_plane = -1;
   cudaStream_t capture_stream = nullptr;  // private stream used to record CUDA graphs
   // Kernels launched on this context so far (graph replays count every
   // kernel node they run).

@@ -21,7 +21,10 @@
 //  * the first call on a device resolves the array's device address with
 //    cudaGetSymbolAddress (host code cannot pass the array's name to a kernel:
 //    on the host it is only a stand-in, not a device address); make that first
-//    call outside any stream capture.
+//    call outside any stream capture.  The address is cached per device for
+//    the life of the process: after cudaDeviceReset (which unloads the
+//    library's device code) the library must be unloaded and loaded again
+//    before this entry point is used on that device.
 #include <cmath>
 #include <mutex>
 
@@ -75,13 +78,23 @@ __global__ void chunk_total_k(const R* __restrict__ f, const R* __restrict__ vol
   }
 }
 
+// One warp: lane l folds partials l, l + 32, l + 64, ... (coalesced loads,
+// at most 2048 dependent adds per lane at the maximum size), then the lanes
+// merge pairwise through shuffles in a fixed order, so the result does not
+// depend on timing.
 __global__ void chunk_final_k(const Pair* __restrict__ part, int np, Pair* __restrict__ slot, double* __restrict__ out) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    Pair t{0.0, 0.0};
-    for (int k = 0; k < np; ++k) {
-      pair_add(t, part[k].s);
-      t.c += part[k].c;
-    }
+  Pair t{0.0, 0.0};
+  for (int k = int(threadIdx.x); k < np; k += 32) {
+    pair_add(t, part[k].s);
+    t.c += part[k].c;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double s = __shfl_xor_sync(0xffffffffu, t.s, o);
+    const double c = __shfl_xor_sync(0xffffffffu, t.c, o);
+    pair_add(t, s);
+    t.c += c;
+  }
+  if (threadIdx.x == 0) {
     *slot = t;
     *out = t.s + t.c;
   }

@@ -178,6 +178,17 @@ extern "C" int cfdb_ctx_launch_count(const cfdb_ctx* ctx, int64_t* out) {
   return CFDB_OK;
 }
 
+
+extern "C" int cfdb_ctx_set_wait_limit(cfdb_ctx* ctx, int64_t cycles, int32_t missing_plane) {
+  if (!ctx) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_ctx_set_wait_limit: ctx is NULL");
+  if (cycles < 1000) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_ctx_set_wait_limit: cycles must be >= 1000");
+  if (missing_plane < -1) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_ctx_set_wait_limit: missing_plane must be >= -1");
+  ctx->wait_cycles = cycles;
+  ctx->missing_plane = missing_plane;
+  cfdb_graphs_clear(ctx);  // recorded launches carry the old values
+  return CFDB_OK;
+}
+
 extern "C" int cfdb_ctx_trim(cfdb_ctx* ctx) {
   if (!ctx) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_ctx_trim: ctx is NULL");
   if (!ctx->pool) return CFDB_OK;

@@ -123,7 +123,7 @@ int launch_sweep(cfdb_ctx* ctx, const cfdb_mesh* m, const void* q, const void* a
     resident_of[ctx->device].store(resident, std::memory_order_release);
   }
   const SweepShape sh = sweep_shape(ctx, m, TZ, TY, ctas_per_sm > 0 ? std::min(ctas_per_sm, resident) : resident);
-  Geometry g{int(m->nx), int(m->ny), int(m->nz), sh.chunks, (long long)m->n};
+  Geometry g{int(m->nx), int(m->ny), int(m->nz), sh.chunks, (long long)m->n, ctx->wait_cycles, ctx->missing_plane};
   // Programmatic stream serialisation: the CTAs of this step may become
   // resident while the previous kernel drains; the kernel waits for it
   // (griddepcontrol.wait) before touching global memory.

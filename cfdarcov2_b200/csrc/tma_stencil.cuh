@@ -72,14 +72,15 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
 __device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void grid_dep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
-// Bounded wait: gives up after ~2 s of SM clocks so a lost transaction can
-// never hang the GPU; the caller records the failure in the error word.
+// Bounded wait: gives up after `limit` SM clock cycles (default ~2 s) so a
+// lost transaction can never hang the GPU; the caller records the failure in
+// the error word.
 constexpr long long kWaitCycles = 4000000000LL;
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, long long limit) {
   if (mbar_try_wait(bar, parity)) return true;
   const long long t0 = clock64();
   while (!mbar_try_wait(bar, parity))
-    if (clock64() - t0 > kWaitCycles) return false;
+    if (clock64() - t0 > limit) return false;
   return true;
 }
 
@@ -93,6 +94,11 @@ struct Geometry {
   int X, Y, Z;      // cells
   int chunks;       // x chunks; chunk c covers planes [c X / chunks, (c+1) X / chunks)
   long long n;      // X*Y*Z
+  long long wait_cycles;  // bound of every mbarrier wait, SM clock cycles
+  // Test hook (-1: off): CTA (0, 0) arms the barrier of its plane k ==
+  // missing_plane with the plane's byte count but issues no copy for it, so
+  // the wait on that plane runs out (the timeout path, without a fault).
+  int missing_plane;
 };
 
 // Staged fields of one cell and its six neighbours (x-, x+, y-, y+, z-, z+).
@@ -209,6 +215,13 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
   // for TMA, which is checked before the first copy is issued.
   extern __shared__ __align__(128) float smem[];
   __shared__ __align__(8) uint64_t bars[S];
+  // Issuer bookkeeping in shared memory (thread 0 only), so it holds no
+  // register through the plane loop: the last plane whose copies were
+  // issued, and, once a wait gave up, the copies to drain (bit s: slot s
+  // holds an issued copy not waited on yet; bit 16 + s: its parity).
+  static_assert(S <= 16, "the drain word holds 16 slots");
+  __shared__ int last_issued;
+  __shared__ uint32_t drain;
 
   const int ntz = (g.Z + TZ - 1) / TZ;
   const int z0 = (blockIdx.x % ntz) * TZ;
@@ -244,15 +257,24 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
     fence_mbar_init();
+    last_issued = -1;
+    drain = 0;
   }
   __syncthreads();
 
+  // A wait that gives up (bad) ends the staging: the issuing thread (0)
+  // issues nothing more and lets the copies it already issued land before
+  // the CTA can exit, every later wait is skipped, and the error word
+  // reports the timeout.  The results of such a launch are invalid.
+  bool bad = false;
   auto issue = [&](int k) {
     const int x = x0 - 1 + k;
-    if (k > kmax || x < 0 || x >= g.X) return;
+    if (bad || k > kmax || x < 0 || x >= g.X) return;
     const int s = k % S;
     float* dst = smem + s * L::SLOT;
     mbar_expect_tx(&bars[s], L::TX_BYTES);
+    last_issued = k;
+    if (k == g.missing_plane && blockIdx.x == 0 && blockIdx.y == 0) return;
     tma_load_4d(dst, &tm_q, z0 - 4, y0 - 1, x, 0, &bars[s]);
     if constexpr (NA > 0) tma_load_4d(dst + L::A_OFF, &tm_a, z0 - 4, y0 - 1, x, 0, &bars[s]);
     if constexpr (Phys::HAS_C) tma_load_3d(dst + L::C_OFF, &tm_c, z0 - 4, y0 - 1, x, &bars[s]);
@@ -261,11 +283,21 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
     for (int k = 0; k < S; ++k) issue(k);
 
   uint32_t parity = 0;  // bit s: parity of the next completion of slot s
-  bool bad = false;
   auto wait_plane = [&](int k) {
     const int s = k % S;
-    if (!mbar_wait_bounded(&bars[s], (parity >> s) & 1u)) bad = true;
+    const uint32_t par = (parity >> s) & 1u;
     parity ^= 1u << s;
+    if (bad) return;
+    if (!mbar_wait_bounded(&bars[s], par, g.wait_cycles)) {
+      bad = true;
+      // planes k+1 .. last_issued sit in other slots, none waited on yet:
+      // their bits in `parity` are the parities of those copies' completions
+      if (threadIdx.x == 0) {
+        uint32_t d = (parity & 0xffffu) << 16;
+        for (int j = k + 1; j <= last_issued; ++j) d |= 1u << (j % S);
+        drain = d;
+      }
+    }
   };
   const int ctr = (ty + 1) * L::RL + 4 + VZ * tz;  // thread's first cell in a field tile
   auto load_center = [&](int k, float v[FT][VZ]) {
@@ -593,7 +625,13 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
       for (int j = 0; j < VZ; ++j) preC[j] = preN[j];
     }
   }
-  if (bad) atomicExch(err, kErrWaitTimeout);
+  if (bad) {
+    // the copies still in flight land in shared memory before the CTA exits
+    if (threadIdx.x == 0)
+      for (int t = 0; t < S; ++t)
+        if ((drain >> t) & 1u) mbar_wait_bounded(&bars[t], (drain >> (16 + t)) & 1u, g.wait_cycles);
+    atomicExch(err, kErrWaitTimeout);
+  }
   Phys::finish(acc, P, active);
 }
 

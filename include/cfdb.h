@@ -110,6 +110,17 @@ int cfdb_ctx_allocated_bytes(const cfdb_ctx* ctx, int64_t* out);
  * never trimmed. */
 int cfdb_ctx_trim(cfdb_ctx* ctx);
 
+/* Bound of every device-side wait of the TMA sweep kernels, in SM clock
+ * cycles (default 4e9, about 2 s), after which a launch gives up, lets the
+ * copies it issued land, and reports CFDB_ETIMEOUT through cfdb_sync; its
+ * results are then invalid and the context stays usable.  missing_plane >= 0
+ * is a test hook: the first CTA of every later sweep arms that plane's
+ * barrier without issuing its copy, so the wait runs out without any fault
+ * (-1 turns it off).  Drops the context's cached step graphs.  No reference
+ * counterpart: the reference's kernels have no waits, and gpuAssert exits
+ * the process on any CUDA error (include/cuda_operators.hpp:29-36). */
+int cfdb_ctx_set_wait_limit(cfdb_ctx* ctx, int64_t cycles, int32_t missing_plane);
+
 /* Kernels this context has launched so far, those run by CUDA-graph replays
  * included (each replay adds the kernels it runs).  No reference
  * counterpart; benchmarks read it around a timed region. */
@@ -244,7 +255,9 @@ int cfdb_total_fp64(cfdb_ctx* ctx, cfdb_mesh* mesh, int dtype, const void* field
  * it uses, so nothing needs clearing, but all calls share it: calls that
  * overlap on the GPU race and must be serialised by the caller.  The first
  * call on a device looks up the scratch's device address; make it before any
- * stream capture.  Errors are read with cfdb_last_error(NULL). */
+ * stream capture.  That address is kept for the life of the process: after a
+ * cudaDeviceReset, reload the library before calling this again on that
+ * device.  Errors are read with cfdb_last_error(NULL). */
 int cfdb_total_fp64_noalloc(int dtype, const void* field, const void* volumes, double volume, int64_t n,
                             void* stream, double* out_device);
 
