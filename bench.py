@@ -140,15 +140,20 @@ def cpu_restatement_rate(n, tsteps_cap=400, budget_s=10.0, threads=None):
     import numpy as np
     from oracle import oracle as O
     from cfdarcov2_b200.workloads import wave_config
+    prev = O.max_threads()
     if threads:
         O.set_threads(threads)
-    cfg = wave_config(n=n)
-    m = O.Mesh(n, n, n, cfg["dx"], cfg["dx"], cfg["dx"], dtype=np.float32)
-    done, secs = 0, 0.0
-    while secs < budget_s and done < tsteps_cap:
-        secs += m.wave_time(cfg["q0"], cfg["dt"], 2, faithful=True)
-        done += 2
-    return n ** 3 * done / secs, done, O.max_threads()
+    try:
+        cfg = wave_config(n=n)
+        m = O.Mesh(n, n, n, cfg["dx"], cfg["dx"], cfg["dx"], dtype=np.float32)
+        done, secs = 0, 0.0
+        while secs < budget_s and done < tsteps_cap:
+            secs += m.wave_time(cfg["q0"], cfg["dt"], 2, faithful=True)
+            done += 2
+        cores = O.max_threads()
+    finally:
+        O.set_threads(prev)
+    return n ** 3 * done / secs, done, cores
 
 
 def run_reference(args, rank):
@@ -246,27 +251,33 @@ def run_native(args, rank, world, local_rank):
     dev_ms = float(t_max.item())
     value = world * cells * T * args.steps / (dev_ms * 1e-3)
 
-    # end to end through the C ABI with host buffers: H2D of the initial state,
-    # the solve, D2H of the final state, every step.  Sequential form: each
+    # End to end through the C ABI with host buffers: the initial state goes
+    # up from page-locked host memory (cfdb_upload), the solve runs, the final
+    # state comes back (cfdb_download), every step.  Sequential form: each
     # step's copies and solve back to back on one stream.
+    nbytes = q0_host.numel() * 4
     out_host = torch.empty_like(q0_host).pin_memory()
     ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     barrier()
     for k in range(args.steps):
         flush.zero_()
         ev2[k][0].record(stream)
-        a.copy_(q0_host, non_blocking=True)
+        ctx.upload(a, src_ptr=q0_host.data_ptr(), nbytes=nbytes, wait=False)
         fin = solve()
-        out_host.copy_(fin, non_blocking=True)
+        ctx.download(fin, dst_ptr=out_host.data_ptr(), nbytes=nbytes, wait=False)
         ev2[k][1].record(stream)
     torch.cuda.synchronize()
     seq_ms = sum(s.elapsed_time(e) for s, e in ev2)
 
     # Pipelined form (what a caller streaming solves does): step k+1's input
-    # copy and step k's result copy run on a second stream (the copy engines)
-    # while step k solves; two buffer pairs and two pinned result buffers
-    # alternate.  Timed from the first H2D to the last D2H, L2 flush included.
+    # copy and step k's result copy run through a second context bound to a
+    # copy stream (cfdb_upload_async / cfdb_download_async on the copy
+    # engines) while step k solves; two buffer pairs and two pinned result
+    # buffers alternate.  Timed from the first H2D to the last D2H, L2 flush
+    # included.
     copy = torch.cuda.Stream(dev)
+    cctx = cfdb.Context(local_rank)
+    cctx.set_stream(copy.cuda_stream)
     pairs = [(a, b), (torch.empty_like(q0), torch.empty_like(q0))]
     outs = [out_host, torch.empty_like(q0_host).pin_memory()]
     K = args.steps
@@ -280,24 +291,23 @@ def run_native(args, rank, world, local_rank):
     torch.cuda.synchronize()
     t_start.record(stream)
     copy.wait_stream(stream)
-    with torch.cuda.stream(copy):
-        pairs[0][0].copy_(q0_host, non_blocking=True)
-        h2d[0].record(copy)
+    cctx.upload(pairs[0][0], src_ptr=q0_host.data_ptr(), nbytes=nbytes, wait=False)
+    h2d[0].record(copy)
     for k in range(K):
         ak, bk = pairs[k % 2]
         stream.wait_event(h2d[k])
         flush.zero_()
         fin = ctx.wave_run(mesh, ak, bk, cfg["dt"], T, c_const=cfg["c"], path=cfdb.FUSED, use_graph=not args.eager)
         done[k].record(stream)
-        with torch.cuda.stream(copy):
-            if k + 1 < K:  # the other pair's last result was copied out earlier on this stream
-                pairs[(k + 1) % 2][0].copy_(q0_host, non_blocking=True)
-                h2d[k + 1].record(copy)
-            copy.wait_event(done[k])
-            outs[k % 2].copy_(fin, non_blocking=True)
+        if k + 1 < K:  # the other pair's last result was copied out earlier on the copy stream
+            cctx.upload(pairs[(k + 1) % 2][0], src_ptr=q0_host.data_ptr(), nbytes=nbytes, wait=False)
+            h2d[k + 1].record(copy)
+        copy.wait_event(done[k])
+        cctx.download(fin, dst_ptr=outs[k % 2].data_ptr(), nbytes=nbytes, wait=False)
     stream.wait_stream(copy)
     t_end.record(stream)
     torch.cuda.synchronize()
+    cctx.close()
     e2e_ms = t_start.elapsed_time(t_end)
     t2 = torch.tensor([e2e_ms, seq_ms], dtype=torch.float64, device=dev)
     if world > 1:
@@ -322,8 +332,9 @@ def run_native(args, rank, world, local_rank):
                      "algorithmic_bytes_per_cell_update": ALG_BYTES},
         "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": int(q0_host.numel() * 4),
                 "d2h_bytes_per_step": int(out_host.numel() * 4),
-                "form": "pipelined: step k+1's H2D and step k's D2H on a copy stream during step k's solve; "
-                        "timed first H2D to last D2H, L2 flush between steps included",
+                "form": "pipelined through the C ABI (cfdb_upload_async / cfdb_download_async on a second "
+                        "context's copy stream, page-locked host buffers): step k+1's H2D and step k's D2H during "
+                        "step k's solve; timed first H2D to last D2H, L2 flush between steps included",
                 "sequential": {"value": seq_value, "unit": "cell-updates/s",
                                "note": "copies and solve back to back on one stream, per-step events"}},
         "gpu_launches": launches,  # counted by the library (cfdb_ctx_launch_count), graph replays included
@@ -339,6 +350,12 @@ def run_native(args, rank, world, local_rank):
             rate, done, cores = cpu_restatement_rate(n)
             line["cpu_baseline"] = {"value": rate, "unit": "cell-updates/s", "cores": cores, "kind": "port",
                                     "sample": f"{n}^3 wave, {done} time steps, FP32 operator-by-operator CPU restatement"}
+            rate1, done1, _ = cpu_restatement_rate(n, budget_s=5.0, threads=1)
+            line["cpu_baseline_1thread"] = {"value": rate1, "unit": "cell-updates/s", "cores": 1, "kind": "port",
+                                            "sample": f"{n}^3 wave, {done1} time steps, FP32 operator-by-operator "
+                                                      "CPU restatement"}
+            # the other benchmark workloads at their own sizes, timed in this same run
+            line["configs"] = run_configs(ctx, cfdb, dev, flush)
         print(json.dumps(line), flush=True)
 
 
@@ -427,32 +444,31 @@ def _timed(fn, steps, warmup, flush, prep=None, ctx=None):
     return total
 
 
-def _line(args, workload, value, ms_per_step, cfg, alg_bytes_per_update, updates_per_launch, launches_per_step,
+def _line(S, workload, value, ms_per_step, cfg, alg_bytes_per_update, updates_per_launch, launches_per_step,
           extra, dtype="f32", launches=None, traffic_profile=None):
-    """One JSON line.  launches_per_step: time steps per bench step (the
-    roofline's per-step time); launches: kernels counted by the library in
-    the timed region (gpu_launches)."""
+    """One workload's line.  launches_per_step: time steps per bench step
+    (the roofline's per-launch time); launches: kernels counted by the
+    library in the timed region (gpu_launches)."""
     peak, kind = measured_peak_hbm()
     launch_ms = ms_per_step / launches_per_step
     ach = alg_bytes_per_update * updates_per_launch / (launch_ms * 1e-3) / 1e9
-    line = {"metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+    line = {"metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": 1, "steps": S.steps,
+            "warmup": S.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded)", "config": dict(cfg, workload=workload),
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                          "traffic": profiled_traffic(traffic_profile) if traffic_profile else None,
                          "traffic_source": f"profiles/{traffic_profile}" if traffic_profile else None,
                          "peak_source": f"{kind} hbm_gbs",
                          "algorithmic_bytes_per_cell_update": alg_bytes_per_update},
-            "gpu_launches": launches if launches is not None else args.steps * launches_per_step}
+            "gpu_launches": launches if launches is not None else S.steps * launches_per_step}
     line.update(extra)
-    print(json.dumps(line), flush=True)
+    return line
 
 
-def _cpu_baseline(fn, cells_per_call, sample, budget_s=4.0, max_calls=40):
-    """cpu_baseline of a secondary line: the CPU restatement (oracle) timed on
-    all host threads on a bounded sample of the workload.  fn() runs one call
-    and returns its seconds (or None: wall time is used); cells_per_call =
-    cell-updates one call performs."""
+def _cpu_baseline(fn, cells_per_call, sample, budget_s=3.0, max_calls=40):
+    """The CPU restatement (oracle) timed on the host's threads on a bounded
+    sample of the workload.  fn() runs one call and returns its seconds (or
+    None: wall time is used); cells_per_call = cell-updates one call does."""
     from oracle import oracle as O
     secs, calls = 0.0, 0
     while secs < budget_s and calls < max_calls:
@@ -464,237 +480,358 @@ def _cpu_baseline(fn, cells_per_call, sample, budget_s=4.0, max_calls=40):
             "sample": f"{calls} x ({sample})"}
 
 
-def run_secondary(args):
+def _cpu_pair(fn, cells_per_call, sample, budget_s=3.0, max_calls=40):
+    """cpu_baseline on all host threads and cpu_baseline_1thread on one."""
+    from oracle import oracle as O
+    out = {"cpu_baseline": _cpu_baseline(fn, cells_per_call, sample, budget_s, max_calls)}
+    nt = O.max_threads()
+    O.set_threads(1)
+    try:
+        out["cpu_baseline_1thread"] = _cpu_baseline(fn, cells_per_call, sample, budget_s, max_calls)
+    finally:
+        O.set_threads(nt)
+    return out
+
+
+class Settings:
+    """Repetitions of one secondary measurement: steps/warmup timed calls of
+    the FP32 fused solve, ref_steps of the FP64 plain one; extras = the
+    beyond-L2 run and the CPU baselines; eager = no CUDA graphs."""
+
+    def __init__(self, steps, warmup, ref_steps, extras=True, eager=False):
+        self.steps, self.warmup, self.ref_steps, self.extras, self.eager = steps, warmup, ref_steps, extras, eager
+
+
+def _rel(a, b):
+    import numpy as np
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b)), float(np.abs(a - b).max() / np.abs(b).max())
+
+
+def bench_heat(ctx, cfdb, dev, flush, S, tsteps=None):
     import numpy as np
     import torch
 
-    import cfdarcov2_b200 as cfdb
     from cfdarcov2_b200 import workloads as W
-
-    dev = torch.device("cuda", 0)
-    ctx = cfdb.Context(0)
-    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    K, Wm = args.steps, args.warmup
-
-    def l2(a, b):
-        a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
-        return float(np.linalg.norm(a - b) / np.linalg.norm(b)), float(np.abs(a - b).max() / np.abs(b).max())
-
-    if args.workload == "heat":
-        cfg = W.heat_config(steps=args.tsteps or 200)
-        n, T = cfg["n"], cfg["steps"]
-        m = cfdb.Mesh.structured(ctx, n, n, n, cfg["dx"], cfg["dx"], cfg["dx"])
-        res = {}
-        for name, dt_, path in (("fp32_fused", torch.float32, cfdb.FUSED), ("fp64_plain", torch.float64, cfdb.PLAIN))[: 1 if args.no_extras else 2]:
-            T0 = torch.tensor(cfg["T0"], dtype=dt_, device=dev)
-            a, b = torch.empty_like(T0), torch.empty_like(T0)
-            out = {}
-            ms = _timed(lambda: out.__setitem__("f", ctx.heat_run(m, a, b, cfg["k"], cfg["dt"], T, path=path, use_graph=not args.eager)),
-                        K, Wm, flush, prep=lambda: a.copy_(T0), ctx=ctx)
-            res[name] = (n ** 3 * T * K / (ms * 1e-3), ms / K, out["f"].double().cpu().numpy(), LAUNCHES["last"])
-        if args.no_extras:
-            res["fp64_plain"] = res["fp32_fused"]
-        err = l2(res["fp32_fused"][2], res["fp64_plain"][2])
-        extra = {"fp64_plain": {"value": res["fp64_plain"][0], "unit": "cell-updates/s"},
-                 "speedup_fused_fp32_vs_plain_fp64": res["fp32_fused"][0] / res["fp64_plain"][0],
-                 "accuracy_vs_fp64": {"l2_rel": err[0], "linf_rel": err[1]},
-                 "path": "cluster-resident (one launch per solve)" if res["fp32_fused"][3] == K else "per-step sweep"}
-        if not args.no_extras:
-            # the same step beyond L2: 512^3 (2 x 537 MB), 50 steps, per-step TMA sweep
-            nb, Tb = 512, 50
-            mb = cfdb.Mesh.structured(ctx, nb, nb, nb, 1 / nb, 1 / nb, 1 / nb)
-            Tl = torch.rand(nb ** 3, dtype=torch.float32, device=dev)
-            al, bl = Tl.clone(), torch.empty_like(Tl)
-            dtb = 0.1 * (1 / nb) ** 2 / cfg["k"]
-            msb = _timed(lambda: ctx.heat_run(mb, al, bl, cfg["k"], dtb, Tb, path=cfdb.FUSED, use_graph=True), 3, 2,
-                         flush, prep=lambda: al.copy_(Tl)) / 3 / Tb
-            peak, _ = measured_peak_hbm()
-            ach = 8 * nb ** 3 / (msb * 1e-3) / 1e9
-            extra["roofline_beyond_l2"] = {"mesh": [nb] * 3, "time_steps": Tb, "achieved": ach, "peak": peak,
-                                           "unit": "GB/s", "frac": ach / peak, "ms_per_step": msb,
-                                           "cell_updates_per_s": nb ** 3 / (msb * 1e-3)}
-            del mb, Tl, al, bl
-            from oracle import oracle as O
-            oc = O.Mesh(n, n, n, cfg["dx"], cfg["dx"], cfg["dx"], dtype=np.float32)
-            extra["cpu_baseline"] = _cpu_baseline(lambda: oc.heat_time(cfg["T0"], cfg["k"], cfg["dt"], 10, faithful=True),
-                                                  n ** 3 * 10, f"{n}^3 heat, 10 steps, FP32 operator-by-operator")
-        _line(args, "heat3d_64^3_x200_steps", res["fp32_fused"][0], res["fp32_fused"][1],
-              {"mesh": [n] * 3, "k": cfg["k"], "dt": cfg["dt"], "time_steps_per_bench_step": T}, 8, n ** 3, T,
-              extra, launches=res["fp32_fused"][3])
-    elif args.workload == "wave_distorted":
-        cfg = W.wave_config(n=args.n, steps=args.tsteps or 500)
-        n, T = cfg["n"], cfg["steps"]
-        V = W.jittered_vertices(n, seed=2)
-        m = cfdb.Mesh.from_vertices(ctx, n, n, n, cfg["dx"], cfg["dx"], cfg["dx"], V)
-        dt = m.wave_dt(0.4)
-        res = {}
-        for name, dt_, path in (("fp32_fused", torch.float32, cfdb.FUSED), ("fp64_plain", torch.float64, cfdb.PLAIN))[: 1 if args.no_extras else 2]:
-            q0 = torch.tensor(cfg["q0"], dtype=dt_, device=dev)
-            a, b = torch.empty_like(q0), torch.empty_like(q0)
-            out = {}
-            ms = _timed(lambda: out.__setitem__("f", ctx.wave_run(m, a, b, dt, T, path=path, use_graph=not args.eager)), K, Wm, flush,
-                        prep=lambda: a.copy_(q0), ctx=ctx)
-            res[name] = (n ** 3 * T * K / (ms * 1e-3), ms / K, out["f"].double().cpu().numpy(), LAUNCHES["last"])
-        if args.no_extras:
-            res["fp64_plain"] = res["fp32_fused"]
-        err = l2(res["fp32_fused"][2], res["fp64_plain"][2])
-        cpu = {}
-        if not args.no_extras:
-            from oracle import oracle as O
-            oc = O.Mesh(n, n, n, cfg["dx"], cfg["dx"], cfg["dx"], vertices=V, dtype=np.float32)
-            cpu["cpu_baseline"] = _cpu_baseline(lambda: oc.wave_time(cfg["q0"], dt, 2, faithful=True), n ** 3 * 2,
-                                                f"{n}^3 jittered wave, 2 steps, FP32 operator-by-operator")
-        _line(args, f"wave3d_rusanov_{n}^3_x{T}_steps_jittered_0.2dx", res["fp32_fused"][0], res["fp32_fused"][1],
-              {"mesh": [n] * 3, "jitter": "U(-0.2,0.2) dx, seed 2", "path": "compact area-vector gather"}, 72, n ** 3,
-              T, {"fp64_plain": {"value": res["fp64_plain"][0], "unit": "cell-updates/s"},
-                  "speedup_fused_fp32_vs_plain_fp64": res["fp32_fused"][0] / res["fp64_plain"][0],
-                  "accuracy_vs_fp64": {"l2_rel": err[0], "linf_rel": err[1]}, **cpu},
-              launches=res["fp32_fused"][3], traffic_profile="distorted_sweep_128.txt" if n == 128 else None)
-    elif args.workload == "sod":
-        from oracle import riemann
-        cfg = W.sod_config()
-        nx, ny, nz = cfg["nx"], cfg["ny"], cfg["nz"]
-        m = cfdb.Mesh.structured(ctx, nx, ny, nz, cfg["dx"], cfg["dy"], cfg["dz"])
-        res = {}
-        for name, dt_, dty, path in (("fp32_fused", torch.float32, cfdb.F32, cfdb.FUSED),
-                                     ("fp64_plain", torch.float64, cfdb.F64, cfdb.PLAIN))[: 1 if args.no_extras else 2]:
-            e = cfdb.Euler(ctx, m, dtype=dty, path=path, gamma=cfg["gamma"], cfl=cfg["cfl"], t_end=cfg["t_end"],
-                           max_steps=args.tsteps or 20000)
-            U0 = torch.tensor(cfg["U0"], dtype=dt_, device=dev)
-            a, b = torch.empty_like(U0), torch.empty_like(U0)
-            out = {}
-
-            def solve():
-                e.begin(a)
-                out["r"] = e.run(a, b, 256)
-            ms = _timed(solve, K, Wm, flush, prep=lambda: a.copy_(U0), ctx=ctx)
-            steps, in_b = out["r"]
-            fin = (b if in_b else a).double().cpu().numpy()
-            res[name] = (nx * ny * nz * steps * K / (ms * 1e-3), ms / K, fin, steps, e.totals(), LAUNCHES["last"])
-        if args.no_extras:
-            res["fp64_plain"] = res["fp32_fused"]
-        err = l2(res["fp32_fused"][2], res["fp64_plain"][2])
-        N = nx * ny * nz
-        rho = res["fp32_fused"][2][:N].reshape(nx, ny * nz)[:, 0]
-        xc = (np.arange(nx) + 0.5) * cfg["dx"]
-        ex = riemann.sample(xc, 0.2, 0.5, (1.0, 0.0, 1.0), (0.125, 0.0, 0.1))
-        tot = res["fp32_fused"][4]
-        steps = res["fp32_fused"][3]
-        extra = {"fp64_plain": {"value": res["fp64_plain"][0], "unit": "cell-updates/s", "time_steps": res["fp64_plain"][3]},
-                 "speedup_fused_fp32_vs_plain_fp64": res["fp32_fused"][0] / res["fp64_plain"][0],
-                 "accuracy_vs_fp64": {"l2_rel": err[0], "linf_rel": err[1]},
-                 "fp64_totals_drift": {"mass": float(np.abs(tot[:, 0] - tot[0, 0]).max() / tot[0, 0]),
-                                       "energy": float(np.abs(tot[:, 1] - tot[0, 1]).max() / tot[0, 1])},
-                 "l1_rho_vs_exact_riemann": float(np.mean(np.abs(rho - ex[0])))}
-        if not args.no_extras:
-            # the same scheme beyond L2: 2048x256x256 (2 x 2.7 GB), the first 40 steps
-            mb = cfdb.Mesh.structured(ctx, 2048, 256, 256, 1 / 2048, 0.125 / 256, 0.125 / 256)
-            Nb, Tb = 2048 * 256 * 256, 40
-            eb = cfdb.Euler(ctx, mb, dtype=cfdb.F32, path=cfdb.FUSED, gamma=1.4, cfl=0.4, t_end=0.2, max_steps=Tb)
-            left = (torch.arange(2048, device=dev, dtype=torch.float64) + 0.5) / 2048 < 0.5
-            Ub = torch.zeros(5 * Nb, dtype=torch.float32, device=dev)  # the Sod state of sod_state(), built on the device
-            Ub[:Nb] = torch.where(left, 1.0, 0.125).float().repeat_interleave(256 * 256)
-            Ub[4 * Nb:] = (torch.where(left, 1.0, 0.1) / 0.4).float().repeat_interleave(256 * 256)
-            ab, bb = torch.empty_like(Ub), torch.empty_like(Ub)
-            outb = {}
-
-            def solve_b():
-                eb.begin(ab)
-                outb["r"] = eb.run(ab, bb, 256)
-            msb = _timed(solve_b, 3, 2, flush, prep=lambda: ab.copy_(Ub)) / 3 / Tb
-            peak, _ = measured_peak_hbm()
-            ach = 40 * Nb / (msb * 1e-3) / 1e9
-            extra["roofline_beyond_l2"] = {"mesh": [2048, 256, 256], "time_steps": outb["r"][0], "achieved": ach,
-                                           "peak": peak, "unit": "GB/s", "frac": ach / peak, "ms_per_step": msb,
-                                           "cell_updates_per_s": Nb / (msb * 1e-3)}
-            del eb, mb, Ub, ab, bb
-            from oracle import oracle as O
-            oc = O.Mesh(nx, ny, nz, cfg["dx"], cfg["dy"], cfg["dz"], dtype=np.float32)
-            extra["cpu_baseline"] = _cpu_baseline(
-                lambda: oc.euler_solve(cfg["U0"], cfg["gamma"], cfg["cfl"], cfg["t_end"], max_steps=4, want_totals=False),
-                N * 4, f"{nx}x{ny}x{nz} Sod, first 4 steps, FP32 per-cell Rusanov")
-        _line(args, "sod_512x64x64_rusanov_to_t0.2", res["fp32_fused"][0], res["fp32_fused"][1],
-              {"mesh": [nx, ny, nz], "gamma": 1.4, "cfl": 0.4, "t_end": 0.2, "time_steps": steps}, 40, N, steps,
-              extra, launches=res["fp32_fused"][5], traffic_profile="euler_sweep_sod.txt")
-    elif args.workload == "ensemble":
-        probs = W.ensemble_problems()
-        b = cfdb.Batch(ctx, probs)
-        pool0 = torch.tensor(W.ensemble_initial(probs, b.offsets, b.pool_elems), device=dev)
-        a, c = pool0.clone(), torch.empty_like(pool0)
-        import tempfile
-        b.tune(a, c, os.path.join(tempfile.gettempdir(), "cfdb_ensemble_tune.json"))
-        T = args.tsteps or 300
-        cells = sum(p["n"] ** 3 for p in probs)
-        alg = sum(p["n"] ** 3 * (8 if p["kind"] == 0 else 32) for p in probs)
-        ms = _timed(lambda: b.run(a, c, T, use_graph=not args.eager), K, Wm, flush, prep=lambda: a.copy_(pool0),
-                    ctx=ctx)
-        ens_launches = LAUNCHES["last"]
-        cpu = {}
-        if not args.no_extras:  # every 16th problem, 2 steps each
-            from oracle import oracle as O
-            sub = probs[::16]
-            meshes = [(O.Mesh(p["n"], p["n"], p["n"], 1 / p["n"], 1 / p["n"], 1 / p["n"], dtype=np.float32), p)
-                      for p in sub]
-            init = W.ensemble_initial(probs, b.offsets, b.pool_elems)
-
-            def run_sample():
-                t = 0.0
-                for (om, p), k in zip(meshes, range(0, len(probs), 16)):
-                    off, nn = int(b.offsets[k]), p["n"] ** 3
-                    if p["kind"] == 0:
-                        t += om.heat_time(init[off:off + nn], p["param"], p["dt"], 2, faithful=True)
-                    else:
-                        t += om.wave_time(init[off:off + 4 * nn], p["dt"], 2, cconst=p["param"], faithful=True)
-                return t
-            cpu["cpu_baseline"] = _cpu_baseline(run_sample, 2 * sum(p["n"] ** 3 for p in sub),
-                                                f"{len(sub)} of the {len(probs)} problems, 2 steps each, FP32")
-        _line(args, "ensemble_512_cubes_n16-96_x300_steps", cells * T * K / (ms * 1e-3), ms / K,
-              {"problems": len(probs), "cells": cells, "time_steps_per_bench_step": T,
-               "heat": sum(1 for p in probs if p["kind"] == 0), "wave": sum(1 for p in probs if p["kind"] == 1),
-               "tuned_config": list(b.get_config())}, alg / cells, cells, T,
-              {"launches_per_step": b.launch_count() // T, **cpu}, launches=ens_launches,
-              traffic_profile="ensemble_batch_512.txt")
-    elif args.workload == "adjoint":
-        cfg = W.adjoint_config(n=args.n, steps=args.tsteps or 400)
-        n, T, dt = cfg["n"], cfg["steps"], cfg["dt"]
-        m = cfdb.Mesh.structured(ctx, n, n, n, 1 / n, 1 / n, 1 / n)
-        q0 = torch.tensor(cfg["q0"], dtype=torch.float32, device=dev)
-        c = torch.tensor(cfg["c"], dtype=torch.float32, device=dev)
-        a, bb = q0.clone(), torch.empty_like(q0)
-        fin = ctx.wave_run(m, a, bb, dt, T, c=torch.tensor(cfg["c_true"], dtype=torch.float32, device=dev), speed_mode=1)
-        tgt = fin[: m.n].clone()
-        g_c, g_p = torch.empty(m.n, device=dev), torch.empty(m.n, device=dev)
+    cfg = W.heat_config(steps=tsteps or 200)
+    n, T = cfg["n"], cfg["steps"]
+    m = cfdb.Mesh.structured(ctx, n, n, n, cfg["dx"], cfg["dx"], cfg["dx"])
+    res = {}
+    for name, dt_, path, K, Wm in (("fp32_fused", torch.float32, cfdb.FUSED, S.steps, S.warmup),
+                                   ("fp64_plain", torch.float64, cfdb.PLAIN, S.ref_steps, 1)):
+        T0 = torch.tensor(cfg["T0"], dtype=dt_, device=dev)
+        a, b = torch.empty_like(T0), torch.empty_like(T0)
         out = {}
-        ms_grad = _timed(lambda: out.__setitem__("g", ctx.wave_gradient(m, q0, c, tgt, T, dt, T, g_c, g_p)), K, Wm, flush,
-                         ctx=ctx)
-        grad_launches = LAUNCHES["last"]
-        ms_fwd = _timed(lambda: ctx.wave_run(m, a, bb, dt, T, c=c, speed_mode=1), K, Wm, flush, prep=lambda: a.copy_(q0))
-        J, st = out["g"]
-        if args.no_extras:
-            print(json.dumps({"workload": "adjoint", "gradient_ms": ms_grad / K, "forward_solve_ms": ms_fwd / K}))
-            return
-        d = W.gaussian_random_field(n, corr=0.1, seed=9)
+        ms = _timed(lambda: out.__setitem__("f", ctx.heat_run(m, a, b, cfg["k"], cfg["dt"], T, path=path,
+                                                               use_graph=not S.eager)),
+                    K, Wm, flush, prep=lambda: a.copy_(T0), ctx=ctx)
+        res[name] = (n ** 3 * T * K / (ms * 1e-3), ms / K, out["f"].double().cpu().numpy(), LAUNCHES["last"])
+    err = _rel(res["fp32_fused"][2], res["fp64_plain"][2])
+    extra = {"fp64_plain": {"value": res["fp64_plain"][0], "unit": "cell-updates/s"},
+             "speedup_fused_fp32_vs_plain_fp64": res["fp32_fused"][0] / res["fp64_plain"][0],
+             "accuracy_vs_fp64": {"l2_rel": err[0], "linf_rel": err[1], "bar_l2": 1e-5},
+             "path": "cluster-resident (one launch per solve)" if res["fp32_fused"][3] == S.steps else "per-step sweep"}
+    if S.extras:
+        # the same step beyond L2: 512^3 (2 x 537 MB), 50 steps, per-step TMA sweep
+        nb, Tb = 512, 50
+        mb = cfdb.Mesh.structured(ctx, nb, nb, nb, 1 / nb, 1 / nb, 1 / nb)
+        Tl = torch.rand(nb ** 3, dtype=torch.float32, device=dev)
+        al, bl = Tl.clone(), torch.empty_like(Tl)
+        dtb = 0.1 * (1 / nb) ** 2 / cfg["k"]
+        msb = _timed(lambda: ctx.heat_run(mb, al, bl, cfg["k"], dtb, Tb, path=cfdb.FUSED, use_graph=True), 3, 2,
+                     flush, prep=lambda: al.copy_(Tl)) / 3 / Tb
+        peak, _ = measured_peak_hbm()
+        ach = 8 * nb ** 3 / (msb * 1e-3) / 1e9
+        extra["roofline_beyond_l2"] = {"mesh": [nb] * 3, "time_steps": Tb, "achieved": ach, "peak": peak,
+                                       "unit": "GB/s", "frac": ach / peak, "ms_per_step": msb,
+                                       "cell_updates_per_s": nb ** 3 / (msb * 1e-3)}
+        del mb, Tl, al, bl
+        from oracle import oracle as O
+        oc = O.Mesh(n, n, n, cfg["dx"], cfg["dx"], cfg["dx"], dtype=np.float32)
+        extra.update(_cpu_pair(lambda: oc.heat_time(cfg["T0"], cfg["k"], cfg["dt"], 10, faithful=True),
+                               n ** 3 * 10, f"{n}^3 heat, 10 steps, FP32 operator-by-operator"))
+    m.close()
+    return _line(S, f"heat3d_{n}^3_x{T}_steps", res["fp32_fused"][0], res["fp32_fused"][1],
+                 {"mesh": [n] * 3, "k": cfg["k"], "dt": cfg["dt"], "time_steps_per_bench_step": T}, 8, n ** 3, T,
+                 extra, launches=res["fp32_fused"][3])
+
+
+def bench_wave_distorted(ctx, cfdb, dev, flush, S, n=128, tsteps=None):
+    import numpy as np
+    import torch
+
+    from cfdarcov2_b200 import workloads as W
+    cfg = W.wave_config(n=n, steps=tsteps or 500)
+    n, T = cfg["n"], cfg["steps"]
+    V = W.jittered_vertices(n, seed=2)
+    m = cfdb.Mesh.from_vertices(ctx, n, n, n, cfg["dx"], cfg["dx"], cfg["dx"], V)
+    dt = m.wave_dt(0.4)
+    res = {}
+    for name, dt_, path, K, Wm in (("fp32_fused", torch.float32, cfdb.FUSED, S.steps, S.warmup),
+                                   ("fp64_plain", torch.float64, cfdb.PLAIN, S.ref_steps, 1)):
+        q0 = torch.tensor(cfg["q0"], dtype=dt_, device=dev)
+        a, b = torch.empty_like(q0), torch.empty_like(q0)
+        out = {}
+        ms = _timed(lambda: out.__setitem__("f", ctx.wave_run(m, a, b, dt, T, path=path, use_graph=not S.eager)),
+                    K, Wm, flush, prep=lambda: a.copy_(q0), ctx=ctx)
+        res[name] = (n ** 3 * T * K / (ms * 1e-3), ms / K, out["f"].double().cpu().numpy(), LAUNCHES["last"])
+    err = _rel(res["fp32_fused"][2], res["fp64_plain"][2])
+    extra = {"fp64_plain": {"value": res["fp64_plain"][0], "unit": "cell-updates/s"},
+             "speedup_fused_fp32_vs_plain_fp64": res["fp32_fused"][0] / res["fp64_plain"][0],
+             "accuracy_vs_fp64": {"l2_rel": err[0], "linf_rel": err[1], "bar_l2": 1e-5}}
+    if S.extras:
+        from oracle import oracle as O
+        oc = O.Mesh(n, n, n, cfg["dx"], cfg["dx"], cfg["dx"], vertices=V, dtype=np.float32)
+        extra.update(_cpu_pair(lambda: oc.wave_time(cfg["q0"], dt, 2, faithful=True), n ** 3 * 2,
+                               f"{n}^3 jittered wave, 2 steps, FP32 operator-by-operator"))
+    m.close()
+    return _line(S, f"wave3d_rusanov_{n}^3_x{T}_steps_jittered_0.2dx", res["fp32_fused"][0], res["fp32_fused"][1],
+                 {"mesh": [n] * 3, "jitter": "U(-0.2,0.2) dx, seed 2", "path": "compact area-vector gather"}, 72,
+                 n ** 3, T, extra, launches=res["fp32_fused"][3],
+                 traffic_profile="distorted_sweep_128.txt" if n == 128 else None)
+
+
+def bench_sod(ctx, cfdb, dev, flush, S, max_steps=None):
+    import numpy as np
+    import torch
+
+    from cfdarcov2_b200 import workloads as W
+    from oracle import riemann
+    cfg = W.sod_config()
+    nx, ny, nz = cfg["nx"], cfg["ny"], cfg["nz"]
+    m = cfdb.Mesh.structured(ctx, nx, ny, nz, cfg["dx"], cfg["dy"], cfg["dz"])
+    res = {}
+    for name, dt_, dty, path, K, Wm in (("fp32_fused", torch.float32, cfdb.F32, cfdb.FUSED, S.steps, S.warmup),
+                                        ("fp64_plain", torch.float64, cfdb.F64, cfdb.PLAIN, S.ref_steps, 1)):
+        e = cfdb.Euler(ctx, m, dtype=dty, path=path, gamma=cfg["gamma"], cfl=cfg["cfl"], t_end=cfg["t_end"],
+                       max_steps=max_steps or 20000)
+        U0 = torch.tensor(cfg["U0"], dtype=dt_, device=dev)
+        a, b = torch.empty_like(U0), torch.empty_like(U0)
+        out = {}
+
+        def solve():
+            e.begin(a)
+            out["r"] = e.run(a, b, 256)
+        ms = _timed(solve, K, Wm, flush, prep=lambda: a.copy_(U0), ctx=ctx)
+        steps, in_b = out["r"]
+        fin = (b if in_b else a).double().cpu().numpy()
+        res[name] = (nx * ny * nz * steps * K / (ms * 1e-3), ms / K, fin, steps, e.totals(), LAUNCHES["last"])
+        e.close()
+    err = _rel(res["fp32_fused"][2], res["fp64_plain"][2])
+    N = nx * ny * nz
+    rho = res["fp32_fused"][2][:N].reshape(nx, ny * nz)[:, 0]
+    xc = (np.arange(nx) + 0.5) * cfg["dx"]
+    ex = riemann.sample(xc, 0.2, 0.5, (1.0, 0.0, 1.0), (0.125, 0.0, 0.1))
+    steps = res["fp32_fused"][3]
+
+    def drift(tot):
+        return {"mass": float(np.abs(tot[:, 0] - tot[0, 0]).max() / tot[0, 0]),
+                "energy": float(np.abs(tot[:, 1] - tot[0, 1]).max() / tot[0, 1])}
+    extra = {"fp64_plain": {"value": res["fp64_plain"][0], "unit": "cell-updates/s", "time_steps": res["fp64_plain"][3]},
+             "speedup_fused_fp32_vs_plain_fp64": res["fp32_fused"][0] / res["fp64_plain"][0],
+             "accuracy_vs_fp64": {"l2_rel": err[0], "linf_rel": err[1], "bar_l2": 1e-5},
+             "fp64_totals_drift": drift(res["fp32_fused"][4]),
+             "fp64_totals_drift_fp64_plain": drift(res["fp64_plain"][4]),
+             "l1_rho_vs_exact_riemann": float(np.mean(np.abs(rho - ex[0])))}
+    if S.extras:
+        # the same scheme beyond L2: 2048x256x256 (2 x 2.7 GB), the first 40 steps
+        mb = cfdb.Mesh.structured(ctx, 2048, 256, 256, 1 / 2048, 0.125 / 256, 0.125 / 256)
+        Nb, Tb = 2048 * 256 * 256, 40
+        eb = cfdb.Euler(ctx, mb, dtype=cfdb.F32, path=cfdb.FUSED, gamma=1.4, cfl=0.4, t_end=0.2, max_steps=Tb)
+        left = (torch.arange(2048, device=dev, dtype=torch.float64) + 0.5) / 2048 < 0.5
+        Ub = torch.zeros(5 * Nb, dtype=torch.float32, device=dev)  # the Sod state of sod_state(), built on the device
+        Ub[:Nb] = torch.where(left, 1.0, 0.125).float().repeat_interleave(256 * 256)
+        Ub[4 * Nb:] = (torch.where(left, 1.0, 0.1) / 0.4).float().repeat_interleave(256 * 256)
+        ab, bb = torch.empty_like(Ub), torch.empty_like(Ub)
+        outb = {}
+
+        def solve_b():
+            eb.begin(ab)
+            outb["r"] = eb.run(ab, bb, 256)
+        msb = _timed(solve_b, 3, 2, flush, prep=lambda: ab.copy_(Ub)) / 3 / Tb
+        peak, _ = measured_peak_hbm()
+        ach = 40 * Nb / (msb * 1e-3) / 1e9
+        extra["roofline_beyond_l2"] = {"mesh": [2048, 256, 256], "time_steps": outb["r"][0], "achieved": ach,
+                                       "peak": peak, "unit": "GB/s", "frac": ach / peak, "ms_per_step": msb,
+                                       "cell_updates_per_s": Nb / (msb * 1e-3)}
+        eb.close()
+        mb.close()
+        del Ub, ab, bb
+        from oracle import oracle as O
+        oc = O.Mesh(nx, ny, nz, cfg["dx"], cfg["dy"], cfg["dz"], dtype=np.float32)
+        extra.update(_cpu_pair(
+            lambda: oc.euler_solve(cfg["U0"], cfg["gamma"], cfg["cfl"], cfg["t_end"], max_steps=4, want_totals=False),
+            N * 4, f"{nx}x{ny}x{nz} Sod, first 4 steps, FP32 per-cell Rusanov"))
+    m.close()
+    return _line(S, "sod_512x64x64_rusanov_to_t0.2", res["fp32_fused"][0], res["fp32_fused"][1],
+                 {"mesh": [nx, ny, nz], "gamma": 1.4, "cfl": 0.4, "t_end": 0.2, "time_steps": steps}, 40, N, steps,
+                 extra, launches=res["fp32_fused"][5], traffic_profile="euler_sweep_sod.txt")
+
+
+def bench_ensemble(ctx, cfdb, dev, flush, S, tsteps=None):
+    import tempfile
+
+    import numpy as np
+    import torch
+
+    from cfdarcov2_b200 import workloads as W
+    probs = W.ensemble_problems()
+    b = cfdb.Batch(ctx, probs)
+    init = W.ensemble_initial(probs, b.offsets, b.pool_elems)
+    pool0 = torch.tensor(init, device=dev)
+    a, c = pool0.clone(), torch.empty_like(pool0)
+    b.tune(a, c, os.path.join(tempfile.gettempdir(), "cfdb_ensemble_tune.json"))
+    T = tsteps or 300
+    cells = sum(p["n"] ** 3 for p in probs)
+    alg = sum(p["n"] ** 3 * (8 if p["kind"] == 0 else 32) for p in probs)
+    ms = _timed(lambda: b.run(a, c, T, use_graph=not S.eager), S.steps, S.warmup, flush, prep=lambda: a.copy_(pool0),
+                ctx=ctx)
+    ens_launches = LAUNCHES["last"]
+    # accuracy: every problem against the FP64 plain path on its own mesh
+    a.copy_(pool0)
+    got = b.run(a, c, T, use_graph=True).cpu().numpy()
+    worst, over = 0.0, 0
+    for p, off in zip(probs, b.offsets):
+        n = p["n"]
+        k = n ** 3 if p["kind"] == 0 else 4 * n ** 3
+        m = cfdb.Mesh.structured(ctx, n, n, n, 1 / n, 1 / n, 1 / n)
+        x = torch.tensor(init[off: off + k], dtype=torch.float64, device=dev)
+        if p["kind"] == 0:
+            ref = ctx.heat_run(m, x, torch.empty_like(x), p["param"], p["dt"], T, path=cfdb.PLAIN, use_graph=False)
+        else:
+            ref = ctx.wave_run(m, x, torch.empty_like(x), p["dt"], T, c_const=p["param"], path=cfdb.PLAIN,
+                               use_graph=False)
+        e = _rel(got[off: off + k], ref.cpu().numpy())[0]
+        worst = max(worst, e)
+        over += e > 1e-5
+        m.close()
+    extra = {"launches_per_step": b.launch_count() // T,
+             "accuracy_vs_fp64": {"worst_problem_l2_rel": worst, "problems_over_bar": int(over), "bar_l2": 1e-5,
+                                  "reference": "FP64 plain path, each problem on its own mesh"}}
+    if S.extras:  # every 16th problem, 2 steps each
+        from oracle import oracle as O
+        sub = probs[::16]
+        meshes = [(O.Mesh(p["n"], p["n"], p["n"], 1 / p["n"], 1 / p["n"], 1 / p["n"], dtype=np.float32), p)
+                  for p in sub]
+
+        def run_sample():
+            t = 0.0
+            for (om, p), k in zip(meshes, range(0, len(probs), 16)):
+                off, nn = int(b.offsets[k]), p["n"] ** 3
+                if p["kind"] == 0:
+                    t += om.heat_time(init[off:off + nn], p["param"], p["dt"], 2, faithful=True)
+                else:
+                    t += om.wave_time(init[off:off + 4 * nn], p["dt"], 2, cconst=p["param"], faithful=True)
+            return t
+        extra.update(_cpu_pair(run_sample, 2 * sum(p["n"] ** 3 for p in sub),
+                               f"{len(sub)} of the {len(probs)} problems, 2 steps each, FP32"))
+    line = _line(S, "ensemble_512_cubes_n16-96_x300_steps", cells * T * S.steps / (ms * 1e-3), ms / S.steps,
+                 {"problems": len(probs), "cells": cells, "time_steps_per_bench_step": T,
+                  "heat": sum(1 for p in probs if p["kind"] == 0), "wave": sum(1 for p in probs if p["kind"] == 1),
+                  "tuned_config": list(b.get_config())}, alg / cells, cells, T, extra, launches=ens_launches,
+                 traffic_profile="ensemble_batch_512.txt")
+    b.close()
+    return line
+
+
+def bench_adjoint(ctx, cfdb, dev, flush, S, n=128, tsteps=None):
+    import numpy as np
+    import torch
+
+    from cfdarcov2_b200 import workloads as W
+    cfg = W.adjoint_config(n=n, steps=tsteps or 400)
+    n, T, dt = cfg["n"], cfg["steps"], cfg["dt"]
+    m = cfdb.Mesh.structured(ctx, n, n, n, 1 / n, 1 / n, 1 / n)
+    q0 = torch.tensor(cfg["q0"], dtype=torch.float32, device=dev)
+    c = torch.tensor(cfg["c"], dtype=torch.float32, device=dev)
+    a, bb = q0.clone(), torch.empty_like(q0)
+    fin = ctx.wave_run(m, a, bb, dt, T, c=torch.tensor(cfg["c_true"], dtype=torch.float32, device=dev), speed_mode=1)
+    tgt = fin[: m.n].clone()
+    g_c, g_p = torch.empty(m.n, device=dev), torch.empty(m.n, device=dev)
+    out = {}
+    ms_grad = _timed(lambda: out.__setitem__("g", ctx.wave_gradient(m, q0, c, tgt, T, dt, T, g_c, g_p)), S.steps,
+                     S.warmup, flush, ctx=ctx)
+    grad_launches = LAUNCHES["last"]
+    ms_fwd = _timed(lambda: ctx.wave_run(m, a, bb, dt, T, c=c, speed_mode=1), S.steps, S.warmup, flush,
+                    prep=lambda: a.copy_(q0))
+    J, st = out["g"]
+    # FP64 central differences (eps = 1e-3) along seeded smooth directions, for c and for p0
+    q64, c64, t64 = q0.double(), c.double(), tgt.double()
+    eps = 1e-3
+    fd_err = {}
+    for which, seed, grad in (("c", 9, g_c), ("p0", 10, g_p)):
+        d = W.gaussian_random_field(n, corr=0.1, seed=seed)
         d = torch.tensor(d / np.abs(d).max(), dtype=torch.float64, device=dev)
-        q64, c64, t64 = q0.double(), c.double(), tgt.double()
-        eps = 1e-3
-        fd = (ctx.wave_objective(m, q64, c64 + eps * d, t64, T, dt, path=cfdb.PLAIN)
-              - ctx.wave_objective(m, q64, c64 - eps * d, t64, T, dt, path=cfdb.PLAIN)) / (2 * eps)
-        adj = float(torch.dot(g_c.double(), d))
+        if which == "c":
+            Jp = ctx.wave_objective(m, q64, c64 + eps * d, t64, T, dt, path=cfdb.PLAIN)
+            Jm = ctx.wave_objective(m, q64, c64 - eps * d, t64, T, dt, path=cfdb.PLAIN)
+        else:
+            dq = torch.zeros_like(q64)
+            dq[: m.n] = d
+            Jp = ctx.wave_objective(m, q64 + eps * dq, c64, t64, T, dt, path=cfdb.PLAIN)
+            Jm = ctx.wave_objective(m, q64 - eps * dq, c64, t64, T, dt, path=cfdb.PLAIN)
+        fd = (Jp - Jm) / (2 * eps)
+        fd_err[which] = abs(float(torch.dot(grad.double(), d)) - fd) / abs(fd)
+    extra = {"adjoint_over_forward_time": (ms_grad / S.steps) / (ms_fwd / S.steps),
+             "reverse_over_forward_sweep": st.reverse_ms / st.forward_ms,
+             "forward_solve_ms": ms_fwd / S.steps, "gradient_ms": ms_grad / S.steps,
+             "grad_rel_err_vs_fd": fd_err["c"], "grad_p0_rel_err_vs_fd": fd_err["p0"], "fd_eps": eps, "J": J,
+             "bar": {"adjoint_over_forward_time": 3.0, "grad_rel_err_vs_fd": 1e-4},
+             "note": "value counts forward + adjoint cell-updates; roofline uses the adjoint sweep's 60 B/cell"}
+    if S.extras:
         from oracle import oracle as O
         oc = O.Mesh(n, n, n, 1 / n, 1 / n, 1 / n, dtype=np.float32)
         tgt_h = tgt.cpu().numpy()
-        cpu = _cpu_baseline(lambda: oc.wave_gradient(cfg["q0"], cfg["c"], tgt_h, dt, 4), 2 * n ** 3 * 4,
-                            f"{n}^3 wave gradient over 4 steps (forward + adjoint), FP32", max_calls=20)
-        _line(args, f"wave_adjoint_{n}^3_x{T}_steps", 2 * n ** 3 * T * K / (ms_grad * 1e-3), ms_grad / K,
-              {"mesh": [n] * 3, "time_steps": T, "snapshots": T, "c": "exp(0.2 g), g Gaussian random field, seed 5"},
-              60, n ** 3, T,
-              {"adjoint_over_forward_time": (ms_grad / K) / (ms_fwd / K),
-               "reverse_over_forward_sweep": st.reverse_ms / st.forward_ms,
-               "forward_solve_ms": ms_fwd / K, "gradient_ms": ms_grad / K,
-               "grad_rel_err_vs_fd": abs(adj - fd) / abs(fd), "fd_eps": eps, "J": J,
-               "note": "value counts forward + adjoint cell-updates; roofline uses the adjoint sweep's 60 B/cell",
-               "cpu_baseline": cpu},
-              launches=grad_launches, traffic_profile="adjoint_sweep_128.txt" if n == 128 else None)
+        extra.update(_cpu_pair(lambda: oc.wave_gradient(cfg["q0"], cfg["c"], tgt_h, dt, 4), 2 * n ** 3 * 4,
+                               f"{n}^3 wave gradient over 4 steps (forward + adjoint), FP32", max_calls=20))
+    m.close()
+    return _line(S, f"wave_adjoint_{n}^3_x{T}_steps", 2 * n ** 3 * T * S.steps / (ms_grad * 1e-3),
+                 ms_grad / S.steps,
+                 {"mesh": [n] * 3, "time_steps": T, "snapshots": T, "c": "exp(0.2 g), g Gaussian random field, seed 5"},
+                 60, n ** 3, T, extra, launches=grad_launches,
+                 traffic_profile="adjoint_sweep_128.txt" if n == 128 else None)
+
+
+SECONDARY = {"heat": bench_heat, "wave_distorted": bench_wave_distorted, "sod": bench_sod,
+             "ensemble": bench_ensemble, "adjoint": bench_adjoint}
+
+
+def run_configs(ctx, cfdb, dev, flush):
+    """The other benchmark workloads at their configured sizes, measured
+    after the headline in the same run (fewer repetitions): one sub-object
+    each, or the error that stopped it."""
+    S = Settings(steps=5, warmup=2, ref_steps=1)
+    out = {}
+    for name, fn in SECONDARY.items():
+        t0 = time.perf_counter()
+        try:
+            line = fn(ctx, cfdb, dev, flush, S)
+            for k in ("metric", "n_gpus", "higher_is_better", "scaling", "vs_baseline", "data"):
+                line.pop(k, None)
+        except Exception as exc:  # record and go on: the headline line must still print
+            line = {"error": f"{type(exc).__name__}: {exc}"}
+        line["wall_s"] = time.perf_counter() - t0
+        out[name] = line
+    return out
+
+
+def run_secondary(args):
+    import torch
+
+    import cfdarcov2_b200 as cfdb
+    dev = torch.device("cuda", 0)
+    ctx = cfdb.Context(0)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    S = Settings(args.steps, args.warmup, ref_steps=max(1, min(args.steps, 3)), extras=not args.no_extras,
+                 eager=args.eager)
+    kw = {}
+    if args.workload in ("wave_distorted", "adjoint"):
+        kw["n"] = args.n
+    if args.workload == "sod":
+        kw["max_steps"] = args.tsteps
+    elif args.tsteps:
+        kw["tsteps"] = args.tsteps
+    print(json.dumps(SECONDARY[args.workload](ctx, cfdb, dev, flush, S, **kw)), flush=True)
 
 
 # the reference's own benchmark rows (scripts/benchmark_cfdarchov2.py: 200

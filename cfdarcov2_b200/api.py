@@ -66,6 +66,22 @@ class Context:
         call("cfdb_ctx_launch_count", self.h, C.byref(v), ctx=self.h)
         return v.value
 
+    # -- host <-> device copies through the C ABI (cfdb_upload / cfdb_download) --
+    def upload(self, dst, src_host: np.ndarray | None = None, *, src_ptr=None, nbytes=None, wait=True):
+        """Copies host memory into the device tensor dst; wait=False queues it
+        on the context's stream (cfdb_upload_async)."""
+        ptr = src_ptr if src_ptr is not None else src_host.ctypes.data
+        n = nbytes if nbytes is not None else dst.numel() * dst.element_size()
+        call("cfdb_upload" if wait else "cfdb_upload_async", self.h, _ptr(dst), C.c_void_p(ptr), int(n), ctx=self.h)
+
+    def download(self, src, dst_host: np.ndarray | None = None, *, dst_ptr=None, nbytes=None, wait=True):
+        """Copies the device tensor src into host memory; wait=False queues it
+        on the context's stream (cfdb_download_async)."""
+        ptr = dst_ptr if dst_ptr is not None else dst_host.ctypes.data
+        n = nbytes if nbytes is not None else src.numel() * src.element_size()
+        call("cfdb_download" if wait else "cfdb_download_async", self.h, C.c_void_p(ptr), _ptr(src), int(n),
+             ctx=self.h)
+
     def set_wait_limit(self, cycles: int = 4000000000, missing_plane: int = -1) -> None:
         """Bound of the sweep kernels' device waits; missing_plane >= 0 is the timeout test hook."""
         call("cfdb_ctx_set_wait_limit", self.h, int(cycles), int(missing_plane), ctx=self.h)
@@ -380,6 +396,10 @@ class Batch:
     def set_config(self, cells_per_item, threads, ctas_per_sm):
         call("cfdb_batch_set_config", self.h, int(cells_per_item), int(threads), int(ctas_per_sm), ctx=self.ctx.h)
 
+    def set_staged(self, staged: bool) -> None:
+        """Kernel form: the staged row ring (default) or the column march."""
+        call("cfdb_batch_set_staged", self.h, int(bool(staged)), ctx=self.ctx.h)
+
     def get_config(self):
         a, b, c = C.c_int32(), C.c_int32(), C.c_int32()
         call("cfdb_batch_get_config", self.h, C.byref(a), C.byref(b), C.byref(c), ctx=self.ctx.h)
@@ -393,7 +413,9 @@ class Batch:
         call("cfdb_batch_step", self.h, _ptr(a), _ptr(b), ctx=self.ctx.h)
 
     def run(self, a, b, steps, use_graph=True):
+        """Advances `steps` steps a -> b -> a ...; returns the pool that holds the final state."""
         call("cfdb_batch_run", self.h, _ptr(a), _ptr(b), int(steps), int(bool(use_graph)), ctx=self.ctx.h)
+        return a if steps % 2 == 0 else b
 
     def launch_count(self) -> int:
         v = C.c_int64()

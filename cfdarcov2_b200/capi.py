@@ -88,6 +88,8 @@ PROTOTYPES = {
     "cfdb_free": (_I, [_P, _P]),
     "cfdb_upload": (_I, [_P, _P, _P, _I64]),
     "cfdb_download": (_I, [_P, _P, _P, _I64]),
+    "cfdb_upload_async": (_I, [_P, _P, _P, _I64]),
+    "cfdb_download_async": (_I, [_P, _P, _P, _I64]),
     "cfdb_mesh_create_structured": (_I, [_P, _I64, _I64, _I64, _D, _D, _D, _PP]),
     "cfdb_mesh_create_from_vertices": (_I, [_P, _I64, _I64, _I64, _D, _D, _D, _P, _I, _PP]),
     "cfdb_mesh_destroy": (_I, [_P]),
@@ -127,6 +129,7 @@ PROTOTYPES = {
     "cfdb_batch_destroy": (_I, [_P]),
     "cfdb_batch_set_config": (_I, [_P, _I32, _I32, _I32]),
     "cfdb_batch_get_config": (_I, [_P, _PI32, _PI32, _PI32]),
+    "cfdb_batch_set_staged": (_I, [_P, _I]),
     "cfdb_batch_tune": (_I, [_P, _P, _P, C.c_char_p]),
     "cfdb_batch_step": (_I, [_P, _P, _P]),
     "cfdb_batch_run": (_I, [_P, _P, _P, _I32, _I]),

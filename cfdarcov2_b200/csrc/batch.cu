@@ -22,6 +22,7 @@
 #include <unistd.h>
 
 #include "cfdb_internal.hpp"
+#include "tma_stencil.cuh"
 
 CFDB_MODULE_ANCHOR
 
@@ -150,10 +151,237 @@ __global__ void batch_step_k(const ProbDev* __restrict__ probs, const ItemDev* _
   }
 }
 
+// ---- staged form: a producer warp streams plane rows into a shared ring -----
+//
+// The same work items and arithmetic as column_step, with the planes staged
+// in shared memory.  Warp 0 is the producer: its lane 0 walks the CTA's
+// items and, for every plane an item needs (x0 - 1 .. x1), issues one 1-D
+// bulk copy (cp.async.bulk, no multicast) per field of the contiguous rows
+// [yz0 - n, yz0 + C + n) of that plane -- the item's C columns and their y
+// neighbours -- into ring slot k % S, completing on the slot's `full`
+// mbarrier.  The remaining warps are consumers: each thread owns one column
+// of the item, takes its own cell and its y/z neighbours from the slot, keeps
+// the x neighbours in registers, and its warp arrives on the slot's `empty`
+// mbarrier when done with the plane; the producer refills a slot once every
+// consumer warp has released it.  No CTA-wide barrier per plane, and the
+// ring runs on across item boundaries, so up to S planes stay in flight per
+// CTA.  Copies start on a 16-byte boundary (rounded down; the consumer skips
+// the 0-3 leading floats) and end on one (rounded up: the pool holds 4 spare
+// floats at its end).  Every wait is bounded; a wait that gives up records
+// the timeout in the error word, skips the remaining waits, and the producer
+// lets its copies land before the CTA exits.
+// Ring depth S (slots): 8 where the shared memory of the configured CTAs
+// holds it, else 4 (ring_slots()).
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   stencil::smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(stencil::smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(stencil::smem_u32(bar)) : "memory");
+}
+
+struct RingArgs {
+  int C;                  // consumer threads = columns per item
+  int cap;                // floats per field tile of a slot (multiple of 4)
+  long long wait_cycles;  // bound of every mbarrier wait
+};
+
+template <int NF, uint32_t S>
+__device__ __forceinline__ void ring_consume(const ProbDev& P, const ItemDev& I, const float* __restrict__ ring,
+                                             uint64_t* full, uint64_t* empty, const RingArgs& A,
+                                             float* __restrict__ b, uint32_t& k, bool& bad) {
+  static_assert((S & (S - 1)) == 0, "ring slots: a power of two");
+  const int n = P.n, n2 = n * n;
+  const int n3 = n2 * n;  // n <= 1024
+  const int t = int(threadIdx.x) - 32;
+  const int col = I.yz0 + t;
+  const bool act = col < n2;
+  const int lo = max(I.yz0 - n, 0);
+  const int y = act ? col / n : 0;
+  const int z = act ? col - y * n : 0;
+  const int j = col - lo;  // the thread's cell in a slot's row block, before the alignment shift
+  const int dym = y > 0 ? -n : 0, dyp = y < n - 1 ? n : 0, dzm = z > 0 ? -1 : 0, dzp = z < n - 1 ? 1 : 0;
+  const float sym = y > 0 ? 1.f : -1.f, syp = y < n - 1 ? 1.f : -1.f;
+  const float szm = z > 0 ? 1.f : -1.f, szp = z < n - 1 ? 1.f : -1.f;
+  const unsigned lane = threadIdx.x & 31u;
+  // Field f of plane x starts its copy at the 16-byte boundary below
+  // element P.offset + f n3 + x n2 + lo, so the thread's cell sits at
+  // j + ((P.offset + f n3 + x n2 + lo) & 3): the shift is tracked mod 4.
+  const int s0 = int((P.offset + lo) & 3), fs = n3 & 3, xs = n2 & 3;
+  auto off = [&](uint32_t kk, int f, int x) {
+    return int(kk & (S - 1)) * (4 * A.cap) + f * A.cap + ((s0 + f * fs + x * xs) & 3) + j;
+  };
+  auto wait_full = [&](uint32_t kk) {
+    if (!bad && !stencil::mbar_wait_bounded(&full[kk & (S - 1)], (kk / S) & 1u, A.wait_cycles)) bad = true;
+  };
+  auto release = [&](uint32_t kk) {
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[kk & (S - 1)]);
+  };
+  auto ghost = [&](float g[NF], const float c[NF]) {
+#pragma unroll
+    for (int f = 0; f < NF; ++f) g[f] = c[f];
+    if constexpr (NF == 4) g[1] = -c[1];
+  };
+  float prv[NF], cur[NF], nxt[NF];
+  if (I.x0 > 0) {
+    wait_full(k);
+    if (act) {
+#pragma unroll
+      for (int f = 0; f < NF; ++f) prv[f] = ring[off(k, f, I.x0 - 1)];
+    }
+    release(k);
+    ++k;
+  }
+  wait_full(k);
+  if (act) {
+#pragma unroll
+    for (int f = 0; f < NF; ++f) cur[f] = ring[off(k, f, I.x0)];
+  }
+  uint32_t kc = k++;
+  if (I.x0 == 0) ghost(prv, cur);
+  float* const o = b + P.offset + col;  // field f of plane x: o[f n3 + x n2]
+  for (int x = I.x0; x < I.x1; ++x) {
+    uint32_t kn = kc;
+    if (x + 1 < n) {
+      wait_full(k);
+      if (act) {
+#pragma unroll
+        for (int f = 0; f < NF; ++f) nxt[f] = ring[off(k, f, x + 1)];
+      }
+      kn = k++;
+    } else {
+      ghost(nxt, cur);
+    }
+    if (act) {
+      float ym[NF], yp[NF], zm[NF], zp[NF];
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        const float* q = ring + off(kc, f, x);
+        ym[f] = q[dym];
+        yp[f] = q[dyp];
+        zm[f] = q[dzm];
+        zp[f] = q[dzp];
+      }
+      const int c = x * n2;
+      if constexpr (NF == 1) {
+        const float tt = cur[0];
+        const float sum = ((prv[0] - tt) + (nxt[0] - tt)) + ((ym[0] - tt) + (yp[0] - tt)) + ((zm[0] - tt) + (zp[0] - tt));
+        o[c] = tt + P.c0 * sum;
+      } else {
+        ym[2] *= sym;
+        yp[2] *= syp;
+        zm[3] *= szm;
+        zp[3] *= szp;
+        float sm[NF];
+#pragma unroll
+        for (int f = 0; f < NF; ++f) sm[f] = ((prv[f] + nxt[f]) + (ym[f] + yp[f])) + (zm[f] + zp[f]);
+        const float div = ((nxt[1] - prv[1]) + (yp[2] - ym[2])) + (zp[3] - zm[3]);
+        o[c] = cur[0] - P.c0 * div + P.c1 * (sm[0] - 6.0f * cur[0]);
+        o[n3 + c] = cur[1] - P.c2 * (nxt[0] - prv[0]) + P.c1 * (sm[1] - 6.0f * cur[1]);
+        o[2 * n3 + c] = cur[2] - P.c2 * (yp[0] - ym[0]) + P.c1 * (sm[2] - 6.0f * cur[2]);
+        o[3 * n3 + c] = cur[3] - P.c2 * (zp[0] - zm[0]) + P.c1 * (sm[3] - 6.0f * cur[3]);
+      }
+    }
+    release(kc);
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+      prv[f] = cur[f];
+      cur[f] = nxt[f];
+    }
+    kc = kn;
+  }
+  if (I.x1 < n) release(kc);  // plane x1, loaded as the last plane's x+1 neighbour
+}
+
+template <int S>
+__global__ void batch_ring_k(const ProbDev* __restrict__ probs, const ItemDev* __restrict__ items, int n_items,
+                             const float* __restrict__ a, float* __restrict__ b, RingArgs A, int* __restrict__ err) {
+  extern __shared__ __align__(128) float ring[];
+  __shared__ __align__(8) uint64_t full[S], empty[S];
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      stencil::mbar_init(&full[s], 1);
+      stencil::mbar_init(&empty[s], blockDim.x / 32 - 1);
+    }
+    stencil::fence_mbar_init();
+  }
+  __syncthreads();
+  bool bad = false;
+  if (threadIdx.x < 32) {
+    // Producer warp: lane s < S owns ring slot s and issues every plane
+    // that lands there (global plane index k with k % S == s), so the lanes
+    // prepare up to S planes per warp instruction and wait on their own
+    // slots independently.
+    const uint32_t lane = threadIdx.x;
+    uint32_t k = 0;        // planes of the CTA's earlier items
+    int64_t last = -1;     // the last plane this lane issued
+    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+      const ItemDev I = items[it];
+      const ProbDev P = probs[I.prob];
+      const int n = P.n, n2 = n * n;
+      const int64_t n3 = int64_t(n2) * n;
+      const int nf = P.kind == 0 ? 1 : 4;
+      const int lo = max(I.yz0 - n, 0), hi = min(I.yz0 + A.C + n, n2);
+      const int xb = max(I.x0 - 1, 0), xe = min(I.x1, n - 1);
+      const int np = xe - xb + 1;
+      if (lane < uint32_t(S) && !bad) {
+        const int64_t base = P.offset + lo;
+        for (int q = int((lane - k) & uint32_t(S - 1)); q < np; q += S) {
+          const uint32_t kk = k + uint32_t(q);  // kk % S == lane
+          // refill the slot only when every consumer warp has released its
+          // previous plane and that plane's copies have landed (the latter
+          // holds whenever the consumers waited for them; checking it keeps
+          // the slot's barrier from being armed over an unfinished phase)
+          if (kk >= uint32_t(S) &&
+              (!stencil::mbar_wait_bounded(&empty[lane], ((kk / S) - 1) & 1u, A.wait_cycles) ||
+               !stencil::mbar_wait_bounded(&full[lane], ((kk / S) - 1) & 1u, A.wait_cycles))) {
+            bad = true;
+            break;
+          }
+          const int64_t plane = base + int64_t(xb + q) * n2;
+          int64_t g0[4];
+          uint32_t bytes[4], total = 0;
+          for (int f = 0; f < nf; ++f) {
+            const int64_t start = plane + f * n3;
+            g0[f] = start & ~int64_t(3);
+            const int64_t end = (start + (hi - lo) + 3) & ~int64_t(3);
+            bytes[f] = uint32_t(4 * (end - g0[f]));
+            total += bytes[f];
+          }
+          float* dst = ring + lane * (4 * A.cap);
+          stencil::mbar_expect_tx(&full[lane], total);
+          for (int f = 0; f < nf; ++f) bulk_g2s(dst + f * A.cap, a + g0[f], bytes[f], &full[lane]);
+          last = kk;
+        }
+      }
+      k += uint32_t(np);
+    }
+    // let every copy this lane issued land before the CTA exits (immediate
+    // unless a consumer gave up): the slot's last copy is its newest phase
+    if (last >= 0 && !stencil::mbar_wait_bounded(&full[lane], (uint32_t(last) / S) & 1u, A.wait_cycles)) bad = true;
+  } else {
+    uint32_t k = 0;
+    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+      const ItemDev I = items[it];
+      const ProbDev P = probs[I.prob];
+      if (P.kind == 0) ring_consume<1, uint32_t(S)>(P, I, ring, full, empty, A, b, k, bad);
+      else ring_consume<4, uint32_t(S)>(P, I, ring, full, empty, A, b, k, bad);
+    }
+  }
+  if (bad) atomicExch(err, stencil::kErrWaitTimeout);
+}
+
 }  // namespace
+
+constexpr int64_t kPoolPad = 4;  // spare floats at the end of a pool
 
 struct cfdb_batch {
   cfdb_ctx* ctx = nullptr;
+  int nmax = 0;  // largest n of the problem set
   std::vector<cfdb_problem> probs;
   int64_t pool = 0;
   ProbDev* d_probs = nullptr;
@@ -161,6 +389,9 @@ struct cfdb_batch {
   int n_items = 0;
   int items_cap = 0;
   int cells_per_item = 2048, threads = 256, ctas_per_sm = 4;
+  int staged = 1;  // use the staged (ring) kernel where it applies
+  int ring_resident = 0;          // CTAs of the staged kernel one SM holds
+  int64_t ring_resident_key = -1;  // (threads, shared bytes) ring_resident was measured for
   int64_t last_launches = 0;
   cudaGraphExec_t graph = nullptr;
   const void* graph_a = nullptr;
@@ -196,10 +427,57 @@ void drop_graph(cfdb_batch* b) {
   b->graph = nullptr;
 }
 
+// Dynamic shared memory of the staged kernel: `slots` slots of 4 field
+// tiles, each the item's C columns plus n rows either side and the alignment
+// slack.
+int ring_cap(int threads, int nmax) { return (threads + 2 * nmax + 8 + 3) / 4 * 4; }
+size_t ring_smem(int slots, int threads, int nmax) { return size_t(slots) * 4 * ring_cap(threads, nmax) * sizeof(float); }
+constexpr size_t kRingSmemPerSm = 220 * 1024;
+// 8 slots where ctas_per_sm CTAs hold them, else 4 (0: not even 4 fit)
+int ring_slots(int threads, int ctas_per_sm, int nmax) {
+  for (int slots : {8, 4})
+    if (ring_smem(slots, threads, nmax) * size_t(ctas_per_sm) <= kRingSmemPerSm) return slots;
+  return 0;
+}
+
+// The staged kernel runs when both pools start on a 16-byte boundary and its
+// ring fits the shared memory of ctas_per_sm CTAs on one SM; otherwise the
+// column march (same arithmetic, same results) runs.
+bool ring_ok(const cfdb_batch* b, int threads, int ctas_per_sm, const void* a, const void* out) {
+  if ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(out)) & 15u) return false;
+  return ring_slots(threads, ctas_per_sm, b->nmax) > 0 && (threads + 32) * ctas_per_sm <= 2048;
+}
+
 int launch(cfdb_batch* b, const void* a, void* out) {
   const int grid = std::max(1, b->ctx->num_sms) * b->ctas_per_sm;
-  batch_step_k<<<grid, b->threads, 0, b->ctx->stream>>>(b->d_probs, b->d_items, b->n_items,
-                                                        static_cast<const float*>(a), static_cast<float*>(out));
+  if (b->staged && ring_ok(b, b->threads, b->ctas_per_sm, a, out)) {
+    const int slots = ring_slots(b->threads, b->ctas_per_sm, b->nmax);
+    const size_t smem = ring_smem(slots, b->threads, b->nmax);
+    auto kern = slots == 8 ? batch_ring_k<8> : batch_ring_k<4>;
+    static size_t attr_set[2][kMaxDevices] = {};
+    const int dev = b->ctx->device;
+    if (dev < 0 || dev >= kMaxDevices) return cfdb_fail(b->ctx, CFDB_EUNSUPPORTED, "device ordinal %d", dev);
+    if (attr_set[slots == 8][dev] < smem) {
+      CFDB_CUDA(b->ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+      attr_set[slots == 8][dev] = smem;
+    }
+    // a persistent grid must be resident at once: clamp to the occupancy
+    const int64_t key = int64_t(b->threads) << 32 | int64_t(smem) << 1 | (slots == 8);
+    if (b->ring_resident_key != key) {
+      int res = 0;
+      CFDB_CUDA(b->ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&res, kern, b->threads + 32, smem));
+      b->ring_resident = std::max(1, res);
+      b->ring_resident_key = key;
+    }
+    const int rgrid = std::max(1, b->ctx->num_sms) * std::min(b->ctas_per_sm, b->ring_resident);
+    RingArgs A{b->threads, ring_cap(b->threads, b->nmax), b->ctx->wait_cycles};
+    kern<<<rgrid, b->threads + 32, smem, b->ctx->stream>>>(b->d_probs, b->d_items, b->n_items,
+                                                           static_cast<const float*>(a), static_cast<float*>(out), A,
+                                                           b->ctx->d_error);
+  } else {
+    batch_step_k<<<grid, b->threads, 0, b->ctx->stream>>>(b->d_probs, b->d_items, b->n_items,
+                                                          static_cast<const float*>(a), static_cast<float*>(out));
+  }
   CFDB_LAUNCHED(b->ctx);
   return CFDB_OK;
 }
@@ -220,8 +498,10 @@ std::string cache_key(const cfdb_batch* b) {
   std::string name(prop.name);
   for (auto& ch : name)
     if (ch == '"' || ch == ' ') ch = '_';
-  // "march": the kernel generation (column march); entries tuned for another kernel never match
-  snprintf(buf, sizeof(buf), "march:%s:%d:%016llx", name.c_str(), int(b->probs.size()), (unsigned long long)h);
+  // the kernel generation ("ring": staged rows, "march": column march); entries
+  // tuned for another kernel never match
+  snprintf(buf, sizeof(buf), "%s:%s:%d:%016llx", b->staged ? "ring" : "march", name.c_str(), int(b->probs.size()),
+           (unsigned long long)h);
   return buf;
 }
 
@@ -288,12 +568,16 @@ extern "C" int cfdb_batch_create(cfdb_ctx* ctx, cfdb_problem* probs, int32_t cou
     p.offset = off;
     off += int64_t(p.n) * p.n * p.n * (p.kind == 1 ? 4 : 1);
   }
+  const int64_t cells = off;
+  off += kPoolPad;  // the staged kernel's copies end on a 16-byte boundary
   CFDB_CUDA(ctx, cudaSetDevice(ctx->device));
   auto* b = new (std::nothrow) cfdb_batch();
   if (!b) return cfdb_fail(ctx, CFDB_ENOMEM, "host allocation failed");
   b->ctx = ctx;
   b->probs.assign(probs, probs + count);
   b->pool = off;
+  for (int32_t i = 0; i < count; ++i) b->nmax = std::max(b->nmax, probs[i].n);
+  (void)cells;
   std::vector<ProbDev> pd(count);
   for (int32_t i = 0; i < count; ++i) {
     const cfdb_problem& p = probs[i];
@@ -353,6 +637,13 @@ extern "C" int cfdb_batch_set_config(cfdb_batch* b, int32_t cells_per_item, int3
   b->ctas_per_sm = ctas_per_sm;
   drop_graph(b);
   return items_change ? build_items(b) : CFDB_OK;
+}
+
+extern "C" int cfdb_batch_set_staged(cfdb_batch* b, int staged) {
+  if (!b || !b->ctx) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_batch_set_staged: handle is NULL or its context was destroyed");
+  b->staged = staged ? 1 : 0;
+  drop_graph(b);
+  return CFDB_OK;
 }
 
 extern "C" int cfdb_batch_get_config(const cfdb_batch* b, int32_t* cells_per_item, int32_t* threads, int32_t* ctas) {
@@ -453,14 +744,19 @@ extern "C" int cfdb_batch_tune(cfdb_batch* b, void* a, void* out, const char* ca
   CFDB_CUDA(ctx, cudaEventCreate(&e1));
   float best = INFINITY;
   int bc[3] = {b->cells_per_item, b->threads, b->ctas_per_sm};
-  const int cpis[] = {512, 1024, 2048, 4096, 8192};
-  const int ths[] = {128, 256, 512};
-  const int ctas[] = {2, 4, 8, 16};
+  // candidates: the column march times items of 512-8192 cells at 2-16 CTAs
+  // per SM; the staged kernel keeps S planes in flight per CTA, so it wants
+  // longer items and fewer, larger CTAs (shared memory bounds them)
+  const std::vector<int> cpis = b->staged ? std::vector<int>{2048, 4096, 8192, 16384, 32768}
+                                          : std::vector<int>{512, 1024, 2048, 4096, 8192};
+  const std::vector<int> ths = {128, 256, 512};
+  const std::vector<int> ctas = b->staged ? std::vector<int>{1, 2, 3, 4, 6} : std::vector<int>{2, 4, 8, 16};
   int rc = CFDB_OK;
   for (int cpi : cpis)
     for (int th : ths)
       for (int ct : ctas) {
         if (th * ct > 2048) continue;
+        if (b->staged && !ring_ok(b, th, ct, a, out)) continue;  // only configurations the staged kernel takes
         if ((rc = cfdb_batch_set_config(b, cpi, th, ct))) break;
         if ((rc = launch(b, a, out))) break;  // warm-up
         cudaEventRecord(e0, ctx->stream);

@@ -328,6 +328,18 @@ extern "C" int cfdb_download(cfdb_ctx* ctx, void* dst, const void* src, int64_t 
   return CFDB_OK;
 }
 
+extern "C" int cfdb_upload_async(cfdb_ctx* ctx, void* dst, const void* src, int64_t bytes) {
+  if (!ctx || !dst || !src || bytes < 0) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_upload_async: bad arguments");
+  CFDB_CUDA(ctx, cudaMemcpyAsync(dst, src, size_t(bytes), cudaMemcpyHostToDevice, ctx->stream));
+  return CFDB_OK;
+}
+
+extern "C" int cfdb_download_async(cfdb_ctx* ctx, void* dst, const void* src, int64_t bytes) {
+  if (!ctx || !dst || !src || bytes < 0) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_download_async: bad arguments");
+  CFDB_CUDA(ctx, cudaMemcpyAsync(dst, src, size_t(bytes), cudaMemcpyDeviceToHost, ctx->stream));
+  return CFDB_OK;
+}
+
 // ---------------------------------------------------------------------------
 // meshes
 // ---------------------------------------------------------------------------

@@ -133,6 +133,15 @@ int cfdb_alloc(cfdb_ctx* ctx, int64_t bytes, void** out);
 int cfdb_free(cfdb_ctx* ctx, void* ptr);
 int cfdb_upload(cfdb_ctx* ctx, void* dst_device, const void* src_host, int64_t bytes);
 int cfdb_download(cfdb_ctx* ctx, void* dst_host, const void* src_device, int64_t bytes);
+/* The same copies queued on the context's stream without waiting: the host
+ * buffer must stay valid (and, for a download, unread) until the stream has
+ * passed the copy (cfdb_sync, or a later stream event).  With page-locked
+ * host memory the copy runs on a copy engine, overlapping kernels of other
+ * streams.  A caller that streams solves puts the copies on a second
+ * context bound to its own stream.  No reference counterpart: from_eigen /
+ * to_eigen are synchronous. */
+int cfdb_upload_async(cfdb_ctx* ctx, void* dst_device, const void* src_host, int64_t bytes);
+int cfdb_download_async(cfdb_ctx* ctx, void* dst_host, const void* src_device, int64_t bytes);
 
 /* ---- mesh ------------------------------------------------------------- */
 
@@ -358,7 +367,8 @@ typedef struct {
 } cfdb_problem;
 
 /* probs[i].offset is filled in on return; *pool_elems = elements (of dtype
- * F32) one state pool must hold. */
+ * F32) one state pool must hold (the problems' cells plus 4 spare floats at
+ * the end, which the staged kernel's 16-byte copies may read). */
 int cfdb_batch_create(cfdb_ctx* ctx, cfdb_problem* probs, int32_t count, int64_t* pool_elems, cfdb_batch** out);
 int cfdb_batch_destroy(cfdb_batch* b);
 /* cells_per_item: cells one CTA work item covers (threads (y, z) columns x
@@ -366,6 +376,13 @@ int cfdb_batch_destroy(cfdb_batch* b);
  * persistent grid = SMs x ctas_per_sm. */
 int cfdb_batch_set_config(cfdb_batch* b, int32_t cells_per_item, int32_t threads, int32_t ctas_per_sm);
 int cfdb_batch_get_config(const cfdb_batch* b, int32_t* cells_per_item, int32_t* threads, int32_t* ctas_per_sm);
+/* Kernel form: staged = 1 (default) streams each work item's plane rows
+ * into a shared-memory ring with bulk copies (a producer warp and `threads`
+ * consumer threads per CTA; needs 16-byte aligned pools and a ring that fits
+ * shared memory, otherwise the column march runs); staged = 0 always runs
+ * the column march.  Both give the same bits.  The tuner's cache entries
+ * are kept per form. */
+int cfdb_batch_set_staged(cfdb_batch* b, int staged);
 /* Autotuner: times candidate configurations on the given pools (contents are
  * advanced and must be re-initialised afterwards) and keeps the fastest;
  * results are cached in cache_path (JSON, may be NULL) keyed by device and

@@ -92,3 +92,34 @@ def test_batch_rejects_bad_problems(cfdb, ctx):
     b = cfdb.Batch(ctx, [dict(n=8, kind=0, param=0.01, dt=1e-3)])
     with pytest.raises(cfdb.CfdbError):
         b.set_config(256, 100, 4)
+
+
+def mixed_problems():
+    from cfdarcov2_b200.workloads import ensemble_problems
+    return ensemble_problems(count=40, nmin=5, nmax=70, seed=17)
+
+
+@pytest.mark.parametrize("cfg", [(2048, 128, 4), (8192, 256, 2), (32768, 512, 1), (256, 256, 3)])
+def test_staged_ring_equals_column_march_bitwise(cfdb, ctx, cfg):
+    """The staged kernel (a producer warp streaming plane rows into a
+    shared-memory ring, consumer warps marching the columns) gives the column
+    march's bits: items shorter and longer than n, column runs shorter and
+    longer than n^2, 1-4 CTAs per SM; the wave velocities are non-zero."""
+    from cfdarcov2_b200.workloads import ensemble_initial
+    probs = mixed_problems()
+    b = cfdb.Batch(ctx, probs)
+    pool0 = ensemble_initial(probs, b.offsets, b.pool_elems)
+    rng = np.random.default_rng(9)
+    for p, off in zip(probs, b.offsets):
+        if p["kind"] == 1:
+            n3 = p["n"] ** 3
+            pool0[off + n3: off + 4 * n3] = rng.standard_normal(3 * n3) * 0.1
+    b.set_config(*cfg)
+    outs = []
+    for staged, graph in ((True, True), (True, False), (False, False)):
+        b.set_staged(staged)
+        a = torch.tensor(pool0, device=DEV)
+        c = torch.empty_like(a)
+        outs.append(b.run(a, c, 9, use_graph=graph).clone())
+    ctx.sync()
+    assert torch.equal(outs[0], outs[2]) and torch.equal(outs[1], outs[2])

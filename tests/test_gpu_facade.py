@@ -130,6 +130,32 @@ def test_reference_euler_system_jit_equals_operator_path(tmp_path, n):
     assert np.array_equal(A, P)
 
 
+@pytest.mark.parametrize("n,steps", [(16, 20), (13, 12)])
+def test_reference_euler_system_matches_oracle(oracle, tmp_path, n, steps):
+    """The reference's 20-equation Euler system (examples/main_3d.cpp:238-263)
+    as the example runs it on the GPU (generated kernels, FP32) against the
+    oracle's run of the same system (oracle/euler_system.py: the CPU path's
+    loop order of src/fvm3d.cpp:1008-1049 over the restated operators),
+    started from the example's own initial state (a 0-step run).  Against
+    the FP64 run every field is within 1e-5 (rel L2); against the FP32 run,
+    which rounds like the reference, within 1e-6."""
+    from oracle import euler_system as ES
+    init, _ = run_example(tmp_path, "euler3d", n, n, n, 0, 5)
+    J, out = run_example(tmp_path, "euler3d", n, n, n, steps, 5)
+    assert "jit_equations=20" in out
+    prim0 = [init[k].astype(np.float32) for k in range(5)]
+    ref64, dts = ES.run(n, n, n, steps, *prim0, dtype=np.float64)
+    ref32, _ = ES.run(n, n, n, steps, *prim0, dtype=np.float32)
+    moved = max(rel_l2(ref64[k], init[k]) for k in range(5))
+    assert moved > 1e-4  # the state has evolved
+    for k, name in enumerate(("rho", "u", "v", "w", "p")):
+        e64, e32 = rel_l2(J[k], ref64[k]), rel_l2(J[k], ref32[k])
+        print(f"{name}: rel L2 vs FP64 oracle {e64:.2e}, vs FP32 oracle {e32:.2e}, "
+              f"bitwise FP32 {np.array_equal(J[k], ref32[k].astype(np.float64))}")
+        assert e64 <= 1e-5, (name, e64)
+        assert e32 <= 1e-6, (name, e32)
+
+
 def test_jit_heat_on_a_mesh_the_sweep_cannot_take(oracle, tmp_path):
     """The heat template on nz % 4 != 0 cannot use the fused TMA step; with
     use_jit it runs as a generated kernel and matches the oracle."""

@@ -1,6 +1,7 @@
 """The bounded device wait of the TMA sweep runs out and reports, without any
-fault: a test hook arms one plane's barrier in the first CTA with the
-plane's byte count but issues no copy for it (a completion that never
+fault: a test hook arms one plane's barrier in the first CTA (its first
+interior plane, which every x chunk has) with the plane's byte count but
+issues no copy for it (a completion that never
 comes), with the wait bound lowered to 1e6 SM cycles (about 0.5 ms).  The
 launch must end by itself, cfdb_sync must return CFDB_ETIMEOUT, and the same
 context must then run a normal step with the correct result.  (The
@@ -35,7 +36,7 @@ def test_wait_runs_out_and_context_recovers(cfdb, kind):
     step(good)
     ctx.sync()
 
-    ctx.set_wait_limit(1_000_000, missing_plane=3)
+    ctx.set_wait_limit(1_000_000, missing_plane=1)  # plane 1 (x = x0) exists in every CTA's chunk
     bad = torch.zeros_like(q)
     step(bad)
     with pytest.raises(cfdb.CfdbError) as ei:

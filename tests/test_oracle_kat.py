@@ -237,3 +237,35 @@ def test_golden_fixtures(oracle):
     now = compute_cases(oracle)
     for k in data.files:
         assert np.array_equal(data[k], now[k]), k
+
+
+def test_reference_euler_system_oracle_fp32_tracks_fp64():
+    """The oracle's run of the reference's 20-equation Euler system
+    (oracle/euler_system.py, examples/main_3d.cpp:187-263) from the example's
+    jet initial state on 16^3 unit cells: the FP32 run (the reference's
+    precision) stays within 1e-6 of the FP64 run over 20 steps, the CFL dt is
+    the same to FP32 rounding, the boundary layer keeps its initial values
+    and the jet has moved the state."""
+    from oracle import euler_system as ES
+    n, steps = 16, 20
+    f32 = np.float32
+    c = (np.arange(n) + 0.5).astype(f32)
+    X, Y, Z = [a.reshape(-1) for a in np.meshgrid(c, c, c, indexing="ij")]
+    L = f32(n)
+    jet = (f32(0.4) * L < X) & (X < f32(0.6) * L) & (f32(0.4) * L < Y) & (Y < f32(0.6) * L)
+    rho0 = np.where(jet, f32(5), f32(1)).astype(f32)
+    band = (Z / (f32(0.1) * L)).astype(int)
+    u0 = np.where(band % 2 == 0, f32(-0.1), f32(0.1)).astype(f32)
+    w0 = np.full(n ** 3, f32(0.6))
+    p0 = np.full(n ** 3, f32(2.5))
+    a, dta = ES.run(n, n, n, steps, rho0, u0, u0.copy(), w0, p0, dtype=np.float64)
+    b, dtb = ES.run(n, n, n, steps, rho0, u0, u0.copy(), w0, p0, dtype=np.float32)
+    for A, B in zip(a, b):
+        assert np.isfinite(B).all()
+        assert np.linalg.norm(A - B) / np.linalg.norm(A) <= 1e-6
+    assert np.allclose(dta, dtb, rtol=1e-6, atol=0)
+    shell = np.zeros((n, n, n), bool)
+    shell[[0, -1], :, :] = shell[:, [0, -1], :] = shell[:, :, [0, -1]] = True
+    shell = shell.reshape(-1)
+    assert np.array_equal(a[0][shell], rho0[shell].astype(np.float64))
+    assert np.abs(a[0] - rho0).max() > 0.1
