@@ -140,8 +140,11 @@ __device__ __forceinline__ void column_step(const ProbDev& P, const ItemDev& I, 
   }
 }
 
-// One launch per step walks the work items.
-__global__ void batch_step_k(const ProbDev* __restrict__ probs, const ItemDev* __restrict__ items, int n_items,
+// One launch per step walks the work items.  Blocks of up to 256 threads
+// are compiled to 48 registers (no spills), so 40 warps fit an SM instead of
+// 32 and more plane loads are in flight; 512-thread blocks keep 64.
+template <int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB) batch_step_k(const ProbDev* __restrict__ probs, const ItemDev* __restrict__ items, int n_items,
                              const float* __restrict__ a, float* __restrict__ b) {
   for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
     const ItemDev I = items[it];
@@ -389,7 +392,7 @@ struct cfdb_batch {
   int n_items = 0;
   int items_cap = 0;
   int cells_per_item = 2048, threads = 256, ctas_per_sm = 4;
-  int staged = 1;  // use the staged (ring) kernel where it applies
+  int staged = 0;  // 1: the staged (ring) kernel where it applies; the tuner picks the faster form
   int ring_resident = 0;          // CTAs of the staged kernel one SM holds
   int64_t ring_resident_key = -1;  // (threads, shared bytes) ring_resident was measured for
   int64_t last_launches = 0;
@@ -474,9 +477,12 @@ int launch(cfdb_batch* b, const void* a, void* out) {
     kern<<<rgrid, b->threads + 32, smem, b->ctx->stream>>>(b->d_probs, b->d_items, b->n_items,
                                                            static_cast<const float*>(a), static_cast<float*>(out), A,
                                                            b->ctx->d_error);
+  } else if (b->threads <= 256) {
+    batch_step_k<256, 5><<<grid, b->threads, 0, b->ctx->stream>>>(b->d_probs, b->d_items, b->n_items,
+                                                                   static_cast<const float*>(a), static_cast<float*>(out));
   } else {
-    batch_step_k<<<grid, b->threads, 0, b->ctx->stream>>>(b->d_probs, b->d_items, b->n_items,
-                                                          static_cast<const float*>(a), static_cast<float*>(out));
+    batch_step_k<512, 2><<<grid, b->threads, 0, b->ctx->stream>>>(b->d_probs, b->d_items, b->n_items,
+                                                                   static_cast<const float*>(a), static_cast<float*>(out));
   }
   CFDB_LAUNCHED(b->ctx);
   return CFDB_OK;
@@ -498,14 +504,14 @@ std::string cache_key(const cfdb_batch* b) {
   std::string name(prop.name);
   for (auto& ch : name)
     if (ch == '"' || ch == ' ') ch = '_';
-  // the kernel generation ("ring": staged rows, "march": column march); entries
-  // tuned for another kernel never match
-  snprintf(buf, sizeof(buf), "%s:%s:%d:%016llx", b->staged ? "ring" : "march", name.c_str(), int(b->probs.size()),
-           (unsigned long long)h);
+  // "forms": entries of this kernel generation hold the winning form too;
+  // entries tuned for an earlier kernel never match
+  snprintf(buf, sizeof(buf), "forms:%s:%d:%016llx", name.c_str(), int(b->probs.size()), (unsigned long long)h);
   return buf;
 }
 
-// The cache file is a flat JSON object {"key": [cells_per_item, threads, ctas_per_sm], ...}.
+// The cache file is a flat JSON object
+// {"key": [cells_per_item, threads, ctas_per_sm, staged], ...}.
 std::map<std::string, std::vector<int>> read_cache(const char* path) {
   std::map<std::string, std::vector<int>> out;
   if (!path) return out;
@@ -521,8 +527,8 @@ std::map<std::string, std::vector<int>> read_cache(const char* path) {
     const std::string key = s.substr(pos + 1, end - pos - 1);
     const size_t lb = s.find('[', end), rb = s.find(']', end);
     if (lb == std::string::npos || rb == std::string::npos) break;
-    int v0 = 0, v1 = 0, v2 = 0;
-    if (sscanf(s.c_str() + lb, "[%d , %d , %d]", &v0, &v1, &v2) == 3) out[key] = {v0, v1, v2};
+    int v0 = 0, v1 = 0, v2 = 0, v3 = 0;
+    if (sscanf(s.c_str() + lb, "[%d , %d , %d , %d]", &v0, &v1, &v2, &v3) == 4) out[key] = {v0, v1, v2, v3};
     pos = rb + 1;
   }
   return out;
@@ -539,8 +545,8 @@ void write_cache(const char* path, const std::map<std::string, std::vector<int>>
     f << "{\n";
     size_t k = 0;
     for (const auto& kv : m) {
-      f << "  \"" << kv.first << "\": [" << kv.second[0] << ", " << kv.second[1] << ", " << kv.second[2] << "]"
-        << (++k < m.size() ? ",\n" : "\n");
+      f << "  \"" << kv.first << "\": [" << kv.second[0] << ", " << kv.second[1] << ", " << kv.second[2] << ", "
+        << kv.second[3] << "]" << (++k < m.size() ? ",\n" : "\n");
     }
     f << "}\n";
     if (!f) {
@@ -737,46 +743,54 @@ extern "C" int cfdb_batch_tune(cfdb_batch* b, void* a, void* out, const char* ca
   auto cache = read_cache(cache_path);
   const std::string key = cache_key(b);
   auto hit = cache.find(key);
-  if (hit != cache.end() && hit->second.size() == 3)
+  if (hit != cache.end() && hit->second.size() == 4) {
+    b->staged = hit->second[3] ? 1 : 0;
     if (cfdb_batch_set_config(b, hit->second[0], hit->second[1], hit->second[2]) == CFDB_OK) return CFDB_OK;
+  }
   cudaEvent_t e0, e1;
   CFDB_CUDA(ctx, cudaEventCreate(&e0));
   CFDB_CUDA(ctx, cudaEventCreate(&e1));
   float best = INFINITY;
-  int bc[3] = {b->cells_per_item, b->threads, b->ctas_per_sm};
-  // candidates: the column march times items of 512-8192 cells at 2-16 CTAs
-  // per SM; the staged kernel keeps S planes in flight per CTA, so it wants
-  // longer items and fewer, larger CTAs (shared memory bounds them)
-  const std::vector<int> cpis = b->staged ? std::vector<int>{2048, 4096, 8192, 16384, 32768}
-                                          : std::vector<int>{512, 1024, 2048, 4096, 8192};
-  const std::vector<int> ths = {128, 256, 512};
-  const std::vector<int> ctas = b->staged ? std::vector<int>{1, 2, 3, 4, 6} : std::vector<int>{2, 4, 8, 16};
+  int bc[4] = {b->cells_per_item, b->threads, b->ctas_per_sm, b->staged};
   int rc = CFDB_OK;
-  for (int cpi : cpis)
-    for (int th : ths)
-      for (int ct : ctas) {
-        if (th * ct > 2048) continue;
-        if (b->staged && !ring_ok(b, th, ct, a, out)) continue;  // only configurations the staged kernel takes
-        if ((rc = cfdb_batch_set_config(b, cpi, th, ct))) break;
-        if ((rc = launch(b, a, out))) break;  // warm-up
-        cudaEventRecord(e0, ctx->stream);
-        for (int k = 0; k < 4 && !rc; ++k) rc = (k & 1) ? launch(b, out, a) : launch(b, a, out);
-        cudaEventRecord(e1, ctx->stream);
-        cudaError_t e = cudaEventSynchronize(e1);
-        if (e != cudaSuccess) rc = cfdb_cuda_fail(ctx, e, "cudaEventSynchronize");
-        if (rc) break;
-        float ms = 0;
-        cudaEventElapsedTime(&ms, e0, e1);
-        if (ms < best) {
-          best = ms;
-          bc[0] = cpi; bc[1] = th; bc[2] = ct;
+  // Both kernel forms.  The column march times items of 512-8192 cells at
+  // 2-16 CTAs per SM; the staged kernel keeps several planes in flight per
+  // CTA, so it wants longer items and fewer, larger CTAs (shared memory
+  // bounds them), and only configurations it takes are timed.
+  for (int staged : {0, 1}) {
+    b->staged = staged;
+    const std::vector<int> cpis = staged ? std::vector<int>{2048, 8192, 32768, 131072}
+                                         : std::vector<int>{512, 1024, 2048, 4096, 8192};
+    const std::vector<int> ths = {128, 256, 512};
+    const std::vector<int> ctas = staged ? std::vector<int>{1, 2, 3, 4} : std::vector<int>{2, 4, 5, 8, 10, 16};
+    for (int cpi : cpis)
+      for (int th : ths)
+        for (int ct : ctas) {
+          if (th * ct > 2048 || rc) continue;
+          if (staged && !ring_ok(b, th, ct, a, out)) continue;
+          if ((rc = cfdb_batch_set_config(b, cpi, th, ct))) break;
+          if ((rc = launch(b, a, out))) break;  // warm-up
+          cudaEventRecord(e0, ctx->stream);
+          for (int k = 0; k < 4 && !rc; ++k) rc = (k & 1) ? launch(b, out, a) : launch(b, a, out);
+          cudaEventRecord(e1, ctx->stream);
+          cudaError_t e = cudaEventSynchronize(e1);
+          if (e != cudaSuccess) rc = cfdb_cuda_fail(ctx, e, "cudaEventSynchronize");
+          if (rc) break;
+          float ms = 0;
+          cudaEventElapsedTime(&ms, e0, e1);
+          if (ms < best) {
+            best = ms;
+            bc[0] = cpi; bc[1] = th; bc[2] = ct; bc[3] = staged;
+          }
         }
-      }
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  if (!rc) rc = cfdb_check_device_error(ctx);  // a staged candidate whose wait ran out
   if (rc) return rc;
+  b->staged = bc[3];
   if ((rc = cfdb_batch_set_config(b, bc[0], bc[1], bc[2]))) return rc;
-  cache[key] = {bc[0], bc[1], bc[2]};
+  cache[key] = {bc[0], bc[1], bc[2], bc[3]};
   write_cache(cache_path, cache);
   return CFDB_OK;
 }
