@@ -396,9 +396,9 @@ class Batch:
     def set_config(self, cells_per_item, threads, ctas_per_sm):
         call("cfdb_batch_set_config", self.h, int(cells_per_item), int(threads), int(ctas_per_sm), ctx=self.ctx.h)
 
-    def set_staged(self, staged: bool) -> None:
-        """Kernel form: the staged row ring (default) or the column march."""
-        call("cfdb_batch_set_staged", self.h, int(bool(staged)), ctx=self.ctx.h)
+    def set_staged(self, form) -> None:
+        """Kernel form: 0 / False column march, 1 / True staged row ring, 2 column march at 48 registers."""
+        call("cfdb_batch_set_staged", self.h, int(form), ctx=self.ctx.h)
 
     def get_config(self):
         a, b, c = C.c_int32(), C.c_int32(), C.c_int32()

@@ -140,9 +140,11 @@ __device__ __forceinline__ void column_step(const ProbDev& P, const ItemDev& I, 
   }
 }
 
-// One launch per step walks the work items.  Blocks of up to 256 threads
-// are compiled to 48 registers (no spills), so 40 warps fit an SM instead of
-// 32 and more plane loads are in flight; 512-thread blocks keep 64.
+// One launch per step walks the work items.  Two register budgets: 64
+// (MINB = 1), or 48 for blocks of up to 256 threads (no spills), where 40
+// warps fit an SM instead of 32 and more plane loads are in flight -- faster
+// for heat-only batches (260 against 312 us per step at 512 cubes), slower
+// for the mixed heat/wave set, so the tuner picks.
 template <int MAXT, int MINB>
 __global__ void __launch_bounds__(MAXT, MINB) batch_step_k(const ProbDev* __restrict__ probs, const ItemDev* __restrict__ items, int n_items,
                              const float* __restrict__ a, float* __restrict__ b) {
@@ -381,6 +383,8 @@ __global__ void batch_ring_k(const ProbDev* __restrict__ probs, const ItemDev* _
 }  // namespace
 
 constexpr int64_t kPoolPad = 4;  // spare floats at the end of a pool
+// kernel forms (cfdb_batch_set_staged)
+constexpr int kFormMarch = 0, kFormRing = 1, kFormMarch48 = 2;
 
 struct cfdb_batch {
   cfdb_ctx* ctx = nullptr;
@@ -392,7 +396,7 @@ struct cfdb_batch {
   int n_items = 0;
   int items_cap = 0;
   int cells_per_item = 2048, threads = 256, ctas_per_sm = 4;
-  int staged = 0;  // 1: the staged (ring) kernel where it applies; the tuner picks the faster form
+  int staged = kFormMarch;  // kernel form (kForm*); the tuner picks the fastest
   int ring_resident = 0;          // CTAs of the staged kernel one SM holds
   int64_t ring_resident_key = -1;  // (threads, shared bytes) ring_resident was measured for
   int64_t last_launches = 0;
@@ -453,7 +457,7 @@ bool ring_ok(const cfdb_batch* b, int threads, int ctas_per_sm, const void* a, c
 
 int launch(cfdb_batch* b, const void* a, void* out) {
   const int grid = std::max(1, b->ctx->num_sms) * b->ctas_per_sm;
-  if (b->staged && ring_ok(b, b->threads, b->ctas_per_sm, a, out)) {
+  if (b->staged == kFormRing && ring_ok(b, b->threads, b->ctas_per_sm, a, out)) {
     const int slots = ring_slots(b->threads, b->ctas_per_sm, b->nmax);
     const size_t smem = ring_smem(slots, b->threads, b->nmax);
     auto kern = slots == 8 ? batch_ring_k<8> : batch_ring_k<4>;
@@ -477,12 +481,12 @@ int launch(cfdb_batch* b, const void* a, void* out) {
     kern<<<rgrid, b->threads + 32, smem, b->ctx->stream>>>(b->d_probs, b->d_items, b->n_items,
                                                            static_cast<const float*>(a), static_cast<float*>(out), A,
                                                            b->ctx->d_error);
-  } else if (b->threads <= 256) {
+  } else if (b->staged == kFormMarch48 && b->threads <= 256) {
     batch_step_k<256, 5><<<grid, b->threads, 0, b->ctx->stream>>>(b->d_probs, b->d_items, b->n_items,
                                                                    static_cast<const float*>(a), static_cast<float*>(out));
   } else {
-    batch_step_k<512, 2><<<grid, b->threads, 0, b->ctx->stream>>>(b->d_probs, b->d_items, b->n_items,
-                                                                   static_cast<const float*>(a), static_cast<float*>(out));
+    batch_step_k<1024, 1><<<grid, b->threads, 0, b->ctx->stream>>>(b->d_probs, b->d_items, b->n_items,
+                                                                    static_cast<const float*>(a), static_cast<float*>(out));
   }
   CFDB_LAUNCHED(b->ctx);
   return CFDB_OK;
@@ -647,7 +651,9 @@ extern "C" int cfdb_batch_set_config(cfdb_batch* b, int32_t cells_per_item, int3
 
 extern "C" int cfdb_batch_set_staged(cfdb_batch* b, int staged) {
   if (!b || !b->ctx) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_batch_set_staged: handle is NULL or its context was destroyed");
-  b->staged = staged ? 1 : 0;
+  if (staged < kFormMarch || staged > kFormMarch48)
+    return cfdb_fail(b->ctx, CFDB_EINVAL, "cfdb_batch_set_staged: form %d is not 0, 1 or 2", staged);
+  b->staged = staged;
   drop_graph(b);
   return CFDB_OK;
 }
@@ -744,7 +750,7 @@ extern "C" int cfdb_batch_tune(cfdb_batch* b, void* a, void* out, const char* ca
   const std::string key = cache_key(b);
   auto hit = cache.find(key);
   if (hit != cache.end() && hit->second.size() == 4) {
-    b->staged = hit->second[3] ? 1 : 0;
+    b->staged = std::min(std::max(hit->second[3], kFormMarch), kFormMarch48);
     if (cfdb_batch_set_config(b, hit->second[0], hit->second[1], hit->second[2]) == CFDB_OK) return CFDB_OK;
   }
   cudaEvent_t e0, e1;
@@ -757,17 +763,19 @@ extern "C" int cfdb_batch_tune(cfdb_batch* b, void* a, void* out, const char* ca
   // 2-16 CTAs per SM; the staged kernel keeps several planes in flight per
   // CTA, so it wants longer items and fewer, larger CTAs (shared memory
   // bounds them), and only configurations it takes are timed.
-  for (int staged : {0, 1}) {
-    b->staged = staged;
-    const std::vector<int> cpis = staged ? std::vector<int>{2048, 8192, 32768, 131072}
-                                         : std::vector<int>{512, 1024, 2048, 4096, 8192};
-    const std::vector<int> ths = {128, 256, 512};
-    const std::vector<int> ctas = staged ? std::vector<int>{1, 2, 3, 4} : std::vector<int>{2, 4, 5, 8, 10, 16};
+  for (int form : {kFormMarch, kFormMarch48, kFormRing}) {
+    b->staged = form;
+    const bool ring = form == kFormRing;
+    const std::vector<int> cpis = ring ? std::vector<int>{2048, 8192, 32768, 131072}
+                                       : std::vector<int>{512, 1024, 2048, 4096, 8192};
+    const std::vector<int> ths = form == kFormMarch48 ? std::vector<int>{128, 256} : std::vector<int>{128, 256, 512};
+    const std::vector<int> ctas = ring ? std::vector<int>{1, 2, 3, 4}
+                                       : (form == kFormMarch48 ? std::vector<int>{5, 10} : std::vector<int>{2, 4, 8, 16});
     for (int cpi : cpis)
       for (int th : ths)
         for (int ct : ctas) {
           if (th * ct > 2048 || rc) continue;
-          if (staged && !ring_ok(b, th, ct, a, out)) continue;
+          if (ring && !ring_ok(b, th, ct, a, out)) continue;
           if ((rc = cfdb_batch_set_config(b, cpi, th, ct))) break;
           if ((rc = launch(b, a, out))) break;  // warm-up
           cudaEventRecord(e0, ctx->stream);
@@ -780,7 +788,7 @@ extern "C" int cfdb_batch_tune(cfdb_batch* b, void* a, void* out, const char* ca
           cudaEventElapsedTime(&ms, e0, e1);
           if (ms < best) {
             best = ms;
-            bc[0] = cpi; bc[1] = th; bc[2] = ct; bc[3] = staged;
+            bc[0] = cpi; bc[1] = th; bc[2] = ct; bc[3] = form;
           }
         }
   }

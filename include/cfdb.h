@@ -376,12 +376,14 @@ int cfdb_batch_destroy(cfdb_batch* b);
  * persistent grid = SMs x ctas_per_sm. */
 int cfdb_batch_set_config(cfdb_batch* b, int32_t cells_per_item, int32_t threads, int32_t ctas_per_sm);
 int cfdb_batch_get_config(const cfdb_batch* b, int32_t* cells_per_item, int32_t* threads, int32_t* ctas_per_sm);
-/* Kernel form: staged = 1 streams each work item's plane rows into a
- * shared-memory ring with bulk copies (a producer warp and `threads`
- * consumer threads per CTA; needs 16-byte aligned pools and a ring that fits
- * shared memory, otherwise the column march runs); staged = 0 (the default)
- * runs the column march.  Both give the same bits.  cfdb_batch_tune times
- * both forms and keeps the faster (its cache entries record the form). */
+/* Kernel form: 0 (the default) = the column march (one (y, z) column per
+ * thread, neighbours through L1); 2 = the same compiled to 48 registers
+ * (blocks of up to 256 threads: more resident warps); 1 = the staged form,
+ * which streams each work item's plane rows into a shared-memory ring with
+ * bulk copies (a producer warp and `threads` consumer threads per CTA; needs
+ * 16-byte aligned pools and a ring that fits shared memory, otherwise the
+ * column march runs).  All give the same bits.  cfdb_batch_tune times every
+ * form and keeps the fastest (its cache entries record the form). */
 int cfdb_batch_set_staged(cfdb_batch* b, int staged);
 /* Autotuner: times candidate configurations on the given pools (contents are
  * advanced and must be re-initialised afterwards) and keeps the fastest;

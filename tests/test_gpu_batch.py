@@ -79,7 +79,7 @@ def test_autotuner_caches_choice(cfdb, ctx, tmp_path):
     chosen = b.get_config()
     data = json.loads(cache.read_text())
     assert len(data) == 1 and list(data.values())[0][:3] == list(chosen)
-    assert list(data.values())[0][3] in (0, 1)  # the kernel form that won
+    assert list(data.values())[0][3] in (0, 1, 2)  # the kernel form that won
     b2 = cfdb.Batch(ctx, probs)
     b2.tune(a, c, cache)  # served from the cache
     assert b2.get_config() == chosen
@@ -117,10 +117,12 @@ def test_staged_ring_equals_column_march_bitwise(cfdb, ctx, cfg):
             pool0[off + n3: off + 4 * n3] = rng.standard_normal(3 * n3) * 0.1
     b.set_config(*cfg)
     outs = []
-    for staged, graph in ((True, True), (True, False), (False, False)):
-        b.set_staged(staged)
+    for form, graph in ((1, True), (1, False), (0, False), (2, True)):
+        b.set_staged(form)
         a = torch.tensor(pool0, device=DEV)
         c = torch.empty_like(a)
         outs.append(b.run(a, c, 9, use_graph=graph).clone())
     ctx.sync()
-    assert torch.equal(outs[0], outs[2]) and torch.equal(outs[1], outs[2])
+    assert all(torch.equal(o, outs[2]) for o in outs)
+    with pytest.raises(cfdb.CfdbError):
+        b.set_staged(3)
