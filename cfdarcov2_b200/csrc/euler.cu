@@ -189,28 +189,41 @@ struct EulerPhys {
       is_last = atomicAdd(&ck->counter, 1u) == nblocks - 1;
     }
     __syncthreads();
-    if (is_last && threadIdx.x == 0) {
+    // The last CTA folds the per-CTA partials with its first warp: lane l
+    // takes partials l, l + 32, ... in order, then the lanes merge pairwise
+    // through shuffles in a fixed pattern, so the totals do not depend on
+    // timing (a single thread folding every partial serially kept all other
+    // SMs waiting for ~3 us per step).
+    if (is_last && threadIdx.x < 32) {
       __threadfence();
       double S0 = 0, C0 = 0, S1 = 0, C1 = 0;
-      for (unsigned k = 0; k < nblocks; ++k) {
+      for (unsigned k = threadIdx.x; k < nblocks; k += 32) {
         const Comp2 q = a.part[k];
         comp_add(S0, C0, q.s0); C0 += q.c0;
         comp_add(S1, C1, q.s1); C1 += q.c1;
       }
-      ck->counter = 0;
-      const int ts = int(a.s & 1);
-      const int ls = int(a.s % 3);
-      const double lam[3] = {bits_to_double(ck->lam[ls][0]), bits_to_double(ck->lam[ls][1]),
-                             bits_to_double(ck->lam[ls][2])};
-      bool last;
-      const double t = ck->t[ts];
-      const double dt = euler_dt(lam, a.dx, a.dy, a.dz, a.cfl, t, a.t_end, &last);
-      const long long step = ck->steps[ts] + 1;
-      ck->t[ts ^ 1] = last ? a.t_end : t + dt;
-      ck->steps[ts ^ 1] = step;
-      ck->finished[ts ^ 1] = (last || !(t + dt < a.t_end) || step >= a.max_steps) ? 1 : 0;
-      a.totals[2 * step] = S0 + C0;
-      a.totals[2 * step + 1] = S1 + C1;
+      for (int o = 16; o > 0; o >>= 1) {
+        const double a0 = __shfl_xor_sync(0xffffffffu, S0, o), b0 = __shfl_xor_sync(0xffffffffu, C0, o);
+        const double a1 = __shfl_xor_sync(0xffffffffu, S1, o), b1 = __shfl_xor_sync(0xffffffffu, C1, o);
+        comp_add(S0, C0, a0); C0 += b0;
+        comp_add(S1, C1, a1); C1 += b1;
+      }
+      if (threadIdx.x == 0) {
+        ck->counter = 0;
+        const int ts = int(a.s & 1);
+        const int ls = int(a.s % 3);
+        const double lam[3] = {bits_to_double(ck->lam[ls][0]), bits_to_double(ck->lam[ls][1]),
+                               bits_to_double(ck->lam[ls][2])};
+        bool last;
+        const double t = ck->t[ts];
+        const double dt = euler_dt(lam, a.dx, a.dy, a.dz, a.cfl, t, a.t_end, &last);
+        const long long step = ck->steps[ts] + 1;
+        ck->t[ts ^ 1] = last ? a.t_end : t + dt;
+        ck->steps[ts ^ 1] = step;
+        ck->finished[ts ^ 1] = (last || !(t + dt < a.t_end) || step >= a.max_steps) ? 1 : 0;
+        a.totals[2 * step] = S0 + C0;
+        a.totals[2 * step + 1] = S1 + C1;
+      }
     }
   }
 };
