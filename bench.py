@@ -46,6 +46,10 @@ def parse():
                    help="launch every step eagerly instead of replaying CUDA graphs (for profilers that skip graph nodes)")
     p.add_argument("--workload", default="wave", choices=["wave", "heat", "wave_distorted", "sod", "ensemble", "adjoint", "reference_rows"],
                    help="wave (default) is the headline; the others measure the remaining workloads on one GPU")
+    p.add_argument("--ensemble-form", default="tuned", choices=["tuned", "march", "ring", "march48"],
+                   help="ensemble kernel form: tuned (the autotuner's pick) or a fixed form with --ensemble-config")
+    p.add_argument("--ensemble-config", default="1024,128,8",
+                   help="cells_per_item,threads,ctas_per_sm for a fixed --ensemble-form")
     return p.parse_args()
 
 
@@ -668,7 +672,7 @@ def bench_sod(ctx, cfdb, dev, flush, S, max_steps=None):
                  extra, launches=res["fp32_fused"][5], traffic_profile="euler_sweep_sod.txt")
 
 
-def bench_ensemble(ctx, cfdb, dev, flush, S, tsteps=None):
+def bench_ensemble(ctx, cfdb, dev, flush, S, tsteps=None, form="tuned", shape=None):
     import tempfile
 
     import numpy as np
@@ -680,7 +684,11 @@ def bench_ensemble(ctx, cfdb, dev, flush, S, tsteps=None):
     init = W.ensemble_initial(probs, b.offsets, b.pool_elems)
     pool0 = torch.tensor(init, device=dev)
     a, c = pool0.clone(), torch.empty_like(pool0)
-    b.tune(a, c, os.path.join(tempfile.gettempdir(), "cfdb_ensemble_tune.json"))
+    if form == "tuned":
+        b.tune(a, c, os.path.join(tempfile.gettempdir(), "cfdb_ensemble_tune.json"))
+    else:
+        b.set_staged({"march": 0, "ring": 1, "march48": 2}[form])
+        b.set_config(*shape)
     T = tsteps or 300
     cells = sum(p["n"] ** 3 for p in probs)
     alg = sum(p["n"] ** 3 * (8 if p["kind"] == 0 else 32) for p in probs)
@@ -728,7 +736,7 @@ def bench_ensemble(ctx, cfdb, dev, flush, S, tsteps=None):
     line = _line(S, "ensemble_512_cubes_n16-96_x300_steps", cells * T * S.steps / (ms * 1e-3), ms / S.steps,
                  {"problems": len(probs), "cells": cells, "time_steps_per_bench_step": T,
                   "heat": sum(1 for p in probs if p["kind"] == 0), "wave": sum(1 for p in probs if p["kind"] == 1),
-                  "tuned_config": list(b.get_config())}, alg / cells, cells, T, extra, launches=ens_launches,
+                  "tuned_config": list(b.get_config()), "form": form}, alg / cells, cells, T, extra, launches=ens_launches,
                  traffic_profile="ensemble_batch_512.txt")
     b.close()
     return line
@@ -831,6 +839,9 @@ def run_secondary(args):
         kw["max_steps"] = args.tsteps
     elif args.tsteps:
         kw["tsteps"] = args.tsteps
+    if args.workload == "ensemble":
+        kw["form"] = args.ensemble_form
+        kw["shape"] = tuple(int(v) for v in args.ensemble_config.split(","))
     print(json.dumps(SECONDARY[args.workload](ctx, cfdb, dev, flush, S, **kw)), flush=True)
 
 
