@@ -449,12 +449,13 @@ def _timed(fn, steps, warmup, flush, prep=None, ctx=None):
 
 
 def _line(S, workload, value, ms_per_step, cfg, alg_bytes_per_update, updates_per_launch, launches_per_step,
-          extra, dtype="f32", launches=None, traffic_profile=None):
+          extra, dtype="f32", launches=None, traffic_profile=None, launch_ms=None):
     """One workload's line.  launches_per_step: time steps per bench step
-    (the roofline's per-launch time); launches: kernels counted by the
+    (the roofline's per-launch time, unless launch_ms gives the dominant
+    kernel's own average launch time); launches: kernels counted by the
     library in the timed region (gpu_launches)."""
     peak, kind = measured_peak_hbm()
-    launch_ms = ms_per_step / launches_per_step
+    launch_ms = launch_ms if launch_ms is not None else ms_per_step / launches_per_step
     ach = alg_bytes_per_update * updates_per_launch / (launch_ms * 1e-3) / 1e9
     line = {"metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": 1, "steps": S.steps,
             "warmup": S.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
@@ -785,7 +786,8 @@ def bench_adjoint(ctx, cfdb, dev, flush, S, n=128, tsteps=None):
              "forward_solve_ms": ms_fwd / S.steps, "gradient_ms": ms_grad / S.steps,
              "grad_rel_err_vs_fd": fd_err["c"], "grad_p0_rel_err_vs_fd": fd_err["p0"], "fd_eps": eps, "J": J,
              "bar": {"adjoint_over_forward_time": 3.0, "grad_rel_err_vs_fd": 1e-4},
-             "note": "value counts forward + adjoint cell-updates; roofline uses the adjoint sweep's 60 B/cell"}
+             "note": "value counts forward + adjoint cell-updates; roofline: the reverse sweep's 60 B/cell over its "
+                     "own average launch time (CUDA events around the reverse sweep inside cfdb_wave_gradient)"}
     if S.extras:
         from oracle import oracle as O
         oc = O.Mesh(n, n, n, 1 / n, 1 / n, 1 / n, dtype=np.float32)
@@ -797,7 +799,7 @@ def bench_adjoint(ctx, cfdb, dev, flush, S, n=128, tsteps=None):
                  ms_grad / S.steps,
                  {"mesh": [n] * 3, "time_steps": T, "snapshots": T, "c": "exp(0.2 g), g Gaussian random field, seed 5"},
                  60, n ** 3, T, extra, launches=grad_launches,
-                 traffic_profile="adjoint_sweep_128.txt" if n == 128 else None)
+                 traffic_profile="adjoint_sweep_128.txt" if n == 128 else None, launch_ms=st.reverse_ms / T)
 
 
 SECONDARY = {"heat": bench_heat, "wave_distorted": bench_wave_distorted, "sod": bench_sod,
