@@ -47,17 +47,20 @@ struct PlainGeomDev {
   void* stab_tmp = nullptr;    // 3 * 6n, allocated on first stab call
 };
 
-// Compact FP32 geometry of vertex meshes for the fused gather kernels: the
-// outward area vector of each cell's +x/+y/+z face (the -faces are the
-// neighbours' +faces negated), 1/V, and the area vectors of the boundary
-// faces on the -x/-y/-z walls.
+// Compact FP32 geometry of vertex meshes for the fused kernels: per cell the
+// outward area vector of its +x/+y/+z face and 1/V (10 fields), stored on
+// the lattice padded by one ghost layer below each axis (x and y) and by four
+// cells below z (so the z origin of every row stays 16-byte aligned):
+// cell (x, y, z) sits at ((x + 1) Yp + y + 1) Zp + z + 4 with Yp = ny + 1,
+// Zp = nz + 4.  The -faces of a cell are its minus neighbours' +faces
+// negated; on the -x/-y/-z walls that neighbour is a ghost entry holding the
+// wall face's outward area vector negated, so no kernel needs a wall table.
+// Ghost entries of the other fields are zero.
 struct CompactGeomDev {
   bool ready = false;
-  float* S = nullptr;      // 10n: [Sx.x|Sx.y|Sx.z|Sy.x|...|Sz.z|1/V]
-  float* inv_vol = nullptr;  // = S + 9n
-  float* wall_x = nullptr; // 3 * ny*nz  (cells x = 0, index y*nz+z)
-  float* wall_y = nullptr; // 3 * nx*nz  (cells y = 0, index x*nz+z)
-  float* wall_z = nullptr; // 3 * nx*ny  (cells z = 0, index x*ny+y)
+  float* S = nullptr;  // 10 np: [Sx.x|Sx.y|Sx.z|Sy.x|...|Sz.z|1/V] over the padded lattice
+  int64_t np = 0;      // padded entries per field: (nx + 1) Yp Zp
+  int64_t yp = 0, zp = 0;
 };
 
 struct cfdb_ctx {

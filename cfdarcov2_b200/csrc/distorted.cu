@@ -1,9 +1,10 @@
 // Fused acoustic step on vertex (distorted) meshes.  Geometry is the compact
 // FP32 form built by cfdb_mesh_need_compact: per cell the outward area
-// vectors S = n_alt A of its +x/+y/+z faces and 1/V (40 B/cell); the -faces
-// are the neighbours' +faces negated (the reference computes one normal and
-// one area per face object and gives the two cells opposite outward normals,
-// src/mesh3d.cpp:69-105), boundary -faces come from three wall tables.
+// vectors S = n_alt A of its +x/+y/+z faces and 1/V (40 B/cell) on a lattice
+// padded below each axis; the -faces are the minus neighbours' +faces negated
+// (the reference computes one normal and one area per face object and gives
+// the two cells opposite outward normals, src/mesh3d.cpp:69-105), and on the
+// -walls that neighbour is a ghost entry holding the wall face's vector.
 // Warps cover consecutive z cells, so every neighbour gather is a coalesced
 // row segment.
 #include "tma_host.hpp"
@@ -15,11 +16,8 @@ namespace {
 constexpr int kThreads = 256;
 
 struct CompactArgs {
-  const float* __restrict__ S;
-  const float* __restrict__ iv;
-  const float* __restrict__ wx;
-  const float* __restrict__ wy;
-  const float* __restrict__ wz;
+  const float* __restrict__ S;  // padded compact geometry, 10 fields of np entries
+  long long np, yp, zp;
   int X, Y, Z;
   long long n;
 };
@@ -39,6 +37,8 @@ __global__ void __launch_bounds__(kThreads)
     const float c2 = cP * cP;
     float ap = 0.f, au = 0.f, av = 0.f, aw = 0.f;
     const long long stride[3] = {yz, (long long)g.Z, 1};
+    const long long pi = ((long long)(x + 1) * g.yp + (y + 1)) * g.zp + (z + 4);  // padded geometry entry
+    const long long pstride[3] = {g.yp * g.zp, g.zp, 1};
     const int coord[3] = {x, y, z};
     const int ext[3] = {g.X, g.Y, g.Z};
 #pragma unroll
@@ -49,20 +49,14 @@ __global__ void __launch_bounds__(kThreads)
         bool wall;
         long long j;
         if (side == 1) {  // +face: own area vector
-          Sx = g.S[(3 * d + 0) * n + i]; Sy = g.S[(3 * d + 1) * n + i]; Sz = g.S[(3 * d + 2) * n + i];
+          Sx = g.S[(3 * d + 0) * g.np + pi]; Sy = g.S[(3 * d + 1) * g.np + pi]; Sz = g.S[(3 * d + 2) * g.np + pi];
           wall = coord[d] == ext[d] - 1;
           j = i + stride[d];
-        } else {          // -face: neighbour's +face negated, or the wall table
+        } else {          // -face: the minus neighbour's (or the wall ghost's) +face negated
           wall = coord[d] == 0;
           j = i - stride[d];
-          if (!wall) {
-            Sx = -g.S[(3 * d + 0) * n + j]; Sy = -g.S[(3 * d + 1) * n + j]; Sz = -g.S[(3 * d + 2) * n + j];
-          } else {
-            const float* w = d == 0 ? g.wx : (d == 1 ? g.wy : g.wz);
-            const long long cnt = d == 0 ? yz : (d == 1 ? (long long)g.X * g.Z : (long long)g.X * g.Y);
-            const long long k = d == 0 ? (long long)y * g.Z + z : (d == 1 ? (long long)x * g.Z + z : (long long)x * g.Y + y);
-            Sx = w[k]; Sy = w[cnt + k]; Sz = w[2 * cnt + k];
-          }
+          const long long pj = pi - pstride[d];
+          Sx = -g.S[(3 * d + 0) * g.np + pj]; Sy = -g.S[(3 * d + 1) * g.np + pj]; Sz = -g.S[(3 * d + 2) * g.np + pj];
         }
         const float A = sqrtf(Sx * Sx + Sy * Sy + Sz * Sz);
         const float unPA = uP * Sx + vP * Sy + wP * Sz;
@@ -84,7 +78,7 @@ __global__ void __launch_bounds__(kThreads)
         aw += pm * Sz - hA * (wN - wP);
       }
     }
-    const float s = -dt * g.iv[i];
+    const float s = -dt * g.S[9 * g.np + pi];
     qn[i] = pP + s * ap;
     qn[n + i] = uP + s * au;
     qn[2 * n + i] = vP + s * av;
@@ -92,12 +86,28 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-// Sweep form (uniform-lattice topology, any vertex positions): the state
-// (p,u,v,w) is swept, the compact geometry [Sx|Sy|Sz|1/V] (10 fields) is
-// staged as auxiliary data with the same halos, so the -face area vector of a
-// cell is its staged neighbour's +face vector.  -wall faces read the wall
-// tables.  Same flux as compact_wave_k.
-struct DistPhys {
+// Face-flux form (face_sweep.cuh): the flux through a face is evaluated once
+// and enters the two cells it separates with opposite signs.  The face with
+// normal e_d between L (minus side) and R carries L's +d area vector S, and
+//   F = ( c^2/2 (u_L + u_R).S - c|S|/2 (p_R - p_L),
+//         (p_L + p_R)/2 S     - c|S|/2 (u_R - u_L) )
+// is what the gather form adds to L (and subtracts from R): the same terms as
+// compact_wave_k per face (constant c, where both speed modes agree), summed
+// as F(+d) - F(-d) per direction.  A wall face reflects the cell's velocity
+// about the face normal (the cell's own +d vector, or on a -wall the ghost
+// entry's vector, which is the wall face's outward vector negated).
+struct DistFacePhys {
+  static constexpr int NF = 4;
+  static constexpr int NG = 10;  // [S+x | S+y | S+z | 1/V]
+  static constexpr int NGF = 3;
+  static constexpr int ND = 0;
+  // the reflection costs a division: evaluate wall faces behind a branch
+  static constexpr bool SELECT_WALLS = false;
+  static constexpr int MIN_BLOCKS = 2;
+  struct Params {
+    float dt, c2h, hc;  // dt, c^2/2, c/2
+  };
+  struct Acc {};
   // |S| of a face: the PTX approximate square root (relative error ~2^-22,
   // far inside the FP32 path's 1e-5 bar) instead of the IEEE sequence
   __device__ static float fast_sqrt(float x) {
@@ -105,76 +115,33 @@ struct DistPhys {
     asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
     return r;
   }
-  static constexpr int NF = 4;
-  static constexpr int NA = 10;
-  static constexpr bool HAS_C = false;
-  static constexpr int FT = 14;
-  static constexpr int MIN_BLOCKS = 3;
-  struct Params {
-    float dt, c;
-    int mode;
-    int X, Y, Z;
-    const float* wx;
-    const float* wy;
-    const float* wz;
-  };
-  struct Acc {};
   __device__ static bool begin(Params&) { return true; }
-  __device__ static void ghost(float g[FT], const float p[FT], int) {
-#pragma unroll
-    for (int f = 0; f < FT; ++f) g[f] = p[f];
+  __device__ static void flux(const float L[NF], const float*, const float R[NF], const float*, const float S[NGF],
+                              int, const Params& a, float F[NF]) {
+    const float A = fast_sqrt(S[0] * S[0] + S[1] * S[1] + S[2] * S[2]);
+    const float unL = L[1] * S[0] + L[2] * S[1] + L[3] * S[2];
+    const float unR = R[1] * S[0] + R[2] * S[1] + R[3] * S[2];
+    const float hA = a.hc * A;
+    const float pm = 0.5f * (L[0] + R[0]);
+    F[0] = a.c2h * (unL + unR) - hA * (R[0] - L[0]);
+    F[1] = pm * S[0] - hA * (R[1] - L[1]);
+    F[2] = pm * S[1] - hA * (R[2] - L[2]);
+    F[3] = pm * S[2] - hA * (R[3] - L[3]);
   }
-  __device__ static void cell(const stencil::CellIn<FT>& in, const Params& a, float o[NF]) {
-    const float* P = in.P;
-    const float pP = P[0], uP = P[1], vP = P[2], wP = P[3];
-    const float cP = a.c, c2 = cP * cP;
-    float ap = 0.f, au = 0.f, av = 0.f, aw = 0.f;
+  // The cell beyond a wall face with area vector S: the cell with its
+  // velocity reflected about the face normal.
+  __device__ static void ghost(const float C[NF], const float*, const float S[NGF], int, float g[NF], float*) {
+    const float k2 = 2.f * (C[1] * S[0] + C[2] * S[1] + C[3] * S[2]) / (S[0] * S[0] + S[1] * S[1] + S[2] * S[2]);
+    g[0] = C[0];
+    g[1] = C[1] - k2 * S[0];
+    g[2] = C[2] - k2 * S[1];
+    g[3] = C[3] - k2 * S[2];
+  }
+  __device__ static void update(const float C[NF], const float*, const float G[NG], const float dF[3][NF],
+                                const Params& a, float o[NF]) {
+    const float s = -a.dt * G[9];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-#pragma unroll
-      for (int side = 0; side < 2; ++side) {
-        const int k = 2 * d + side;
-        const bool wall = (in.walls >> k) & 1;
-        float Sx, Sy, Sz;
-        if (side) {
-          Sx = P[4 + 3 * d]; Sy = P[5 + 3 * d]; Sz = P[6 + 3 * d];
-        } else if (!wall) {
-          const float* N = in.nb[k];
-          Sx = -N[4 + 3 * d]; Sy = -N[5 + 3 * d]; Sz = -N[6 + 3 * d];
-        } else {
-          const long long yz = (long long)a.Y * a.Z;
-          const int x = int(in.idx / yz);
-          const int r = int(in.idx - (long long)x * yz);
-          const int y = r / a.Z, z = r - (r / a.Z) * a.Z;
-          const float* w = d == 0 ? a.wx : (d == 1 ? a.wy : a.wz);
-          const long long cnt = d == 0 ? yz : (d == 1 ? (long long)a.X * a.Z : (long long)a.X * a.Y);
-          const long long kk = d == 0 ? (long long)y * a.Z + z : (d == 1 ? (long long)x * a.Z + z : (long long)x * a.Y + y);
-          Sx = w[kk]; Sy = w[cnt + kk]; Sz = w[2 * cnt + kk];
-        }
-        const float A = fast_sqrt(Sx * Sx + Sy * Sy + Sz * Sz);
-        const float unPA = uP * Sx + vP * Sy + wP * Sz;
-        float pN, uN, vN, wN;
-        if (!wall) {
-          const float* N = in.nb[k];
-          pN = N[0]; uN = N[1]; vN = N[2]; wN = N[3];
-        } else {
-          const float k2 = 2.f * unPA / (A * A);
-          pN = pP; uN = uP - k2 * Sx; vN = vP - k2 * Sy; wN = wP - k2 * Sz;
-        }
-        const float unNA = uN * Sx + vN * Sy + wN * Sz;
-        const float hA = 0.5f * cP * A;
-        const float pm = 0.5f * (pP + pN);
-        ap += c2 * 0.5f * (unPA + unNA) - hA * (pN - pP);
-        au += pm * Sx - hA * (uN - uP);
-        av += pm * Sy - hA * (vN - vP);
-        aw += pm * Sz - hA * (wN - wP);
-      }
-    }
-    const float s = -a.dt * P[13];
-    o[0] = pP + s * ap;
-    o[1] = uP + s * au;
-    o[2] = vP + s * av;
-    o[3] = wP + s * aw;
+    for (int f = 0; f < NF; ++f) o[f] = C[f] + s * (dF[0][f] + dF[1][f] + dF[2][f]);
   }
   __device__ static void acc_init(Acc&) {}
   __device__ static void acc_cell(Acc&, const float*, const Params&) {}
@@ -190,10 +157,15 @@ int compact_wave_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* q, voi
   if (int rc = cfdb_mesh_need_compact(m)) return rc;
   const CompactGeomDev& cg = m->compact;
   if (!c && m->nz % 4 == 0 && !(reinterpret_cast<uintptr_t>(q) & 15u) && !(reinterpret_cast<uintptr_t>(qn) & 15u)) {
-    DistPhys::Params p{float(dt), float(cconst), mode, int(m->nx), int(m->ny), int(m->nz), cg.wall_x, cg.wall_y, cg.wall_z};
-    return stencil::launch_sweep<DistPhys, 32, 8, 3, 1>(ctx, m, q, cg.S, nullptr, qn, p, 0);
+    const float cs = float(cconst);
+    const DistFacePhys::Params p{float(dt), 0.5f * cs * cs, 0.5f * cs};
+    const stencil::PaddedGeom pg{cg.S, cg.zp, cg.yp, m->nx + 1, cg.np};
+    // 64-wide z tiles (two cells per thread) unless 32-wide ones pad the z rows less
+    const int64_t pad64 = (m->nz + 63) / 64 * 64 - m->nz, pad32 = (m->nz + 31) / 32 * 32 - m->nz;
+    if (m->nz > 32 && pad64 <= pad32) return stencil::launch_face_sweep<DistFacePhys, 64, 8, 3, 2>(ctx, m, q, pg, qn, p, 0);
+    return stencil::launch_face_sweep<DistFacePhys, 32, 8, 3, 1>(ctx, m, q, pg, qn, p, 0);
   }
-  CompactArgs a{cg.S, cg.inv_vol, cg.wall_x, cg.wall_y, cg.wall_z, int(m->nx), int(m->ny), int(m->nz), (long long)m->n};
+  CompactArgs a{cg.S, cg.np, cg.yp, cg.zp, int(m->nx), int(m->ny), int(m->nz), (long long)m->n};
   compact_wave_k<<<grid_for(ctx, m->n, kThreads, 8), kThreads, 0, ctx->stream>>>(
       a, static_cast<const float*>(q), static_cast<float*>(qn), static_cast<const float*>(c), float(cconst), mode,
       float(dt));

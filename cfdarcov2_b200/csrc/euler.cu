@@ -1,5 +1,5 @@
 // Compressible Euler solver object (cfdb_euler_*) and its fused FP32 step:
-// one TMA sweep per step (tma_stencil.cuh) that reads the device clock, does
+// one face-flux TMA sweep per step (face_sweep.cuh) that reads the device clock, does
 // the Rusanov update of all five conserved fields in one HBM pass and, in its
 // epilogue, reduces the new state's per-direction signal speeds (for the next
 // dt) and its FP64 Neumaier totals.  The plain path lives in euler_plain.cu.
@@ -23,8 +23,6 @@ __device__ __forceinline__ void comp_add(double& s, double& c, double x) {
 
 struct EulerPhys {
   static constexpr int NF = 5;
-  static constexpr int NA = 0;
-  static constexpr bool HAS_C = false;
   static constexpr int MIN_BLOCKS = 2;  // 64x8 tile, 2 cells per thread: 256 threads at <= 128 registers
   struct Params {
     float ih[3];
@@ -71,12 +69,6 @@ struct EulerPhys {
     return true;
   }
 
-  // zero-gradient at the x ends, reflective walls in y and z
-  __device__ static void ghost(float g[NF], const float q[NF], int dir) {
-#pragma unroll
-    for (int f = 0; f < NF; ++f) g[f] = q[f];
-    if (dir != 0) g[1 + dir] = -q[1 + dir];
-  }
 
   // 1/rho and the sound speed with the approximate reciprocal and square
   // root of the SFU (relative error ~1e-7, far inside the FP32 solver's
@@ -97,8 +89,10 @@ struct EulerPhys {
 
   // Derived per cell, computed once per cell and plane by the sweep:
   // d = (1/rho, p, a).  A reflective or zero-gradient ghost has the same
-  // values as its cell, but the sweep derives ghosts itself anyway.
+  // values as its cell (ghost() copies them).
   static constexpr int ND = 3;
+  static constexpr int NG = 0;   // uniform mesh: no per-cell geometry
+  static constexpr int NGF = 0;
   __device__ static void derive(const float q[NF], float d[ND], const Params& a) {
     float u[3];
     prim(q, a.gamma - 1.0f, a.gamma, d[0], u, d[1], d[2]);
@@ -108,12 +102,11 @@ struct EulerPhys {
   //   F = (F_L + F_R)/2 . e_d - lambda/2 (U_R - U_L),  lambda = max(|u_d| + a)
   // regrouped per conserved component U as U_L (u_L/2 + l) + U_R (u_R/2 - l)
   // with l = lambda/2 (two instructions per component), the pressure terms
-  // added to the momentum and energy components.  Each face is evaluated
-  // once by the sweep (FACE_FLUX) and enters the two cells it separates with
-  // opposite signs.
-  static constexpr bool FACE_FLUX = true;
-  __device__ static void flux(const float L[NF], const float Ld[ND], const float R[NF], const float Rd[ND], int d,
-                              const Params&, float F[NF]) {
+  // added to the momentum and energy components.  The sweep evaluates each
+  // face once and enters it into the two cells it separates with opposite
+  // signs.
+  __device__ static void flux(const float L[NF], const float Ld[ND], const float R[NF], const float Rd[ND],
+                              const float*, int d, const Params&, float F[NF]) {
     const float uL = L[1 + d] * Ld[0], uR = R[1 + d] * Rd[0];
     const float pL = Ld[1], pR = Rd[1];
     const float l = 0.5f * fmaxf(fabsf(uL) + Ld[2], fabsf(uR) + Rd[2]);
@@ -123,8 +116,22 @@ struct EulerPhys {
     F[1 + d] += 0.5f * (pL + pR);
     F[4] += 0.5f * (pL * uL + pR * uR);
   }
-  __device__ static void update(const float P[NF], const float[ND], const float dF[3][NF], long long,
-                                const Params& a, float o[NF]) {
+  // Walls: a face on the domain boundary is evaluated against a ghost cell,
+  // which the sweep builds for every face that can be a wall and selects
+  // (SELECT_WALLS: a few selects, no branch around the flux).  Zero-gradient
+  // at the x ends (a copy), reflective in y and z (the wall-normal momentum
+  // negated); 1/rho, p and a are the cell's own.
+  static constexpr bool SELECT_WALLS = true;
+  __device__ static void ghost(const float C[NF], const float Cd[ND], const float*, int d, float g[NF], float gd[ND]) {
+#pragma unroll
+    for (int f = 0; f < NF; ++f) g[f] = C[f];
+    if (d == 1) g[2] = -C[2];
+    if (d == 2) g[3] = -C[3];
+#pragma unroll
+    for (int e = 0; e < ND; ++e) gd[e] = Cd[e];
+  }
+  __device__ static void update(const float P[NF], const float*, const float*, const float dF[3][NF], const Params& a,
+                                float o[NF]) {
 #pragma unroll
     for (int c = 0; c < NF; ++c) o[c] = P[c] - (a.kd[0] * dF[0][c] + (a.kd[1] * dF[1][c] + a.kd[2] * dF[2][c]));
   }
@@ -243,7 +250,8 @@ int launch_euler(cfdb_euler* e, const void* U, void* Un, int64_t s) {
   p.clock = e->clock; p.totals = e->totals; p.part = e->part;
   p.s = (long long)s;
   p.max_steps = (long long)e->max_steps;
-  return stencil::launch_sweep<EulerPhys, TZ, 8, 4, kEulerVZ>(e->ctx, m, U, nullptr, nullptr, Un, p, kEulerCtasPerSm);
+  const stencil::PaddedGeom none{nullptr, 0, 0, 0, 0};
+  return stencil::launch_face_sweep<EulerPhys, TZ, 8, 4, kEulerVZ>(e->ctx, m, U, none, Un, p, kEulerCtasPerSm);
 }
 
 int tz_for(const cfdb_mesh* m) { return m->nz >= 64 ? 64 : 32; }

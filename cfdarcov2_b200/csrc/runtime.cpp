@@ -461,9 +461,7 @@ extern "C" int cfdb_mesh_destroy(cfdb_mesh* m) {
     free_plain(m->ctx, m->plain[0]);
     free_plain(m->ctx, m->plain[1]);
     cfdb_dev_free(m->ctx, m->d_ids);
-    CompactGeomDev& c = m->compact;
-    float** ptrs[] = {&c.S, &c.wall_x, &c.wall_y, &c.wall_z};  // inv_vol lives inside S's allocation
-    for (float** q : ptrs) cfdb_dev_free(m->ctx, *q);
+    cfdb_dev_free(m->ctx, m->compact.S);
   }
   delete m;
   return CFDB_OK;
@@ -588,42 +586,34 @@ int cfdb_mesh_need_compact(cfdb_mesh* m) {
   if (int rc = cfdb_mesh_need_host_geom(m)) return rc;
   const HostGeom& g = *m->geom;
   const int64_t n = m->n, nx = m->nx, ny = m->ny, nz = m->nz;
-  std::vector<double> S(static_cast<size_t>(9 * n)), iv(static_cast<size_t>(n));
-  std::vector<double> wx(static_cast<size_t>(3 * ny * nz)), wy(static_cast<size_t>(3 * nx * nz));
-  std::vector<double> wz(static_cast<size_t>(3 * nx * ny));
-  // +x face = slot 5, +y = slot 3, +z = slot 1; wall -x = 4, -y = 2, -z = 0
+  const int64_t yp = ny + 1, zp = nz + 4, np = (nx + 1) * yp * zp;
+  auto pidx = [&](int64_t x, int64_t y, int64_t z) { return ((x + 1) * yp + (y + 1)) * zp + (z + 4); };
+  std::vector<double> G(static_cast<size_t>(10 * np), 0.0);
+  // face slots: +x = 5, +y = 3, +z = 1; -x = 4, -y = 2, -z = 0
+  auto face = [&](int slot, int64_t i, int c3) {
+    const int64_t k6 = int64_t(slot) * n + i;
+    return g.normal_alt[c3 * 6 * n + k6] * g.area[k6];
+  };
   const int plus_slot[3] = {5, 3, 1};
-  for (int64_t i = 0; i < n; ++i) {
-    for (int d = 0; d < 3; ++d) {
-      const int64_t k6 = int64_t(plus_slot[d]) * n + i;
-      for (int c3 = 0; c3 < 3; ++c3) S[(3 * d + c3) * n + i] = g.normal_alt[c3 * 6 * n + k6] * g.area[k6];
-    }
-    iv[i] = 1.0 / g.volume[i];
-  }
-  for (int64_t y = 0; y < ny; ++y)
-    for (int64_t z = 0; z < nz; ++z) {
-      const int64_t i = nz * y + z, k6 = 4 * n + i;
-      for (int c3 = 0; c3 < 3; ++c3) wx[c3 * ny * nz + (y * nz + z)] = g.normal_alt[c3 * 6 * n + k6] * g.area[k6];
-    }
   for (int64_t x = 0; x < nx; ++x)
-    for (int64_t z = 0; z < nz; ++z) {
-      const int64_t i = nz * ny * x + z, k6 = 2 * n + i;
-      for (int c3 = 0; c3 < 3; ++c3) wy[c3 * nx * nz + (x * nz + z)] = g.normal_alt[c3 * 6 * n + k6] * g.area[k6];
-    }
-  for (int64_t x = 0; x < nx; ++x)
-    for (int64_t y = 0; y < ny; ++y) {
-      const int64_t i = nz * ny * x + nz * y, k6 = 0 * n + i;
-      for (int c3 = 0; c3 < 3; ++c3) wz[c3 * nx * ny + (x * ny + y)] = g.normal_alt[c3 * 6 * n + k6] * g.area[k6];
-    }
-  cfdb_ctx* ctx = m->ctx;
-  // one allocation [S (9n) | 1/V (n)]: the fused sweep stages it as 10 fields
-  S.insert(S.end(), iv.begin(), iv.end());
-  int rc = upload_as<float>(ctx, S.data(), int64_t(S.size()), reinterpret_cast<void**>(&c.S));
-  if (!rc) c.inv_vol = c.S + 9 * n;
-  if (!rc) rc = upload_as<float>(ctx, wx.data(), int64_t(wx.size()), reinterpret_cast<void**>(&c.wall_x));
-  if (!rc) rc = upload_as<float>(ctx, wy.data(), int64_t(wy.size()), reinterpret_cast<void**>(&c.wall_y));
-  if (!rc) rc = upload_as<float>(ctx, wz.data(), int64_t(wz.size()), reinterpret_cast<void**>(&c.wall_z));
+    for (int64_t y = 0; y < ny; ++y)
+      for (int64_t z = 0; z < nz; ++z) {
+        const int64_t i = (x * ny + y) * nz + z, pi = pidx(x, y, z);
+        for (int d = 0; d < 3; ++d)
+          for (int c3 = 0; c3 < 3; ++c3) G[(3 * d + c3) * np + pi] = face(plus_slot[d], i, c3);
+        G[9 * np + pi] = 1.0 / g.volume[i];
+        // ghost neighbours below the walls: the wall face's outward vector negated
+        for (int c3 = 0; c3 < 3; ++c3) {
+          if (x == 0) G[(0 + c3) * np + pidx(-1, y, z)] = -face(4, i, c3);
+          if (y == 0) G[(3 + c3) * np + pidx(x, -1, z)] = -face(2, i, c3);
+          if (z == 0) G[(6 + c3) * np + pidx(x, y, -1)] = -face(0, i, c3);
+        }
+      }
+  int rc = upload_as<float>(m->ctx, G.data(), int64_t(G.size()), reinterpret_cast<void**>(&c.S));
   if (rc) return rc;
+  c.np = np;
+  c.yp = yp;
+  c.zp = zp;
   c.ready = true;
   return CFDB_OK;
 }

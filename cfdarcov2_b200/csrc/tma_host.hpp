@@ -97,7 +97,7 @@ inline SweepShape sweep_shape(const cfdb_ctx* ctx, const cfdb_mesh* m, int tz, i
 template <class Phys, int TZ, int TY, int S, int VZ = 4>
 int launch_sweep(cfdb_ctx* ctx, const cfdb_mesh* m, const void* q, const void* aux, const void* c, void* out,
                  const typename Phys::Params& prm, int ctas_per_sm, int* launched_grid = nullptr) {
-  using L = Layout<TZ, TY, S, Phys::NF, Phys::NA, Phys::HAS_C, VZ, derived_count<Phys>::value>;
+  using L = Layout<TZ, TY, S, Phys::NF, Phys::NA, Phys::HAS_C, VZ>;
   static_assert(TZ % VZ == 0 && (VZ == 1 || VZ == 2 || VZ == 4), "bad vector width");
   CUtensorMap tq, ta, tc;
   if (int rc = encode_state(ctx, &tq, q, m, Phys::NF, TZ, TY)) return rc;
@@ -138,6 +138,78 @@ int launch_sweep(cfdb_ctx* ctx, const cfdb_mesh* m, const void* q, const void* a
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   CFDB_CUDA(ctx, cudaLaunchKernelEx(&cfg, kern, tq, ta, tc, g, static_cast<float*>(out), prm, ctx->d_error));
+  ++ctx->launches;
+  if (launched_grid) *launched_grid = sh.tiles * sh.chunks;
+  return CFDB_OK;
+}
+
+}  // namespace stencil
+
+#include "face_sweep.cuh"
+
+namespace stencil {
+
+// 4-D map over nf float32 fields stored field after field on a (zp, yp, xp)
+// lattice of np entries per field, box (bz, by, 1, nf): one plane and all
+// fields per copy.
+inline int encode_box(cfdb_ctx* ctx, CUtensorMap* map, const void* base, int64_t zp, int64_t yp, int64_t xp,
+                      int64_t np, int nf, int bz, int by) {
+  auto fn = encode_fn();
+  if (!fn) return cfdb_fail(ctx, CFDB_ECUDA, "cuTensorMapEncodeTiled entry point unavailable");
+  cuuint64_t dims[4] = {cuuint64_t(zp), cuuint64_t(yp), cuuint64_t(xp), cuuint64_t(nf)};
+  cuuint64_t strides[3] = {cuuint64_t(zp) * 4, cuuint64_t(zp * yp) * 4, cuuint64_t(np) * 4};
+  cuuint32_t box[4] = {cuuint32_t(bz), cuuint32_t(by), 1, cuuint32_t(nf)};
+  cuuint32_t es[4] = {1, 1, 1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<void*>(base), dims, strides, box, es,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return cfdb_fail(ctx, CFDB_ECUDA, "cuTensorMapEncodeTiled (box) failed with %d", int(r));
+  return CFDB_OK;
+}
+
+// Launches one face-flux sweep (face_sweep.cuh): q holds the NF state
+// fields, pg the NG per-cell geometry fields on the padded lattice (unused
+// when NG == 0), out receives the NF new state fields.  Grid and launch as
+// launch_sweep.
+template <class Phys, int TZ, int TY, int S, int VZ>
+int launch_face_sweep(cfdb_ctx* ctx, const cfdb_mesh* m, const void* q, const PaddedGeom& pg, void* out,
+                      const typename Phys::Params& prm, int ctas_per_sm, int* launched_grid = nullptr) {
+  using L = FaceLayout<TZ, TY, S, Phys::NF, Phys::NG, Phys::ND, VZ>;
+  static_assert(TZ % VZ == 0 && (VZ == 1 || VZ == 2 || VZ == 4), "bad vector width");
+  static_assert(TZ % 4 == 0, "z tiles must keep 16-byte aligned origins");
+  CUtensorMap tq, tg;
+  if (int rc = encode_box(ctx, &tq, q, m->nz, m->ny, m->nx, m->n, Phys::NF, TZ + 8, TY + 2)) return rc;
+  tg = tq;
+  if constexpr (Phys::NG > 0) {
+    if (pg.zp != m->nz + 4 || pg.yp != m->ny + 1 || pg.xp != m->nx + 1 || pg.np != pg.zp * pg.yp * pg.xp ||
+        (reinterpret_cast<uintptr_t>(pg.base) & 15u))
+      return cfdb_fail(ctx, CFDB_EINVAL, "face sweep: geometry is not on the padded lattice of the mesh");
+    if (int rc = encode_box(ctx, &tg, pg.base, pg.zp, pg.yp, pg.xp, pg.np, Phys::NG, TZ + 4, TY + 1)) return rc;
+  }
+  auto kern = face_sweep_kernel<Phys, TZ, TY, S, VZ>;
+  static std::atomic<int> resident_of[kMaxDevices] = {};
+  if (ctx->device < 0 || ctx->device >= kMaxDevices)
+    return cfdb_fail(ctx, CFDB_EUNSUPPORTED, "device ordinal %d beyond %d", ctx->device, kMaxDevices);
+  int resident = resident_of[ctx->device].load(std::memory_order_acquire);
+  if (!resident) {
+    CFDB_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L::SMEM_BYTES)));
+    CFDB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kern, L::THREADS, L::SMEM_BYTES));
+    if (resident < 1) return cfdb_fail(ctx, CFDB_EUNSUPPORTED, "face sweep kernel does not fit on an SM");
+    resident_of[ctx->device].store(resident, std::memory_order_release);
+  }
+  const SweepShape sh = sweep_shape(ctx, m, TZ, TY, ctas_per_sm > 0 ? std::min(ctas_per_sm, resident) : resident);
+  Geometry g{int(m->nx), int(m->ny), int(m->nz), sh.chunks, (long long)m->n, ctx->wait_cycles, ctx->missing_plane};
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(sh.tiles, sh.chunks);
+  cfg.blockDim = dim3(L::THREADS);
+  cfg.dynamicSmemBytes = L::SMEM_BYTES;
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  CFDB_CUDA(ctx, cudaLaunchKernelEx(&cfg, kern, tq, tg, g, static_cast<float*>(out), prm, ctx->d_error));
   ++ctx->launches;
   if (launched_grid) *launched_grid = sh.tiles * sh.chunks;
   return CFDB_OK;

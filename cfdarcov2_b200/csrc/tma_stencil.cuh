@@ -129,14 +129,11 @@ struct Geometry {
 // The FT staged fields are the NF state fields (read from `q`, written to
 // `out`), then NA auxiliary fields (read from `aux`), then the coefficient
 // field c when HAS_C.  Neighbours beyond a wall hold Phys::ghost(P, dir);
-// bit 2*dir + side of `walls` marks them.  With ND > 0 derived values per
-// cell (Phys::derive of the staged fields, e.g. 1/rho, p, a) come along in
-// Pd / nbd, each computed once per cell and plane instead of once per use.
-template <int FT, int ND = 0> struct CellIn {
+// bit 2*dir + side of `walls` marks them.  (Conservative schemes that
+// evaluate each face once run on the face sweep, face_sweep.cuh.)
+template <int FT> struct CellIn {
   float P[FT];
   float nb[6][FT];
-  float Pd[ND > 0 ? ND : 1];
-  float nbd[6][ND > 0 ? ND : 1];
   int walls;
   long long idx;  // cell id
   float pre;      // Phys::pre_ptr(params)[idx], loaded one plane ahead (physics with HAS_PRE)
@@ -149,15 +146,6 @@ template <int FT, int ND = 0> struct CellIn {
 template <class P, class = void> struct has_pre { static constexpr bool value = false; };
 template <class P> struct has_pre<P, decltype(void(P::HAS_PRE))> { static constexpr bool value = P::HAS_PRE; };
 
-// Number of derived values a physics declares (Phys::ND), 0 when it has none.
-template <class P, class = void> struct derived_count { static constexpr int value = 0; };
-template <class P> struct derived_count<P, decltype(void(P::ND))> { static constexpr int value = P::ND; };
-// Face-flux physics (Phys::FACE_FLUX): the sweep evaluates each x face once
-// (the flux through a cell's +x face is carried in registers to the next
-// plane as its neighbour's -x flux) and each z face between a thread's own
-// cells once, instead of two one-sided evaluations per face.
-template <class P, class = void> struct is_face_flux { static constexpr bool value = false; };
-template <class P> struct is_face_flux<P, decltype(void(P::FACE_FLUX))> { static constexpr bool value = P::FACE_FLUX; };
 // Paired physics (Phys::PAIRED): with two cells per thread (VZ == 2) the sweep
 // calls Phys::cell2(in0, in1, params, o0, o1) once instead of cell() twice, so
 // the physics can advance both cells with packed FP32 pairs (f32x2.cuh).
@@ -173,18 +161,10 @@ template <class P> struct is_paired<P, decltype(void(P::PAIRED))> { static const
 //   __device__ static bool begin(Params&)  -> false: skip the sweep (e.g. a finished clock); may
 //        fill per-launch values (a device-side dt) into its copy of the parameters
 //   __device__ static void ghost(float g[FT], const float p[FT], int dir);   dir 0=x,1=y,2=z
-//   __device__ static void cell(const CellIn<FT, ND>&, const Params&, float out[NF]);
+//   __device__ static void cell(const CellIn<FT>&, const Params&, float out[NF]);
 //   __device__ static void acc_init(Acc&), acc_cell(Acc&, const float out[NF], const Params&)
 //   __device__ static void finish(Acc&, const Params&, bool thread_active)   (called by all threads)
-// and optionally
-//   static constexpr int ND;            derived values per cell
-//   __device__ static void derive(const float q[FT], float d[ND], const Params&);
-// A face-flux physics (FACE_FLUX = true) replaces cell() by
-//   __device__ static void flux(const float L[FT], const float Ld[ND], const float R[FT], const float Rd[ND],
-//                               int dir, const Params&, float F[NF]);      flux along +e_dir from L to R
-//   __device__ static void update(const float P[FT], const float Pd[ND], const float dF[3][NF],
-//                                 long long idx, const Params&, float out[NF]);   dF[d] = F(d+) - F(d-)
-template <int TZ, int TY, int S, int NF, int NA, bool HAS_C, int VZ, int ND = 0> struct Layout {
+template <int TZ, int TY, int S, int NF, int NA, bool HAS_C, int VZ> struct Layout {
   static constexpr int FT = NF + NA + (HAS_C ? 1 : 0);  // staged fields
   static constexpr int RL = TZ + 8;                       // row length (floats)
   static constexpr int RR = TY + 2;                       // rows
@@ -193,9 +173,7 @@ template <int TZ, int TY, int S, int NF, int NA, bool HAS_C, int VZ, int ND = 0>
   static constexpr int C_OFF = (A_OFF + NA * TILE + 31) / 32 * 32;      // 128-byte aligned
   static constexpr int SLOT = (C_OFF + (HAS_C ? TILE : 0) + 31) / 32 * 32;
   static constexpr uint32_t TX_BYTES = uint32_t(4 * TILE * FT);
-  // two buffers of derived values (same tile layout) after the ring
-  static constexpr int DSLOT = (ND * TILE + 31) / 32 * 32;
-  static constexpr size_t SMEM_BYTES = (size_t(S) * SLOT + 2 * size_t(DSLOT)) * 4;
+  static constexpr size_t SMEM_BYTES = size_t(S) * SLOT * 4;
   static constexpr int THREADS = (TZ / VZ) * TY;
   __host__ __device__ static constexpr int off(int f) {
     return f < NF ? f * TILE : (f < NF + NA ? A_OFF + (f - NF) * TILE : C_OFF);
@@ -227,12 +205,9 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
                  typename Phys::Params prm, int* __restrict__ err) {
   constexpr int NF = Phys::NF;
   constexpr int NA = Phys::NA;
-  constexpr int ND = derived_count<Phys>::value;
-  constexpr int NDA = ND > 0 ? ND : 1;  // array extent
-  constexpr bool FF = is_face_flux<Phys>::value;
   constexpr bool PRE = has_pre<Phys>::value;
   constexpr bool PAIR = is_paired<Phys>::value && VZ == 2;
-  using L = Layout<TZ, TY, S, NF, NA, Phys::HAS_C, VZ, ND>;
+  using L = Layout<TZ, TY, S, NF, NA, Phys::HAS_C, VZ>;
   constexpr int FT = L::FT;
   // Indexing the extern array directly keeps the accesses in the shared
   // address space (LDS, not generic loads); its start must be 128-byte aligned
@@ -260,7 +235,7 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
     return;
   }
   {
-    // the launch must provide the layout's dynamic shared memory (ring + derived buffers)
+    // the launch must provide the layout's dynamic shared memory (the ring)
     uint32_t dyn;
     asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
     if (dyn < L::SMEM_BYTES) {
@@ -341,57 +316,7 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
     }
   };
 
-  // Derived values (ND > 0): own cells in registers next to the staged ones;
-  // for the y/z neighbours, each plane's values go to one of two shared
-  // buffers (own cells by their owner, the one-cell tile-edge halo by the
-  // edge threads), written while the previous plane is being computed and
-  // read after the plane's closing __syncthreads.
-  float* const dsm = smem + S * L::SLOT;
-  auto derive_one = [&](const float q[FT], float d[NDA]) {
-    if constexpr (ND > 0) Phys::derive(q, d, P);
-  };
-  auto derive_v = [&](const float v[FT][VZ], float d[NDA][VZ]) {
-    if constexpr (ND > 0) {
-#pragma unroll
-      for (int j = 0; j < VZ; ++j) {
-        float q[FT], t[NDA];
-#pragma unroll
-        for (int f = 0; f < FT; ++f) q[f] = v[f][j];
-        derive_one(q, t);
-#pragma unroll
-        for (int e = 0; e < ND; ++e) d[e][j] = t[e];
-      }
-    }
-  };
-  auto publish = [&](int k, const float d[NDA][VZ]) {  // derived values of plane k for the neighbours
-    if constexpr (ND > 0) {
-      float* b = dsm + (k & 1) * L::DSLOT;
-#pragma unroll
-      for (int e = 0; e < ND; ++e) stv<VZ>(b + e * L::TILE + ctr, d[e]);
-      const float* base = smem + (k % S) * L::SLOT;
-      auto halo = [&](int o) {
-        float q[FT], t[NDA];
-#pragma unroll
-        for (int f = 0; f < FT; ++f) q[f] = base[L::off(f) + o];
-        derive_one(q, t);
-#pragma unroll
-        for (int e = 0; e < ND; ++e) b[e * L::TILE + o] = t[e];
-      };
-      // the 2 TZ + 2 TY halo cells, one per thread (threads 0, 1, ...)
-      constexpr int H = 2 * TZ + 2 * TY;
-      for (int h = int(threadIdx.x); h < H; h += L::THREADS) {
-        int row, z;  // tile row (-1 .. TY) and z offset (-1 .. TZ)
-        if (h < TZ) { row = -1; z = h; }
-        else if (h < 2 * TZ) { row = TY; z = h - TZ; }
-        else if (h < 2 * TZ + TY) { row = h - 2 * TZ; z = -1; }
-        else { row = h - 2 * TZ - TY; z = TZ; }
-        halo((row + 1) * L::RL + 4 + z);
-      }
-    }
-  };
-
   float prv[FT][VZ], cur[FT][VZ], nxt[FT][VZ];
-  float prvD[NDA][VZ], curD[NDA][VZ], nxtD[NDA][VZ];
   if (x0 > 0) {
     wait_plane(0);
     load_center(0, prv);
@@ -399,28 +324,6 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
   wait_plane(1);
   load_center(1, cur);
   if (x0 == 0) ghostv(prv, cur, 0);
-  derive_v(prv, prvD);
-  derive_v(cur, curD);
-  publish(1, curD);
-  // face-flux mode: flux through the -x face of the first plane's cells
-  float fxm[NF][VZ];
-  auto cell_of = [&](const float v[FT][VZ], const float d[NDA][VZ], int j, float q[FT], float qd[NDA]) {
-#pragma unroll
-    for (int f = 0; f < FT; ++f) q[f] = v[f][j];
-#pragma unroll
-    for (int e = 0; e < NDA; ++e) qd[e] = d[e][j];
-  };
-  if constexpr (FF) {
-#pragma unroll
-    for (int j = 0; j < VZ; ++j) {
-      float a[FT], ad[NDA], b[FT], bd[NDA], F[NF];
-      cell_of(prv, prvD, j, a, ad);
-      cell_of(cur, curD, j, b, bd);
-      Phys::flux(a, ad, b, bd, 0, P, F);
-#pragma unroll
-      for (int f = 0; f < NF; ++f) fxm[f][j] = F[f];
-    }
-  }
   __syncthreads();
   if (threadIdx.x == 0) {
     fence_proxy_async();
@@ -446,11 +349,8 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
     if (x + 1 < g.X) {
       wait_plane(k + 1);
       load_center(k + 1, nxt);
-      derive_v(nxt, nxtD);
-      publish(k + 1, nxtD);
     } else {
       ghostv(nxt, cur, 0);
-      derive_v(nxt, nxtD);
     }
     if (active) {
       const float* base = smem + (k % S) * L::SLOT;
@@ -463,106 +363,14 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
         zl[f] = t[ctr - 1];
         zr[f] = t[ctr + VZ];
       }
-      float ymD[NDA][VZ], ypD[NDA][VZ], zlD[NDA], zrD[NDA];
-      if constexpr (ND > 0) {
-        const float* b = dsm + (k & 1) * L::DSLOT;
-#pragma unroll
-        for (int e = 0; e < ND; ++e) {
-          const float* t = b + e * L::TILE;
-          ldv<VZ>(t + ctr - L::RL, ymD[e]);
-          ldv<VZ>(t + ctr + L::RL, ypD[e]);
-          zlD[e] = t[ctr - 1];
-          zrD[e] = t[ctr + VZ];
-        }
-      }
-      if (wy & 4) {
-        ghostv(ym, cur, 1);
-        derive_v(ym, ymD);
-      }
-      if (wy & 8) {
-        ghostv(yp, cur, 1);
-        derive_v(yp, ypD);
-      }
+      if (wy & 4) ghostv(ym, cur, 1);
+      if (wy & 8) ghostv(yp, cur, 1);
       const int wx = (x == 0 ? 1 : 0) | (x == g.X - 1 ? 2 : 0);
       float res[NF][VZ];
-      if constexpr (FF) {
-        // z faces of the thread's cells: VZ + 1 fluxes for VZ cells
-        float zq[FT], zd[NDA], zq2[FT], zd2[NDA];
-#pragma unroll
-        for (int f = 0; f < FT; ++f) {
-          zq[f] = zl[f];
-          zq2[f] = zr[f];
-        }
-#pragma unroll
-        for (int e = 0; e < NDA; ++e) {
-          zd[e] = zlD[e];
-          zd2[e] = zrD[e];
-        }
-        if (zb == 0) {
-          float c0[FT], t[NDA];
-          cell_of(cur, curD, 0, c0, t);
-          Phys::ghost(zq, c0, 2);
-          derive_one(zq, zd);
-        }
-        if (zb + VZ - 1 == g.Z - 1) {
-          float c1[FT], t[NDA];
-          cell_of(cur, curD, VZ - 1, c1, t);
-          Phys::ghost(zq2, c1, 2);
-          derive_one(zq2, zd2);
-        }
-        float fz[VZ + 1][NF];
-#pragma unroll
-        for (int j = 0; j <= VZ; ++j) {
-          float a[FT], ad[NDA], b[FT], bd[NDA];
-          if (j == 0) {
-#pragma unroll
-            for (int f = 0; f < FT; ++f) a[f] = zq[f];
-#pragma unroll
-            for (int e = 0; e < NDA; ++e) ad[e] = zd[e];
-          } else {
-            cell_of(cur, curD, j - 1, a, ad);
-          }
-          if (j == VZ) {
-#pragma unroll
-            for (int f = 0; f < FT; ++f) b[f] = zq2[f];
-#pragma unroll
-            for (int e = 0; e < NDA; ++e) bd[e] = zd2[e];
-          } else {
-            cell_of(cur, curD, j, b, bd);
-          }
-          Phys::flux(a, ad, b, bd, 2, P, fz[j]);
-        }
-#pragma unroll
-        for (int j = 0; j < VZ; ++j) {
-          float c[FT], cd[NDA], nb[FT], nbd[NDA], fp[NF], fm[NF], dF[3][NF];
-          cell_of(cur, curD, j, c, cd);
-          cell_of(nxt, nxtD, j, nb, nbd);
-          Phys::flux(c, cd, nb, nbd, 0, P, fp);
-#pragma unroll
-          for (int f = 0; f < NF; ++f) {
-            dF[0][f] = fp[f] - fxm[f][j];
-            fxm[f][j] = fp[f];
-          }
-          cell_of(yp, ypD, j, nb, nbd);
-          Phys::flux(c, cd, nb, nbd, 1, P, fp);
-          cell_of(ym, ymD, j, nb, nbd);
-          Phys::flux(nb, nbd, c, cd, 1, P, fm);
-#pragma unroll
-          for (int f = 0; f < NF; ++f) {
-            dF[1][f] = fp[f] - fm[f];
-            dF[2][f] = fz[j + 1][f] - fz[j][f];
-          }
-          float o[NF];
-          Phys::update(c, cd, dF, (long long)x * plane + (long long)y * g.Z + zb + j, P, o);
-          Phys::acc_cell(acc, o, P);
-#pragma unroll
-          for (int f = 0; f < NF; ++f) res[f][j] = o[f];
-        }
-      } else {
-      CellIn<FT, ND> ins[VZ];
+      CellIn<FT> ins[VZ];
 #pragma unroll
       for (int j = 0; j < VZ; ++j) {
-        CellIn<FT, ND>& in = ins[j];
+        CellIn<FT>& in = ins[j];
 #pragma unroll
         for (int f = 0; f < FT; ++f) {
           in.P[f] = cur[f][j];
@@ -573,27 +381,13 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
           in.nb[4][f] = j == 0 ? zl[f] : cur[f][j - 1];
           in.nb[5][f] = j == VZ - 1 ? zr[f] : cur[f][j + 1];
         }
-        if constexpr (ND > 0) {
-#pragma unroll
-          for (int e = 0; e < ND; ++e) {
-            in.Pd[e] = curD[e][j];
-            in.nbd[0][e] = prvD[e][j];
-            in.nbd[1][e] = nxtD[e][j];
-            in.nbd[2][e] = ymD[e][j];
-            in.nbd[3][e] = ypD[e][j];
-            in.nbd[4][e] = j == 0 ? zlD[e] : curD[e][j - 1];
-            in.nbd[5][e] = j == VZ - 1 ? zrD[e] : curD[e][j + 1];
-          }
-        }
         int w = wx | wy;
         if (j == 0 && zb == 0) {
           Phys::ghost(in.nb[4], in.P, 2);
-          derive_one(in.nb[4], in.nbd[4]);
           w |= 16;
         }
         if (j == VZ - 1 && zb + VZ - 1 == g.Z - 1) {
           Phys::ghost(in.nb[5], in.P, 2);
-          derive_one(in.nb[5], in.nbd[5]);
           w |= 32;
         }
         in.walls = w;
@@ -618,7 +412,6 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
           res[f][1] = o1[f];
         }
       }
-      }
       const long long idx = (long long)x * plane + (long long)y * g.Z + zb;
 #pragma unroll
       for (int f = 0; f < NF; ++f) stv<VZ>(out + f * g.n + idx, res[f]);
@@ -632,18 +425,9 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
     for (int f = 0; f < FT; ++f)
 #pragma unroll
       for (int j = 0; j < VZ; ++j) {
-        if constexpr (!FF) prv[f][j] = cur[f][j];
+        prv[f][j] = cur[f][j];
         cur[f][j] = nxt[f][j];
       }
-    if constexpr (ND > 0) {
-#pragma unroll
-      for (int e = 0; e < ND; ++e)
-#pragma unroll
-        for (int j = 0; j < VZ; ++j) {
-          if constexpr (!FF) prvD[e][j] = curD[e][j];
-          curD[e][j] = nxtD[e][j];
-        }
-    }
     if constexpr (PRE) {
 #pragma unroll
       for (int j = 0; j < VZ; ++j) preC[j] = preN[j];

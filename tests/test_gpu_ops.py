@@ -416,6 +416,42 @@ def test_wave_fused_distorted_vs_fp64_oracle(cfdb, oracle, ctx):
     assert rel_l2(host(out), ref) <= 1e-5
 
 
+def _jittered_box(nx, ny, nz, seed):
+    """(nx+1)(ny+1)(nz+1) vertices of the unit box's lattice, interior ones
+    jittered by U(-0.2, 0.2) of the local spacing (walls stay planar)."""
+    rng = np.random.default_rng(seed)
+    g = np.meshgrid(np.arange(nx + 1) / nx, np.arange(ny + 1) / ny, np.arange(nz + 1) / nz, indexing="ij")
+    V = np.stack(g, axis=-1)
+    J = rng.uniform(-0.2, 0.2, V.shape) * np.array([1 / nx, 1 / ny, 1 / nz])
+    inner = np.zeros(V.shape[:3], bool)
+    inner[1:-1, 1:-1, 1:-1] = True
+    return (V + J * inner[..., None]).reshape(-1, 3)
+
+
+# z extents on both sides of the 32/64-wide tile choice of the face sweep,
+# partial y and z tiles, x shorter than the chunk count; nz = 13 and a c field
+# take the gather form
+@pytest.mark.parametrize("shape,cfield", [((20, 12, 24), False), ((9, 7, 68), False), ((6, 70, 8), False),
+                                          ((11, 9, 132), False), ((7, 9, 13), False), ((10, 6, 12), True)])
+def test_wave_fused_distorted_ragged_vs_fp64_oracle(cfdb, oracle, ctx, shape, cfield):
+    nx, ny, nz = shape
+    V = _jittered_box(nx, ny, nz, seed=5)
+    m = cfdb.Mesh.from_vertices(ctx, nx, ny, nz, 1 / nx, 1 / ny, 1 / nz, V)
+    o = oracle.Mesh(nx, ny, nz, 1 / nx, 1 / ny, 1 / nz, vertices=V)
+    rng = np.random.default_rng(6)
+    q0 = 0.1 * rng.standard_normal(4 * m.n)
+    c = np.exp(0.2 * rng.standard_normal(m.n)) if cfield else None
+    mode = 1 if cfield else 0
+    dt = o.wave_dt(0.4, c=c)
+    a = dev(q0, torch.float32)
+    b = torch.empty_like(a)
+    tc = None if c is None else dev(c, torch.float32)
+    out = run_steps(lambda x, y: ctx.wave_step(m, x, y, dt, c=tc, speed_mode=mode, path=cfdb.FUSED), a, b, 12)
+    ref = o.wave_solve(q0, dt, 12, c=c, speed_mode=mode)
+    assert rel_l2(host(out), ref) <= 1e-5
+    assert rel_linf(host(out), ref) <= 1e-5
+
+
 def test_wave_config2_fused_fp32_vs_fp64_plain_full_size(cfdb, ctx):
     """The wave workload at full size (128^3, 500 steps): FP32 fused vs the
     FP64 plain GPU path (bit-identical to the FP64 oracle on the small cases
