@@ -7,6 +7,7 @@
 #include <new>
 
 #include "euler_internal.hpp"
+#include "f32x2.cuh"
 #include "tma_host.hpp"
 
 CFDB_MODULE_ANCHOR
@@ -130,29 +131,65 @@ struct EulerPhys {
 #pragma unroll
     for (int e = 0; e < ND; ++e) gd[e] = Cd[e];
   }
-  __device__ static void update(const float P[NF], const float*, const float*, const float dF[3][NF], const Params& a,
-                                float o[NF]) {
-#pragma unroll
-    for (int c = 0; c < NF; ++c) o[c] = P[c] - (a.kd[0] * dF[0][c] + (a.kd[1] * dF[1][c] + a.kd[2] * dF[2][c]));
-  }
-
   __device__ static void acc_init(Acc& s) {
     s.l[0] = s.l[1] = s.l[2] = 0.f;
     s.s0 = s.c0 = s.s1 = s.c1 = 0.0;
   }
 
-  // A thread's own cells (VZ columns of one x chunk) are summed in plain
-  // double: with 24-bit inputs the error stays near 1e-13 relative even for
-  // thousands of cells; compensation starts at the thread level, where the
-  // partial sums of millions of cells meet.  The uniform volume multiplies once.
-  __device__ static void acc_cell(Acc& s, const float o[NF], const Params& a) {
-    float ir, u[3], p, c;
-    prim(o, a.gamma - 1.0f, a.gamma, ir, u, p, c);
-    s.l[0] = fmaxf(s.l[0], fabsf(u[0]) + c);
-    s.l[1] = fmaxf(s.l[1], fabsf(u[1]) + c);
-    s.l[2] = fmaxf(s.l[2], fabsf(u[2]) + c);
-    s.s0 += double(o[0]);
-    s.s1 += double(o[4]);
+  // The sweep runs two z cells per thread and hands them over as (cell 0,
+  // cell 1) pairs: every FP32 add, multiply and fma below is one packed
+  // f32x2 instruction (each lane rounds like the scalar instruction); the
+  // reciprocal, square root, |.| and max stay per lane.  The scalar flux
+  // and derive above serve the single faces and halo cells.
+  static constexpr bool PAIRED = true;
+  __device__ static float2 rcp2(float2 x) { return make_float2(fast_rcp(x.x), fast_rcp(x.y)); }
+  __device__ static float2 sqrt2(float2 x) { return make_float2(fast_sqrt(x.x), fast_sqrt(x.y)); }
+  __device__ static void prim2(const float2 q[NF], const Params& a, float2& ir, float2 u[3], float2& p, float2& c) {
+    using namespace f2;
+    ir = rcp2(q[0]);
+    u[0] = mul(q[1], ir); u[1] = mul(q[2], ir); u[2] = mul(q[3], ir);
+    const float2 ke = fma(q[3], u[2], fma(q[2], u[1], mul(q[1], u[0])));
+    p = mul(splat(a.gamma - 1.0f), fma(splat(-0.5f), ke, q[4]));
+    c = sqrt2(mul(mul(splat(a.gamma), p), ir));
+  }
+  __device__ static void derive2(const float2 q[NF], float2 d[ND], const Params& a) {
+    float2 u[3];
+    prim2(q, a, d[0], u, d[1], d[2]);
+  }
+  __device__ static void flux2(const float2 L[NF], const float2 Ld[ND], const float2 R[NF], const float2 Rd[ND], int d,
+                               const Params&, float2 F[NF]) {
+    using namespace f2;
+    const float2 uL = mul(L[1 + d], Ld[0]), uR = mul(R[1 + d], Rd[0]);
+    const float2 pL = Ld[1], pR = Rd[1];
+    const float2 m = make_float2(fmaxf(fabsf(uL.x) + Ld[2].x, fabsf(uR.x) + Rd[2].x),
+                                 fmaxf(fabsf(uL.y) + Ld[2].y, fabsf(uR.y) + Rd[2].y));
+    const float2 h = splat(0.5f);
+    const float2 wL = fma(h, uL, mul(h, m)), wR = fma(h, uR, mul(splat(-0.5f), m));
+#pragma unroll
+    for (int c = 0; c < NF; ++c) F[c] = fma(L[c], wL, mul(R[c], wR));
+    F[1 + d] = fma(h, add(pL, pR), F[1 + d]);
+    F[4] = fma(h, fma(pL, uL, mul(pR, uR)), F[4]);
+  }
+  // Update: U' = U - sum_d (dt/h_d) (F(d+) - F(d-)).
+  __device__ static void update2(const float2 P[NF], const float2*, const float2 dF[3][NF], const Params& a,
+                                 float2 o[NF]) {
+    using namespace f2;
+    const float2 k0 = splat(a.kd[0]), k1 = splat(a.kd[1]), k2 = splat(a.kd[2]);
+#pragma unroll
+    for (int c = 0; c < NF; ++c) o[c] = sub(P[c], fma(k0, dF[0][c], fma(k1, dF[1][c], mul(k2, dF[2][c]))));
+  }
+  // Epilogue per cell of the new state: the signal speeds |u_d| + a for the
+  // next dt, and the mass and energy summed in plain double (with 24-bit
+  // inputs the error of a thread's few hundred cells stays near 1e-13
+  // relative; compensation starts where the per-thread sums meet).  The
+  // uniform volume multiplies once.
+  __device__ static void acc_cell2(Acc& s, const float2 o[NF], const Params& a) {
+    float2 ir, u[3], p, c;
+    prim2(o, a, ir, u, p, c);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) s.l[i] = fmaxf(s.l[i], fmaxf(fabsf(u[i].x) + c.x, fabsf(u[i].y) + c.y));
+    s.s0 += double(o[0].x) + double(o[0].y);
+    s.s1 += double(o[4].x) + double(o[4].y);
   }
 
   __device__ static void finish(Acc& s, const Params& a, bool) {
@@ -237,6 +274,8 @@ struct EulerPhys {
 
 constexpr int kEulerCtasPerSm = 2;
 constexpr int kEulerVZ = 2;
+
+static_assert(kEulerVZ == 2, "EulerPhys provides its per-cell update only as packed pairs");
 
 template <int TZ>
 int launch_euler(cfdb_euler* e, const void* U, void* Un, int64_t s) {

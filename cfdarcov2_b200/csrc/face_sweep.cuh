@@ -54,7 +54,13 @@
 //                                 const float dF[3][NF], const Params&, float out[NF]);  dF[d] = F(d+) - F(d-)
 //   __device__ static void acc_init(Acc&), acc_cell(Acc&, const float out[NF], const Params&),
 //                          finish(Acc&, const Params&, bool thread_active);
-// (array extents of size 0 are passed as 1).
+// (array extents of size 0 are passed as 1), and optionally, with two cells
+// per thread (VZ == 2), the same operations on (cell 0, cell 1) pairs
+// (Phys::PAIRED, NGF == 0), which the physics can run as packed f32x2
+// instructions:
+//   derive2(const float2 q[NF], float2 d[ND], P), flux2(const float2 L[NF], const float2 Ld[ND],
+//   const float2 R[NF], const float2 Rd[ND], int d, P, float2 F[NF]), update2(const float2 C[NF],
+//   const float2 Cd[ND], const float2 dF[3][NF], P, float2 out[NF]), acc_cell2(Acc&, const float2 out[NF], P).
 #pragma once
 
 #include "tma_stencil.cuh"
@@ -66,6 +72,132 @@ namespace stencil {
 struct PaddedGeom {
   const void* base;
   int64_t zp, yp, xp, np;
+};
+
+template <class P, class = void> struct face_paired { static constexpr bool value = false; };
+template <class P> struct face_paired<P, decltype(void(P::PAIRED))> { static constexpr bool value = P::PAIRED; };
+
+// The physics operations on a thread's VZ cells ([field][cell] arrays): one
+// packed call for paired physics with VZ == 2, a loop over the cells
+// otherwise.
+template <class Phys, int VZ> struct FaceOps {
+  static constexpr int NF = Phys::NF, ND = Phys::ND, NG = Phys::NG, NGF = Phys::NGF;
+  static constexpr int NDA = ND > 0 ? ND : 1, NGA = NG > 0 ? NG : 1, NGFA = NGF > 0 ? NGF : 1;
+  static constexpr bool PAIR = face_paired<Phys>::value && VZ == 2;
+  using Params = typename Phys::Params;
+
+  template <int N> __device__ static void col(const float v[][VZ], int j, float* out) {
+#pragma unroll
+    for (int f = 0; f < N; ++f) out[f] = v[f][j];
+  }
+  template <int N> __device__ static void pack(const float v[][VZ], float2* out) {
+#pragma unroll
+    for (int f = 0; f < N; ++f) out[f] = make_float2(v[f][0], v[f][VZ - 1]);
+  }
+  template <int N> __device__ static void unpack(const float2* in, float v[][VZ]) {
+#pragma unroll
+    for (int f = 0; f < N; ++f) { v[f][0] = in[f].x; v[f][VZ - 1] = in[f].y; }
+  }
+
+  __device__ static void derive(const float q[NF][VZ], float d[NDA][VZ], const Params& P) {
+    if constexpr (ND > 0) {
+      if constexpr (PAIR) {
+        float2 q2[NF], d2[ND];
+        pack<NF>(q, q2);
+        Phys::derive2(q2, d2, P);
+        unpack<ND>(d2, d);
+      } else {
+#pragma unroll
+        for (int j = 0; j < VZ; ++j) {
+          float a[NF], t[NDA];
+          col<NF>(q, j, a);
+          Phys::derive(a, t, P);
+#pragma unroll
+          for (int e = 0; e < ND; ++e) d[e][j] = t[e];
+        }
+      }
+    }
+  }
+  __device__ static void flux(const float L[NF][VZ], const float Ld[NDA][VZ], const float R[NF][VZ],
+                              const float Rd[NDA][VZ], const float Sf[NGFA][VZ], int d, const Params& P,
+                              float F[NF][VZ]) {
+    if constexpr (PAIR) {
+      float2 l[NF], ld[NDA], r[NF], rd[NDA], f2[NF];
+      pack<NF>(L, l);
+      pack<NDA>(Ld, ld);
+      pack<NF>(R, r);
+      pack<NDA>(Rd, rd);
+      Phys::flux2(l, ld, r, rd, d, P, f2);
+      unpack<NF>(f2, F);
+    } else {
+#pragma unroll
+      for (int j = 0; j < VZ; ++j) {
+        float a[NF], ad[NDA], b[NF], bd[NDA], s[NGFA], o[NF];
+        col<NF>(L, j, a);
+        col<NDA>(Ld, j, ad);
+        col<NF>(R, j, b);
+        col<NDA>(Rd, j, bd);
+        col<NGFA>(Sf, j, s);
+        Phys::flux(a, ad, b, bd, s, d, P, o);
+#pragma unroll
+        for (int f = 0; f < NF; ++f) F[f][j] = o[f];
+      }
+    }
+  }
+  __device__ static void ghost(const float C[NF][VZ], const float Cd[NDA][VZ], const float Sf[NGFA][VZ], int d,
+                               float g[NF][VZ], float gd[NDA][VZ]) {
+#pragma unroll
+    for (int j = 0; j < VZ; ++j) {
+      float c[NF], cd[NDA], s[NGFA], gq[NF], gdd[NDA];
+      col<NF>(C, j, c);
+      col<NDA>(Cd, j, cd);
+      col<NGFA>(Sf, j, s);
+      Phys::ghost(c, cd, s, d, gq, gdd);
+#pragma unroll
+      for (int f = 0; f < NF; ++f) g[f][j] = gq[f];
+#pragma unroll
+      for (int e = 0; e < NDA; ++e) gd[e][j] = gdd[e];
+    }
+  }
+  __device__ static void update(const float C[NF][VZ], const float Cd[NDA][VZ], const float G[NGA][VZ],
+                                const float dF[3][NF][VZ], const Params& P, float o[NF][VZ]) {
+    if constexpr (PAIR) {
+      float2 c[NF], cd[NDA], df[3][NF], r[NF];
+      pack<NF>(C, c);
+      pack<NDA>(Cd, cd);
+#pragma unroll
+      for (int d = 0; d < 3; ++d) pack<NF>(dF[d], df[d]);
+      Phys::update2(c, cd, df, P, r);
+      unpack<NF>(r, o);
+    } else {
+#pragma unroll
+      for (int j = 0; j < VZ; ++j) {
+        float c[NF], cd[NDA], gg[NGA], df[3][NF], r[NF];
+        col<NF>(C, j, c);
+        col<NDA>(Cd, j, cd);
+        col<NGA>(G, j, gg);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) col<NF>(dF[d], j, df[d]);
+        Phys::update(c, cd, gg, df, P, r);
+#pragma unroll
+        for (int f = 0; f < NF; ++f) o[f][j] = r[f];
+      }
+    }
+  }
+  __device__ static void acc(typename Phys::Acc& a, const float o[NF][VZ], const Params& P) {
+    if constexpr (PAIR) {
+      float2 r[NF];
+      pack<NF>(o, r);
+      Phys::acc_cell2(a, r, P);
+    } else {
+#pragma unroll
+      for (int j = 0; j < VZ; ++j) {
+        float r[NF];
+        col<NF>(o, j, r);
+        Phys::acc_cell(a, r, P);
+      }
+    }
+  }
 };
 
 template <int TZ, int TY, int S, int NF, int NG, int ND, int VZ> struct FaceLayout {
@@ -184,19 +316,7 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
   float* const dsm = smem + S * L::SLOT;
   auto dbuf = [&](int k) -> float* { return dsm + (k & 1) * L::DSLOT; };
 
-  auto derive_v = [&](const float v[NF][VZ], float d[NDA][VZ]) {
-    if constexpr (ND > 0) {
-#pragma unroll
-      for (int j = 0; j < VZ; ++j) {
-        float q[NF], t[NDA];
-#pragma unroll
-        for (int f = 0; f < NF; ++f) q[f] = v[f][j];
-        Phys::derive(q, t, P);
-#pragma unroll
-        for (int e = 0; e < ND; ++e) d[e][j] = t[e];
-      }
-    }
-  };
+  using Ops = FaceOps<Phys, VZ>;
   // derived values of plane k for the y/z neighbours: the thread's own cells
   // (from its registers) and one cell of the tile's halo ring per thread
   auto publish = [&](int k, const float d[NDA][VZ]) {
@@ -229,30 +349,9 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
 #pragma unroll
     for (int f = 0; f < NF; ++f) ldv<VZ>(b + f * L::TILE + off, v[f]);
   };
-  // The ghosts of a thread's VZ cells across their d faces with geometry Sf;
-  // used behind a branch that is uniform over the CTA (x walls) or the warp
-  // (y walls, a tile row being one warp), so no lane diverges.
-  auto ghost_v = [&](const float C[NF][VZ], const float Cd[NDA][VZ], const float Sf[NGFA][VZ], int d,
-                     float nb[NF][VZ], float nbd[NDA][VZ]) {
-#pragma unroll
-    for (int j = 0; j < VZ; ++j) {
-      float c[NF], cd[NDA], s[NGFA], gq[NF], gd[NDA];
-#pragma unroll
-      for (int f = 0; f < NF; ++f) c[f] = C[f][j];
-#pragma unroll
-      for (int e = 0; e < NDA; ++e) cd[e] = ND > 0 ? Cd[e][j] : 0.f;
-#pragma unroll
-      for (int e = 0; e < NGFA; ++e) s[e] = NGF > 0 ? Sf[e][j] : 0.f;
-      Phys::ghost(c, cd, s, d, gq, gd);
-#pragma unroll
-      for (int f = 0; f < NF; ++f) nb[f][j] = gq[f];
-#pragma unroll
-      for (int e = 0; e < NDA; ++e) nbd[e][j] = gd[e];
-    }
-  };
-  // The neighbour across a z face, which is a wall for single lanes only: the
-  // loaded cell, or the ghost of C (built behind a branch, or always and
-  // selected).
+  // The neighbour across a z face, which is a wall for single lanes only:
+  // the loaded cell, or the ghost of C (built behind a branch, or always
+  // and selected).
   auto across = [&](bool wall, const float C[NF], const float Cd[NDA], const float Sf[NGFA], int d, float nb[NF],
                     float nbd[NDA]) {
     if (SEL || wall) {
@@ -264,6 +363,21 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
       for (int e = 0; e < NDA; ++e) nbd[e] = wall ? gd[e] : nbd[e];
     }
   };
+  // Flux through a face set whose walls are uniform over the warp (x walls
+  // over the CTA, y walls over a tile row = one warp): the neighbours R, or
+  // the ghosts of C when `wall` (plus = true: C on the minus side).
+  auto wall_or = [&](bool wall, bool plus, const float C[NF][VZ], const float Cd[NDA][VZ], const float R[NF][VZ],
+                     const float Rd[NDA][VZ], const float Sf[NGFA][VZ], int d, float F[NF][VZ]) {
+    if (!wall) {
+      if (plus) Ops::flux(C, Cd, R, Rd, Sf, d, P, F);
+      else Ops::flux(R, Rd, C, Cd, Sf, d, P, F);
+    } else {
+      float gq[NF][VZ], gd[NDA][VZ];
+      Ops::ghost(C, Cd, Sf, d, gq, gd);
+      if (plus) Ops::flux(C, Cd, gq, gd, Sf, d, P, F);
+      else Ops::flux(gq, gd, C, Cd, Sf, d, P, F);
+    }
+  };
 
   // the first plane's derived values, and the flux through its -x faces
   float Cd[NDA][VZ] = {};
@@ -273,7 +387,7 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
   {
     float C[NF][VZ];
     load_state(1, cs, C);
-    derive_v(C, Cd);
+    Ops::derive(C, Cd, P);
     publish(1, Cd);
     if (active) {
       float Sf[NGFA][VZ] = {}, Q[NF][VZ], Qd[NDA][VZ] = {};
@@ -282,23 +396,9 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
       for (int e = 0; e < NGF; ++e) ldv<VZ>(g0 + e * L::GTILE + cg, Sf[e]);
       if (x0 > 0) {
         load_state(0, cs, Q);
-        derive_v(Q, Qd);
-      } else {
-        ghost_v(C, Cd, Sf, 0, Q, Qd);
+        Ops::derive(Q, Qd, P);
       }
-#pragma unroll
-      for (int j = 0; j < VZ; ++j) {
-        float a[NF], ad[NDA], b[NF], bd[NDA], s[NGFA], F[NF];
-#pragma unroll
-        for (int f = 0; f < NF; ++f) { b[f] = C[f][j]; a[f] = Q[f][j]; }
-#pragma unroll
-        for (int e = 0; e < NDA; ++e) { bd[e] = Cd[e][j]; ad[e] = Qd[e][j]; }
-#pragma unroll
-        for (int e = 0; e < NGFA; ++e) s[e] = NGF > 0 ? Sf[e][j] : 0.f;
-        Phys::flux(a, ad, b, bd, s, 0, P, F);
-#pragma unroll
-        for (int f = 0; f < NF; ++f) fxm[f][j] = F[f];
-      }
+      wall_or(x0 == 0, false, C, Cd, Q, Qd, Sf, 0, fxm);
     }
   }
   __syncthreads();
@@ -320,23 +420,15 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
     if (!xhi) {
       wait_plane(k + 1);
       load_state(k + 1, cs, N);
-      derive_v(N, Nd);
+      Ops::derive(N, Nd, P);
       publish(k + 1, Nd);
     }
     if (active) {
-      float C[NF][VZ], G[NGA][VZ];
+      float C[NF][VZ], G[NGA][VZ] = {};
       load_state(k, cs, C);
       const float* cgm = geom(k);
 #pragma unroll
       for (int e = 0; e < NG; ++e) ldv<VZ>(cgm + e * L::GTILE + cg, G[e]);
-      auto cell = [&](int j, float c[NF], float cd[NDA], float gg[NGA]) {
-#pragma unroll
-        for (int f = 0; f < NF; ++f) c[f] = C[f][j];
-#pragma unroll
-        for (int e = 0; e < NDA; ++e) cd[e] = Cd[e][j];
-#pragma unroll
-        for (int e = 0; e < NGA; ++e) gg[e] = G[e][j];
-      };
       // the geometry of the thread's cells' +d faces
       auto gface = [&](int d, float Sf[NGFA][VZ]) {
 #pragma unroll
@@ -344,32 +436,24 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
 #pragma unroll
           for (int j = 0; j < VZ; ++j) Sf[e][j] = NGF > 0 ? G[d * NGF + e][j] : 0.f;
       };
-      float dF[VZ][3][NF];
-      // x faces
-      float Sx[NGFA][VZ];
-      gface(0, Sx);
-      if (xhi) ghost_v(C, Cd, Sx, 0, N, Nd);
+      float dF[3][NF][VZ];
+      // x faces: the +x flux of plane k is the -x flux of plane k + 1
+      {
+        float Sx[NGFA][VZ], F[NF][VZ];
+        gface(0, Sx);
+        wall_or(xhi, true, C, Cd, N, Nd, Sx, 0, F);
 #pragma unroll
-      for (int j = 0; j < VZ; ++j) {
-        float c[NF], cd[NDA], gg[NGA], b[NF], bd[NDA], s[NGFA], F[NF];
-        cell(j, c, cd, gg);
+        for (int f = 0; f < NF; ++f)
 #pragma unroll
-        for (int f = 0; f < NF; ++f) b[f] = N[f][j];
-#pragma unroll
-        for (int e = 0; e < NDA; ++e) bd[e] = Nd[e][j];
-#pragma unroll
-        for (int e = 0; e < NGFA; ++e) s[e] = Sx[e][j];
-        Phys::flux(c, cd, b, bd, s, 0, P, F);
-#pragma unroll
-        for (int f = 0; f < NF; ++f) {
-          dF[j][0][f] = F[f] - fxm[f][j];
-          fxm[f][j] = F[f];
-        }
+          for (int j = 0; j < VZ; ++j) {
+            dF[0][f][j] = F[f][j] - fxm[f][j];
+            fxm[f][j] = F[f][j];
+          }
       }
-      // y faces
+      // y faces: both per cell
       {
         const float* db = dbuf(k);
-        float Ym[NF][VZ], Yp[NF][VZ], Ymd[NDA][VZ] = {}, Ypd[NDA][VZ] = {}, Sm[NGFA][VZ] = {};
+        float Ym[NF][VZ], Yp[NF][VZ], Ymd[NDA][VZ] = {}, Ypd[NDA][VZ] = {}, Sm[NGFA][VZ] = {}, Sy[NGFA][VZ];
         load_state(k, cs - L::RL, Ym);
         load_state(k, cs + L::RL, Yp);
 #pragma unroll
@@ -379,91 +463,71 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
         }
 #pragma unroll
         for (int e = 0; e < NGF; ++e) ldv<VZ>(cgm + (NGF + e) * L::GTILE + cg - L::GL, Sm[e]);
-        float Sy[NGFA][VZ];
         gface(1, Sy);
-        if (yhi) ghost_v(C, Cd, Sy, 1, Yp, Ypd);
-        if (ylo) ghost_v(C, Cd, Sm, 1, Ym, Ymd);
+        float Fp[NF][VZ], Fm[NF][VZ];
+        wall_or(yhi, true, C, Cd, Yp, Ypd, Sy, 1, Fp);
+        wall_or(ylo, false, C, Cd, Ym, Ymd, Sm, 1, Fm);
 #pragma unroll
-        for (int j = 0; j < VZ; ++j) {
-          float c[NF], cd[NDA], gg[NGA], Fp[NF], Fm[NF];
-          cell(j, c, cd, gg);
-          {
-            float b[NF], bd[NDA], s[NGFA];
+        for (int f = 0; f < NF; ++f)
 #pragma unroll
-            for (int f = 0; f < NF; ++f) b[f] = Yp[f][j];
-#pragma unroll
-            for (int e = 0; e < NDA; ++e) bd[e] = Ypd[e][j];
-#pragma unroll
-            for (int e = 0; e < NGFA; ++e) s[e] = Sy[e][j];
-            Phys::flux(c, cd, b, bd, s, 1, P, Fp);
-          }
-          {
-            float a[NF], ad[NDA], s[NGFA];
-#pragma unroll
-            for (int f = 0; f < NF; ++f) a[f] = Ym[f][j];
-#pragma unroll
-            for (int e = 0; e < NDA; ++e) ad[e] = Ymd[e][j];
-#pragma unroll
-            for (int e = 0; e < NGFA; ++e) s[e] = Sm[e][j];
-            Phys::flux(a, ad, c, cd, s, 1, P, Fm);
-          }
-#pragma unroll
-          for (int f = 0; f < NF; ++f) dF[j][1][f] = Fp[f] - Fm[f];
-        }
+          for (int j = 0; j < VZ; ++j) dF[1][f][j] = Fp[f][j] - Fm[f][j];
       }
-      // z faces: VZ + 1 for the thread's VZ cells
+      // z faces: VZ + 1 for the thread's VZ cells; faces 0 .. VZ-1 (left
+      // cells zl, C_0 .. C_{VZ-2}) as one vector call, face VZ alone
       {
         const float* cq = state(k);
         const float* db = dbuf(k);
-        float Fz[VZ + 1][NF];
+        float Lz[NF][VZ], Lzd[NDA][VZ] = {}, Sz[NGFA][VZ] = {};
+#pragma unroll
+        for (int j = 1; j < VZ; ++j) {
+#pragma unroll
+          for (int f = 0; f < NF; ++f) Lz[f][j] = C[f][j - 1];
+#pragma unroll
+          for (int e = 0; e < ND; ++e) Lzd[e][j] = Cd[e][j - 1];
+#pragma unroll
+          for (int e = 0; e < NGF; ++e) Sz[e][j] = G[2 * NGF + e][j - 1];
+        }
         {
-          float c[NF], cd[NDA], gg[NGA], a[NF], ad[NDA], s[NGFA];
-          cell(0, c, cd, gg);
+          float a[NF], ad[NDA] = {}, s[NGFA] = {}, c[NF], cd[NDA];
 #pragma unroll
           for (int f = 0; f < NF; ++f) a[f] = cq[f * L::TILE + cs - 1];
 #pragma unroll
-          for (int e = 0; e < NDA; ++e) ad[e] = ND > 0 ? db[e * L::TILE + cs - 1] : 0.f;
+          for (int e = 0; e < ND; ++e) ad[e] = db[e * L::TILE + cs - 1];
 #pragma unroll
-          for (int e = 0; e < NGFA; ++e) s[e] = NGF > 0 ? cgm[(2 * NGF + e) * L::GTILE + cg - 1] : 0.f;
+          for (int e = 0; e < NGF; ++e) s[e] = cgm[(2 * NGF + e) * L::GTILE + cg - 1];
+          Ops::template col<NF>(C, 0, c);
+          Ops::template col<NDA>(Cd, 0, cd);
           across(zlo, c, cd, s, 2, a, ad);
-          Phys::flux(a, ad, c, cd, s, 2, P, Fz[0]);
-        }
 #pragma unroll
-        for (int j = 1; j < VZ; ++j) {
-          float a[NF], ad[NDA], ga[NGA], b[NF], bd[NDA], gb[NGA], s[NGFA];
-          cell(j - 1, a, ad, ga);
-          cell(j, b, bd, gb);
+          for (int f = 0; f < NF; ++f) Lz[f][0] = a[f];
 #pragma unroll
-          for (int e = 0; e < NGFA; ++e) s[e] = NGF > 0 ? ga[2 * NGF + e] : 0.f;
-          Phys::flux(a, ad, b, bd, s, 2, P, Fz[j]);
+          for (int e = 0; e < NDA; ++e) Lzd[e][0] = ad[e];
+#pragma unroll
+          for (int e = 0; e < NGFA; ++e) Sz[e][0] = s[e];
         }
+        float Fz[NF][VZ], Fl[NF];
+        Ops::flux(Lz, Lzd, C, Cd, Sz, 2, P, Fz);
         {
-          float c[NF], cd[NDA], gg[NGA], b[NF], bd[NDA], s[NGFA];
-          cell(VZ - 1, c, cd, gg);
+          float c[NF], cd[NDA], b[NF], bd[NDA] = {}, s[NGFA] = {};
+          Ops::template col<NF>(C, VZ - 1, c);
+          Ops::template col<NDA>(Cd, VZ - 1, cd);
 #pragma unroll
           for (int f = 0; f < NF; ++f) b[f] = cq[f * L::TILE + cs + VZ];
 #pragma unroll
-          for (int e = 0; e < NDA; ++e) bd[e] = ND > 0 ? db[e * L::TILE + cs + VZ] : 0.f;
+          for (int e = 0; e < ND; ++e) bd[e] = db[e * L::TILE + cs + VZ];
 #pragma unroll
-          for (int e = 0; e < NGFA; ++e) s[e] = NGF > 0 ? gg[2 * NGF + e] : 0.f;
+          for (int e = 0; e < NGF; ++e) s[e] = G[2 * NGF + e][VZ - 1];
           across(zhi, c, cd, s, 2, b, bd);
-          Phys::flux(c, cd, b, bd, s, 2, P, Fz[VZ]);
+          Phys::flux(c, cd, b, bd, s, 2, P, Fl);
         }
 #pragma unroll
-        for (int j = 0; j < VZ; ++j)
+        for (int f = 0; f < NF; ++f)
 #pragma unroll
-          for (int f = 0; f < NF; ++f) dF[j][2][f] = Fz[j + 1][f] - Fz[j][f];
+          for (int j = 0; j < VZ; ++j) dF[2][f][j] = (j + 1 < VZ ? Fz[f][j + 1] : Fl[f]) - Fz[f][j];
       }
       float res[NF][VZ];
-#pragma unroll
-      for (int j = 0; j < VZ; ++j) {
-        float c[NF], cd[NDA], gg[NGA], o[NF];
-        cell(j, c, cd, gg);
-        Phys::update(c, cd, gg, dF[j], P, o);
-        Phys::acc_cell(acc, o, P);
-#pragma unroll
-        for (int f = 0; f < NF; ++f) res[f][j] = o[f];
-      }
+      Ops::update(C, Cd, G, dF, P, res);
+      Ops::acc(acc, res, P);
       const long long idx = (long long)x * plane + (long long)y * g.Z + zb;
 #pragma unroll
       for (int f = 0; f < NF; ++f) stv<VZ>(out + f * g.n + idx, res[f]);
