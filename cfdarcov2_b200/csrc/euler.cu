@@ -233,15 +233,16 @@ struct EulerPhys {
       is_last = atomicAdd(&ck->counter, 1u) == nblocks - 1;
     }
     __syncthreads();
-    // The last CTA folds the per-CTA partials with its first warp: lane l
-    // takes partials l, l + 32, ... in order, then the lanes merge pairwise
-    // through shuffles in a fixed pattern, so the totals do not depend on
-    // timing (a single thread folding every partial serially kept all other
-    // SMs waiting for ~3 us per step).
-    if (is_last && threadIdx.x < 32) {
+    // The last CTA folds the per-CTA partials with all its threads: thread t
+    // takes partials t, t + blockDim, ... in order, the lanes of each warp
+    // merge through shuffles in a fixed pattern and thread 0 merges the warps
+    // in order, so the totals do not depend on timing.  (One thread folding
+    // every partial serially kept all other SMs waiting for ~13 us per step;
+    // one warp, ~10 dependent loads per lane.)
+    if (is_last) {
       __threadfence();
       double S0 = 0, C0 = 0, S1 = 0, C1 = 0;
-      for (unsigned k = threadIdx.x; k < nblocks; k += 32) {
+      for (unsigned k = threadIdx.x; k < nblocks; k += blockDim.x) {
         const Comp2 q = a.part[k];
         comp_add(S0, C0, q.s0); C0 += q.c0;
         comp_add(S1, C1, q.s1); C1 += q.c1;
@@ -252,7 +253,16 @@ struct EulerPhys {
         comp_add(S0, C0, a0); C0 += b0;
         comp_add(S1, C1, a1); C1 += b1;
       }
+      if ((threadIdx.x & 31) == 0) {
+        sh[w][0] = S0; sh[w][1] = C0; sh[w][2] = S1; sh[w][3] = C1;
+      }
+      __syncthreads();
       if (threadIdx.x == 0) {
+        S0 = C0 = S1 = C1 = 0;
+        for (int k = 0; k < int(blockDim.x / 32); ++k) {
+          comp_add(S0, C0, sh[k][0]); C0 += sh[k][1];
+          comp_add(S1, C1, sh[k][2]); C1 += sh[k][3];
+        }
         ck->counter = 0;
         const int ts = int(a.s & 1);
         const int ls = int(a.s % 3);
