@@ -56,13 +56,16 @@
 //                          finish(Acc&, const Params&, bool thread_active);
 // (array extents of size 0 are passed as 1), and optionally, with two cells
 // per thread (VZ == 2), the same operations on (cell 0, cell 1) pairs
-// (Phys::PAIRED, NGF == 0), which the physics can run as packed f32x2
-// instructions:
+// (Phys::PAIRED; derived values, no per-cell geometry), which the physics
+// can run as packed f32x2 instructions (the kernel then keeps a thread's
+// cells in register pairs throughout; update and acc_cell are needed only in
+// pair form):
 //   derive2(const float2 q[NF], float2 d[ND], P), flux2(const float2 L[NF], const float2 Ld[ND],
 //   const float2 R[NF], const float2 Rd[ND], int d, P, float2 F[NF]), update2(const float2 C[NF],
 //   const float2 Cd[ND], const float2 dF[3][NF], P, float2 out[NF]), acc_cell2(Acc&, const float2 out[NF], P).
 #pragma once
 
+#include "f32x2.cuh"
 #include "tma_stencil.cuh"
 
 namespace stencil {
@@ -77,9 +80,9 @@ struct PaddedGeom {
 template <class P, class = void> struct face_paired { static constexpr bool value = false; };
 template <class P> struct face_paired<P, decltype(void(P::PAIRED))> { static constexpr bool value = P::PAIRED; };
 
-// The physics operations on a thread's VZ cells ([field][cell] arrays): one
-// packed call for paired physics with VZ == 2, a loop over the cells
-// otherwise.
+// The physics operations on a thread's VZ cells ([field][cell] arrays), as
+// loops over the cells.  Paired physics (PAIR) run a path of their own in the
+// kernel, on register pairs.
 template <class Phys, int VZ> struct FaceOps {
   static constexpr int NF = Phys::NF, ND = Phys::ND, NG = Phys::NG, NGF = Phys::NGF;
   static constexpr int NDA = ND > 0 ? ND : 1, NGA = NG > 0 ? NG : 1, NGFA = NGF > 0 ? NGF : 1;
@@ -90,58 +93,33 @@ template <class Phys, int VZ> struct FaceOps {
 #pragma unroll
     for (int f = 0; f < N; ++f) out[f] = v[f][j];
   }
-  template <int N> __device__ static void pack(const float v[][VZ], float2* out) {
-#pragma unroll
-    for (int f = 0; f < N; ++f) out[f] = make_float2(v[f][0], v[f][VZ - 1]);
-  }
-  template <int N> __device__ static void unpack(const float2* in, float v[][VZ]) {
-#pragma unroll
-    for (int f = 0; f < N; ++f) { v[f][0] = in[f].x; v[f][VZ - 1] = in[f].y; }
-  }
 
   __device__ static void derive(const float q[NF][VZ], float d[NDA][VZ], const Params& P) {
     if constexpr (ND > 0) {
-      if constexpr (PAIR) {
-        float2 q2[NF], d2[ND];
-        pack<NF>(q, q2);
-        Phys::derive2(q2, d2, P);
-        unpack<ND>(d2, d);
-      } else {
 #pragma unroll
-        for (int j = 0; j < VZ; ++j) {
-          float a[NF], t[NDA];
-          col<NF>(q, j, a);
-          Phys::derive(a, t, P);
+      for (int j = 0; j < VZ; ++j) {
+        float a[NF], t[NDA];
+        col<NF>(q, j, a);
+        Phys::derive(a, t, P);
 #pragma unroll
-          for (int e = 0; e < ND; ++e) d[e][j] = t[e];
-        }
+        for (int e = 0; e < ND; ++e) d[e][j] = t[e];
       }
     }
   }
   __device__ static void flux(const float L[NF][VZ], const float Ld[NDA][VZ], const float R[NF][VZ],
                               const float Rd[NDA][VZ], const float Sf[NGFA][VZ], int d, const Params& P,
                               float F[NF][VZ]) {
-    if constexpr (PAIR) {
-      float2 l[NF], ld[NDA], r[NF], rd[NDA], f2[NF];
-      pack<NF>(L, l);
-      pack<NDA>(Ld, ld);
-      pack<NF>(R, r);
-      pack<NDA>(Rd, rd);
-      Phys::flux2(l, ld, r, rd, d, P, f2);
-      unpack<NF>(f2, F);
-    } else {
 #pragma unroll
-      for (int j = 0; j < VZ; ++j) {
-        float a[NF], ad[NDA], b[NF], bd[NDA], s[NGFA], o[NF];
-        col<NF>(L, j, a);
-        col<NDA>(Ld, j, ad);
-        col<NF>(R, j, b);
-        col<NDA>(Rd, j, bd);
-        col<NGFA>(Sf, j, s);
-        Phys::flux(a, ad, b, bd, s, d, P, o);
+    for (int j = 0; j < VZ; ++j) {
+      float a[NF], ad[NDA], b[NF], bd[NDA], s[NGFA], o[NF];
+      col<NF>(L, j, a);
+      col<NDA>(Ld, j, ad);
+      col<NF>(R, j, b);
+      col<NDA>(Rd, j, bd);
+      col<NGFA>(Sf, j, s);
+      Phys::flux(a, ad, b, bd, s, d, P, o);
 #pragma unroll
-        for (int f = 0; f < NF; ++f) F[f][j] = o[f];
-      }
+      for (int f = 0; f < NF; ++f) F[f][j] = o[f];
     }
   }
   __device__ static void ghost(const float C[NF][VZ], const float Cd[NDA][VZ], const float Sf[NGFA][VZ], int d,
@@ -161,41 +139,25 @@ template <class Phys, int VZ> struct FaceOps {
   }
   __device__ static void update(const float C[NF][VZ], const float Cd[NDA][VZ], const float G[NGA][VZ],
                                 const float dF[3][NF][VZ], const Params& P, float o[NF][VZ]) {
-    if constexpr (PAIR) {
-      float2 c[NF], cd[NDA], df[3][NF], r[NF];
-      pack<NF>(C, c);
-      pack<NDA>(Cd, cd);
 #pragma unroll
-      for (int d = 0; d < 3; ++d) pack<NF>(dF[d], df[d]);
-      Phys::update2(c, cd, df, P, r);
-      unpack<NF>(r, o);
-    } else {
+    for (int j = 0; j < VZ; ++j) {
+      float c[NF], cd[NDA], gg[NGA], df[3][NF], r[NF];
+      col<NF>(C, j, c);
+      col<NDA>(Cd, j, cd);
+      col<NGA>(G, j, gg);
 #pragma unroll
-      for (int j = 0; j < VZ; ++j) {
-        float c[NF], cd[NDA], gg[NGA], df[3][NF], r[NF];
-        col<NF>(C, j, c);
-        col<NDA>(Cd, j, cd);
-        col<NGA>(G, j, gg);
+      for (int d = 0; d < 3; ++d) col<NF>(dF[d], j, df[d]);
+      Phys::update(c, cd, gg, df, P, r);
 #pragma unroll
-        for (int d = 0; d < 3; ++d) col<NF>(dF[d], j, df[d]);
-        Phys::update(c, cd, gg, df, P, r);
-#pragma unroll
-        for (int f = 0; f < NF; ++f) o[f][j] = r[f];
-      }
+      for (int f = 0; f < NF; ++f) o[f][j] = r[f];
     }
   }
   __device__ static void acc(typename Phys::Acc& a, const float o[NF][VZ], const Params& P) {
-    if constexpr (PAIR) {
-      float2 r[NF];
-      pack<NF>(o, r);
-      Phys::acc_cell2(a, r, P);
-    } else {
 #pragma unroll
-      for (int j = 0; j < VZ; ++j) {
-        float r[NF];
-        col<NF>(o, j, r);
-        Phys::acc_cell(a, r, P);
-      }
+    for (int j = 0; j < VZ; ++j) {
+      float r[NF];
+      col<NF>(o, j, r);
+      Phys::acc_cell(a, r, P);
     }
   }
 };
@@ -379,6 +341,165 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
     }
   };
 
+  typename Phys::Acc acc;
+  Phys::acc_init(acc);
+  const long long plane = (long long)g.Y * g.Z;
+  const bool ylo = y == 0, yhi = y == g.Y - 1;
+  const bool zlo = zb == 0, zhi = zb + VZ - 1 == g.Z - 1;
+
+  if constexpr (Ops::PAIR) {
+    // Paired physics, two cells per thread: the state, derived values and
+    // fluxes of the thread's cells stay (cell 0, cell 1) register pairs from
+    // the 8-byte shared-memory loads to the 8-byte global stores, so the
+    // packed instructions need no repacking.
+    static_assert(NG == 0 && NGF == 0 && ND > 0, "paired face physics: derived values, no per-cell geometry");
+    auto ld2 = [](const float* p) { return *reinterpret_cast<const float2*>(p); };
+    auto load2 = [&](const float* b, int off, float2 v[NF]) {
+#pragma unroll
+      for (int f = 0; f < NF; ++f) v[f] = ld2(b + f * L::TILE + off);
+    };
+    auto loadd2 = [&](const float* b, int off, float2 v[ND]) {
+#pragma unroll
+      for (int e = 0; e < ND; ++e) v[e] = ld2(b + e * L::TILE + off);
+    };
+    auto publish2 = [&](int k, const float2 d[ND]) {
+      float dv[NDA][VZ];
+#pragma unroll
+      for (int e = 0; e < ND; ++e) { dv[e][0] = d[e].x; dv[e][1] = d[e].y; }
+      publish(k, dv);
+    };
+    // one lane (cell j) of a pair as scalars
+    auto lane = [](const float2* v, int n, int j, float* o) {
+      for (int i = 0; i < n; ++i) o[i] = j ? v[i].y : v[i].x;
+    };
+    // the ghosts of both cells across a d face
+    auto ghost2 = [&](const float2 C[NF], const float2 Cd[ND], int d, float2 gq[NF], float2 gd[ND]) {
+      float c[NF], cd[ND], a[NF], ad[ND], b[NF], bd[ND];
+      lane(C, NF, 0, c); lane(Cd, ND, 0, cd);
+      Phys::ghost(c, cd, nullptr, d, a, ad);
+      lane(C, NF, 1, c); lane(Cd, ND, 1, cd);
+      Phys::ghost(c, cd, nullptr, d, b, bd);
+#pragma unroll
+      for (int f = 0; f < NF; ++f) gq[f] = make_float2(a[f], b[f]);
+#pragma unroll
+      for (int e = 0; e < ND; ++e) gd[e] = make_float2(ad[e], bd[e]);
+    };
+    float2 Cd2[ND], fx2[NF];
+    if (x0 > 0) wait_plane(0);
+    wait_plane(1);
+    {
+      float2 C[NF];
+      load2(state(1), cs, C);
+      Phys::derive2(C, Cd2, P);
+      publish2(1, Cd2);
+      if (active) {
+        float2 Q[NF], Qd[ND];
+        if (x0 > 0) {
+          load2(state(0), cs, Q);
+          Phys::derive2(Q, Qd, P);
+        } else {
+          ghost2(C, Cd2, 0, Q, Qd);
+        }
+        Phys::flux2(Q, Qd, C, Cd2, 0, P, fx2);
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      fence_proxy_async();
+      issue(S);
+    }
+    for (int x = x0; x < x1; ++x) {
+      const int k = x - x0 + 1;
+      const bool xhi = x + 1 >= g.X;
+      float2 N[NF], Nd[ND];
+      if (!xhi) {
+        wait_plane(k + 1);
+        load2(state(k + 1), cs, N);
+        Phys::derive2(N, Nd, P);
+        publish2(k + 1, Nd);
+      }
+      if (active) {
+        const float* cq = state(k);
+        const float* db = dbuf(k);
+        float2 C[NF], dF[3][NF];
+        load2(cq, cs, C);
+        {  // x faces: the +x flux of plane k is the -x flux of plane k + 1
+          float2 F[NF];
+          if (!xhi) {
+            Phys::flux2(C, Cd2, N, Nd, 0, P, F);
+          } else {
+            float2 gq[NF], gd[ND];
+            ghost2(C, Cd2, 0, gq, gd);
+            Phys::flux2(C, Cd2, gq, gd, 0, P, F);
+          }
+#pragma unroll
+          for (int f = 0; f < NF; ++f) {
+            dF[0][f] = f2::sub(F[f], fx2[f]);
+            fx2[f] = F[f];
+          }
+        }
+        {  // y faces (walls uniform over the warp)
+          float2 Fp[NF], Fm[NF], R[NF], Rd[ND];
+          if (!yhi) {
+            load2(cq, cs + L::RL, R);
+            loadd2(db, cs + L::RL, Rd);
+          } else {
+            ghost2(C, Cd2, 1, R, Rd);
+          }
+          Phys::flux2(C, Cd2, R, Rd, 1, P, Fp);
+          if (!ylo) {
+            load2(cq, cs - L::RL, R);
+            loadd2(db, cs - L::RL, Rd);
+          } else {
+            ghost2(C, Cd2, 1, R, Rd);
+          }
+          Phys::flux2(R, Rd, C, Cd2, 1, P, Fm);
+#pragma unroll
+          for (int f = 0; f < NF; ++f) dF[1][f] = f2::sub(Fp[f], Fm[f]);
+        }
+        {  // z faces: faces 0 and 1 (left cells zl, cell 0) as a pair, face 2 alone
+          float a[NF], ad[ND], c[NF], cd[ND];
+#pragma unroll
+          for (int f = 0; f < NF; ++f) a[f] = cq[f * L::TILE + cs - 1];
+#pragma unroll
+          for (int e = 0; e < ND; ++e) ad[e] = db[e * L::TILE + cs - 1];
+          lane(C, NF, 0, c);
+          lane(Cd2, ND, 0, cd);
+          across(zlo, c, cd, nullptr, 2, a, ad);
+          float2 Lz[NF], Lzd[ND], F01[NF];
+#pragma unroll
+          for (int f = 0; f < NF; ++f) Lz[f] = make_float2(a[f], C[f].x);
+#pragma unroll
+          for (int e = 0; e < ND; ++e) Lzd[e] = make_float2(ad[e], Cd2[e].x);
+          Phys::flux2(Lz, Lzd, C, Cd2, 2, P, F01);
+          float b[NF], bd[ND], F2[NF];
+#pragma unroll
+          for (int f = 0; f < NF; ++f) b[f] = cq[f * L::TILE + cs + 2];
+#pragma unroll
+          for (int e = 0; e < ND; ++e) bd[e] = db[e * L::TILE + cs + 2];
+          lane(C, NF, 1, c);
+          lane(Cd2, ND, 1, cd);
+          across(zhi, c, cd, nullptr, 2, b, bd);
+          Phys::flux(c, cd, b, bd, nullptr, 2, P, F2);
+#pragma unroll
+          for (int f = 0; f < NF; ++f) dF[2][f] = f2::sub(make_float2(F01[f].y, F2[f]), F01[f]);
+        }
+        float2 res[NF];
+        Phys::update2(C, Cd2, dF, P, res);
+        Phys::acc_cell2(acc, res, P);
+        const long long idx = (long long)x * plane + (long long)y * g.Z + zb;
+#pragma unroll
+        for (int f = 0; f < NF; ++f) *reinterpret_cast<float2*>(out + f * g.n + idx) = res[f];
+      }
+#pragma unroll
+      for (int e = 0; e < ND; ++e) Cd2[e] = Nd[e];
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        fence_proxy_async();
+        issue(k + S);
+      }
+    }
+  } else {
   // the first plane's derived values, and the flux through its -x faces
   float Cd[NDA][VZ] = {};
   float fxm[NF][VZ];
@@ -406,12 +527,6 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
     fence_proxy_async();
     issue(S);
   }
-
-  typename Phys::Acc acc;
-  Phys::acc_init(acc);
-  const long long plane = (long long)g.Y * g.Z;
-  const bool ylo = y == 0, yhi = y == g.Y - 1;
-  const bool zlo = zb == 0, zhi = zb + VZ - 1 == g.Z - 1;
 
   for (int x = x0; x < x1; ++x) {
     const int k = x - x0 + 1;
@@ -544,6 +659,7 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
       issue(k + S);
     }
   }
+  }  // generic path
   if (bad) {
     if (threadIdx.x == 0)
       for (int t = 0; t < S; ++t)
