@@ -92,11 +92,13 @@ def blast(X, Y, Z, seed=7):
     return np.concatenate([rho.ravel(), (rho * u[0]).ravel(), (rho * u[1]).ravel(), (rho * u[2]).ravel(), E.ravel()])
 
 
-@pytest.mark.parametrize("shape", [(24, 20, 36), (16, 9, 68), (12, 33, 8)])
+@pytest.mark.parametrize("shape", [(24, 20, 36), (16, 9, 68), (12, 33, 8), (1, 6, 8), (9, 1, 12), (3, 5, 4)])
 def test_fused_fp32_3d_vs_fp64_oracle(cfdb, oracle, ctx, shape):
     """Structure along x, y and z: exercises the face fluxes of every
     direction, the z faces between a thread's cells and across threads and
-    tiles (32- and 64-wide z tiles, partial tiles), and every wall."""
+    tiles (32- and 64-wide z tiles, partial tiles), and every wall; meshes
+    one cell thick in x or y have both walls of that axis on one cell, and
+    nz = 4 is the smallest z extent of the fused path."""
     X, Y, Z = shape
     U0 = blast(X, Y, Z)
     m = cfdb.Mesh.structured(ctx, X, Y, Z, 1 / X, 1 / Y, 1 / Z)

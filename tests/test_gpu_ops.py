@@ -429,10 +429,11 @@ def _jittered_box(nx, ny, nz, seed):
 
 
 # z extents on both sides of the 32/64-wide tile choice of the face sweep,
-# partial y and z tiles, x shorter than the chunk count; nz = 13 and a c field
-# take the gather form
+# partial y and z tiles, x shorter than the chunk count, meshes one cell thick
+# in x or y and the smallest nz; nz = 13 and a c field take the gather form
 @pytest.mark.parametrize("shape,cfield", [((20, 12, 24), False), ((9, 7, 68), False), ((6, 70, 8), False),
-                                          ((11, 9, 132), False), ((7, 9, 13), False), ((10, 6, 12), True)])
+                                          ((11, 9, 132), False), ((1, 5, 8), False), ((3, 1, 12), False),
+                                          ((2, 3, 4), False), ((7, 9, 13), False), ((10, 6, 12), True)])
 def test_wave_fused_distorted_ragged_vs_fp64_oracle(cfdb, oracle, ctx, shape, cfield):
     nx, ny, nz = shape
     V = _jittered_box(nx, ny, nz, seed=5)
