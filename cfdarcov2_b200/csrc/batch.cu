@@ -70,51 +70,59 @@ __device__ __forceinline__ void column_step(const ProbDev& P, const ItemDev& I, 
   if (col >= n2) return;
   const int y = col / n;
   const int z = col - y * n;
+  // One pointer per field to the column's cell in the current plane,
+  // advanced by a plane per step of the march; the y neighbours sit at a
+  // fixed offset from it (or at the cell itself on a wall) and the z
+  // neighbours at +-1, read unconditionally and replaced by the cell itself
+  // on a wall (the pool keeps spare floats before its first and after its
+  // last problem, so those reads stay inside it).
   const float* q[NF];
   float* o[NF];
 #pragma unroll
-  for (int f = 0; f < NF; ++f) {  // 64-bit bases; all offsets below are 32-bit element offsets
-    q[f] = a + P.offset + f * n3 + col;
-    o[f] = b + P.offset + f * n3 + col;
+  for (int f = 0; f < NF; ++f) {
+    q[f] = a + P.offset + f * n3 + int64_t(I.x0) * n2 + col;
+    o[f] = b + P.offset + f * n3 + int64_t(I.x0) * n2 + col;
   }
-  const int dym = y > 0 ? -n : 0, dyp = y < n - 1 ? n : 0, dzm = z > 0 ? -1 : 0, dzp = z < n - 1 ? 1 : 0;
+  const int dym = y > 0 ? -n : 0, dyp = y < n - 1 ? n : 0;
+  const bool zlo = z == 0, zhi = z == n - 1;
   const float sym = y > 0 ? 1.f : -1.f, syp = y < n - 1 ? 1.f : -1.f;
-  const float szm = z > 0 ? 1.f : -1.f, szp = z < n - 1 ? 1.f : -1.f;
-  int c = I.x0 * n2;
+  const float szm = zlo ? -1.f : 1.f, szp = zhi ? -1.f : 1.f;
   float cur[NF], prv[NF], nxt[NF];
 #pragma unroll
-  for (int f = 0; f < NF; ++f) cur[f] = __ldg(q[f] + c);
+  for (int f = 0; f < NF; ++f) cur[f] = __ldg(q[f]);
   if (I.x0 > 0) {
 #pragma unroll
-    for (int f = 0; f < NF; ++f) prv[f] = __ldg(q[f] + (c - n2));
+    for (int f = 0; f < NF; ++f) prv[f] = __ldg(q[f] - n2);
   } else {
 #pragma unroll
     for (int f = 0; f < NF; ++f) prv[f] = cur[f];
     if constexpr (NF == 4) prv[1] = -cur[1];
   }
-  for (int x = I.x0; x < I.x1; ++x, c += n2) {
-    if (x + 1 < n) {
-      const int cn = c + n2;
+  for (int x = I.x0; x < I.x1; ++x) {
+    const float* qn[NF];
 #pragma unroll
-      for (int f = 0; f < NF; ++f) nxt[f] = __ldg(q[f] + cn);
+    for (int f = 0; f < NF; ++f) qn[f] = q[f] + n2;
+    if (x + 1 < n) {
+#pragma unroll
+      for (int f = 0; f < NF; ++f) nxt[f] = __ldg(qn[f]);
     } else {
 #pragma unroll
       for (int f = 0; f < NF; ++f) nxt[f] = cur[f];
       if constexpr (NF == 4) nxt[1] = -cur[1];
     }
-    const int iym = c + dym, iyp = c + dyp, izm = c + dzm, izp = c + dzp;
     float ym[NF], yp[NF], zm[NF], zp[NF];
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
-      ym[f] = __ldg(q[f] + iym);
-      yp[f] = __ldg(q[f] + iyp);
-      zm[f] = __ldg(q[f] + izm);
-      zp[f] = __ldg(q[f] + izp);
+      ym[f] = __ldg(q[f] + dym);
+      yp[f] = __ldg(q[f] + dyp);
+      const float l = __ldg(q[f] - 1), r = __ldg(q[f] + 1);
+      zm[f] = zlo ? cur[f] : l;
+      zp[f] = zhi ? cur[f] : r;
     }
     if constexpr (NF == 1) {
       const float t = cur[0];
       const float s = ((prv[0] - t) + (nxt[0] - t)) + ((ym[0] - t) + (yp[0] - t)) + ((zm[0] - t) + (zp[0] - t));
-      o[0][c] = t + P.c0 * s;
+      *o[0] = t + P.c0 * s;
     } else {
       ym[2] *= sym;
       yp[2] *= syp;
@@ -127,15 +135,17 @@ __device__ __forceinline__ void column_step(const ProbDev& P, const ItemDev& I, 
 #pragma unroll
       for (int f = 0; f < NF; ++f) s[f] = ((prv[f] + nxt[f]) + (ym[f] + yp[f])) + (zm[f] + zp[f]);
       const float div = ((nxt[1] - prv[1]) + (yp[2] - ym[2])) + (zp[3] - zm[3]);
-      o[0][c] = cur[0] - P.c0 * div + P.c1 * (s[0] - 6.0f * cur[0]);
-      o[1][c] = cur[1] - P.c2 * (nxt[0] - prv[0]) + P.c1 * (s[1] - 6.0f * cur[1]);
-      o[2][c] = cur[2] - P.c2 * (yp[0] - ym[0]) + P.c1 * (s[2] - 6.0f * cur[2]);
-      o[3][c] = cur[3] - P.c2 * (zp[0] - zm[0]) + P.c1 * (s[3] - 6.0f * cur[3]);
+      *o[0] = cur[0] - P.c0 * div + P.c1 * (s[0] - 6.0f * cur[0]);
+      *o[1] = cur[1] - P.c2 * (nxt[0] - prv[0]) + P.c1 * (s[1] - 6.0f * cur[1]);
+      *o[2] = cur[2] - P.c2 * (yp[0] - ym[0]) + P.c1 * (s[2] - 6.0f * cur[2]);
+      *o[3] = cur[3] - P.c2 * (zp[0] - zm[0]) + P.c1 * (s[3] - 6.0f * cur[3]);
     }
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
       prv[f] = cur[f];
       cur[f] = nxt[f];
+      q[f] = qn[f];
+      o[f] += n2;
     }
   }
 }
@@ -382,7 +392,7 @@ __global__ void batch_ring_k(const ProbDev* __restrict__ probs, const ItemDev* _
 
 }  // namespace
 
-constexpr int64_t kPoolPad = 4;  // spare floats at the end of a pool
+constexpr int64_t kPoolPad = 4;  // spare floats before the first and after the last problem of a pool
 // kernel forms (cfdb_batch_set_staged)
 constexpr int kFormMarch = 0, kFormRing = 1, kFormMarch48 = 2;
 
@@ -568,7 +578,7 @@ extern "C" int cfdb_batch_create(cfdb_ctx* ctx, cfdb_problem* probs, int32_t cou
   if (!out) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_batch_create: out is NULL");
   *out = nullptr;
   if (!ctx || !probs || count < 1) return cfdb_fail(ctx, CFDB_EINVAL, "cfdb_batch_create: need a context and >= 1 problem");
-  int64_t off = 0;
+  int64_t off = kPoolPad;  // the column march reads one float before a column's first cell
   for (int32_t i = 0; i < count; ++i) {
     cfdb_problem& p = probs[i];
     if (p.n < 2 || p.n > 1024) return cfdb_fail(ctx, CFDB_EINVAL, "problem %d: n = %d outside [2, 1024]", i, p.n);
@@ -579,7 +589,7 @@ extern "C" int cfdb_batch_create(cfdb_ctx* ctx, cfdb_problem* probs, int32_t cou
     off += int64_t(p.n) * p.n * p.n * (p.kind == 1 ? 4 : 1);
   }
   const int64_t cells = off;
-  off += kPoolPad;  // the staged kernel's copies end on a 16-byte boundary
+  off += kPoolPad;  // the staged kernel's copies end on a 16-byte boundary; the march reads one past
   CFDB_CUDA(ctx, cudaSetDevice(ctx->device));
   auto* b = new (std::nothrow) cfdb_batch();
   if (!b) return cfdb_fail(ctx, CFDB_ENOMEM, "host allocation failed");

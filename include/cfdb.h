@@ -367,8 +367,10 @@ typedef struct {
 } cfdb_problem;
 
 /* probs[i].offset is filled in on return; *pool_elems = elements (of dtype
- * F32) one state pool must hold (the problems' cells plus 4 spare floats at
- * the end, which the staged kernel's 16-byte copies may read). */
+ * F32) one state pool must hold: the problems' cells plus 4 spare floats
+ * before the first problem and 4 after the last (the kernels read, and
+ * discard, one float beyond a column's end and the staged kernel's 16-byte
+ * copies may reach past the last problem). */
 int cfdb_batch_create(cfdb_ctx* ctx, cfdb_problem* probs, int32_t count, int64_t* pool_elems, cfdb_batch** out);
 int cfdb_batch_destroy(cfdb_batch* b);
 /* cells_per_item: cells one CTA work item covers (threads (y, z) columns x
