@@ -150,6 +150,62 @@ __device__ __forceinline__ void column_step(const ProbDev& P, const ItemDev& I, 
   }
 }
 
+// Heat columns carry one field, so a thread marching one column has a
+// single load chain in flight; with two columns per thread (heat items are
+// twice as wide: columns yz0 + t and yz0 + t + blockDim.x) the two marches
+// interleave and twice the loads are in flight.  Same arithmetic per cell.
+__device__ __forceinline__ void heat_columns2(const ProbDev& P, const ItemDev& I, const float* __restrict__ a,
+                                              float* __restrict__ b) {
+  const int n = P.n, n2 = n * n;
+  int colv[2] = {I.yz0 + int(threadIdx.x), I.yz0 + int(threadIdx.x) + int(blockDim.x)};
+  const bool act[2] = {colv[0] < n2, colv[1] < n2};
+  if (!act[0]) return;
+  const float* q[2];
+  float* o[2];
+  int dym[2], dyp[2];
+  bool zlo[2], zhi[2];
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    const int col = act[c] ? colv[c] : colv[0];  // an idle second column shadows the first
+    const int y = col / n, z = col - (col / n) * n;
+    q[c] = a + P.offset + int64_t(I.x0) * n2 + col;
+    o[c] = b + P.offset + int64_t(I.x0) * n2 + col;
+    dym[c] = y > 0 ? -n : 0;
+    dyp[c] = y < n - 1 ? n : 0;
+    zlo[c] = z == 0;
+    zhi[c] = z == n - 1;
+  }
+  float cur[2], prv[2], nxt[2];
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    cur[c] = __ldg(q[c]);
+    prv[c] = I.x0 > 0 ? __ldg(q[c] - n2) : cur[c];
+  }
+  for (int x = I.x0; x < I.x1; ++x) {
+    const float* qn[2] = {q[0] + n2, q[1] + n2};
+    float ym[2], yp[2], zm[2], zp[2];
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      nxt[c] = x + 1 < n ? __ldg(qn[c]) : cur[c];
+      ym[c] = __ldg(q[c] + dym[c]);
+      yp[c] = __ldg(q[c] + dyp[c]);
+      const float l = __ldg(q[c] - 1), r = __ldg(q[c] + 1);
+      zm[c] = zlo[c] ? cur[c] : l;
+      zp[c] = zhi[c] ? cur[c] : r;
+    }
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const float t = cur[c];
+      const float s = ((prv[c] - t) + (nxt[c] - t)) + ((ym[c] - t) + (yp[c] - t)) + ((zm[c] - t) + (zp[c] - t));
+      if (act[c]) *o[c] = t + P.c0 * s;
+      prv[c] = cur[c];
+      cur[c] = nxt[c];
+      q[c] = qn[c];
+      o[c] += n2;
+    }
+  }
+}
+
 // One launch per step walks the work items.  Two register budgets: 64
 // (MINB = 1), or 48 for blocks of up to 256 threads (no spills), where 40
 // warps fit an SM instead of 32 and more plane loads are in flight -- faster
@@ -157,12 +213,13 @@ __device__ __forceinline__ void column_step(const ProbDev& P, const ItemDev& I, 
 // for the mixed heat/wave set, so the tuner picks.
 template <int MAXT, int MINB>
 __global__ void __launch_bounds__(MAXT, MINB) batch_step_k(const ProbDev* __restrict__ probs, const ItemDev* __restrict__ items, int n_items,
-                             const float* __restrict__ a, float* __restrict__ b) {
+                             const float* __restrict__ a, float* __restrict__ b, int heat_cols) {
   for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
     const ItemDev I = items[it];
     const ProbDev P = probs[I.prob];
-    if (P.kind == 0) column_step<1>(P, I, a, b);
-    else column_step<4>(P, I, a, b);
+    if (P.kind == 1) column_step<4>(P, I, a, b);
+    else if (heat_cols == 2) heat_columns2(P, I, a, b);
+    else column_step<1>(P, I, a, b);
   }
 }
 
@@ -407,6 +464,7 @@ struct cfdb_batch {
   int items_cap = 0;
   int cells_per_item = 2048, threads = 256, ctas_per_sm = 4;
   int staged = kFormMarch;  // kernel form (kForm*); the tuner picks the fastest
+  int heat_cols = 1;        // columns per thread of the heat items in the item table (2 for the march forms)
   int ring_resident = 0;          // CTAs of the staged kernel one SM holds
   int64_t ring_resident_key = -1;  // (threads, shared bytes) ring_resident was measured for
   int64_t last_launches = 0;
@@ -422,9 +480,12 @@ int build_items(cfdb_batch* b) {
   // runs of `threads` columns x `planes` x planes, planes = cells_per_item / threads
   std::vector<ItemDev> items;
   const int planes = std::max(1, b->cells_per_item / b->threads);
+  const int heat_cols = b->staged == kFormRing ? 1 : 2;
   for (size_t p = 0; p < b->probs.size(); ++p) {
     const int n = b->probs[p].n;
-    for (int yz0 = 0; yz0 < n * n; yz0 += b->threads)
+    // heat items of the column march cover two columns per thread
+    const int width = b->probs[p].kind == 0 ? heat_cols * b->threads : b->threads;
+    for (int yz0 = 0; yz0 < n * n; yz0 += width)
       for (int x0 = 0; x0 < n; x0 += planes) items.push_back(ItemDev{int32_t(p), yz0, x0, std::min(n, x0 + planes)});
   }
   if (int(items.size()) > b->items_cap) {
@@ -436,6 +497,7 @@ int build_items(cfdb_batch* b) {
   }
   CFDB_CUDA(b->ctx, cudaMemcpy(b->d_items, items.data(), sizeof(ItemDev) * items.size(), cudaMemcpyHostToDevice));
   b->n_items = int(items.size());
+  b->heat_cols = heat_cols;
   return CFDB_OK;
 }
 
@@ -493,10 +555,12 @@ int launch(cfdb_batch* b, const void* a, void* out) {
                                                            b->ctx->d_error);
   } else if (b->staged == kFormMarch48 && b->threads <= 256) {
     batch_step_k<256, 5><<<grid, b->threads, 0, b->ctx->stream>>>(b->d_probs, b->d_items, b->n_items,
-                                                                   static_cast<const float*>(a), static_cast<float*>(out));
+                                                                   static_cast<const float*>(a), static_cast<float*>(out),
+                                                                   b->heat_cols);
   } else {
     batch_step_k<1024, 1><<<grid, b->threads, 0, b->ctx->stream>>>(b->d_probs, b->d_items, b->n_items,
-                                                                    static_cast<const float*>(a), static_cast<float*>(out));
+                                                                    static_cast<const float*>(a), static_cast<float*>(out),
+                                                                    b->heat_cols);
   }
   CFDB_LAUNCHED(b->ctx);
   return CFDB_OK;
@@ -520,7 +584,7 @@ std::string cache_key(const cfdb_batch* b) {
     if (ch == '"' || ch == ' ') ch = '_';
   // "forms": entries of this kernel generation hold the winning form too;
   // entries tuned for an earlier kernel never match
-  snprintf(buf, sizeof(buf), "forms:%s:%d:%016llx", name.c_str(), int(b->probs.size()), (unsigned long long)h);
+  snprintf(buf, sizeof(buf), "forms2:%s:%d:%016llx", name.c_str(), int(b->probs.size()), (unsigned long long)h);
   return buf;
 }
 
@@ -663,9 +727,10 @@ extern "C" int cfdb_batch_set_staged(cfdb_batch* b, int staged) {
   if (!b || !b->ctx) return cfdb_fail(nullptr, CFDB_EINVAL, "cfdb_batch_set_staged: handle is NULL or its context was destroyed");
   if (staged < kFormMarch || staged > kFormMarch48)
     return cfdb_fail(b->ctx, CFDB_EINVAL, "cfdb_batch_set_staged: form %d is not 0, 1 or 2", staged);
+  const bool items_change = (staged == kFormRing) != (b->staged == kFormRing);  // heat item width differs
   b->staged = staged;
   drop_graph(b);
-  return CFDB_OK;
+  return items_change ? build_items(b) : CFDB_OK;
 }
 
 extern "C" int cfdb_batch_get_config(const cfdb_batch* b, int32_t* cells_per_item, int32_t* threads, int32_t* ctas) {
@@ -760,8 +825,9 @@ extern "C" int cfdb_batch_tune(cfdb_batch* b, void* a, void* out, const char* ca
   const std::string key = cache_key(b);
   auto hit = cache.find(key);
   if (hit != cache.end() && hit->second.size() == 4) {
-    b->staged = std::min(std::max(hit->second[3], kFormMarch), kFormMarch48);
-    if (cfdb_batch_set_config(b, hit->second[0], hit->second[1], hit->second[2]) == CFDB_OK) return CFDB_OK;
+    if (cfdb_batch_set_staged(b, std::min(std::max(hit->second[3], kFormMarch), kFormMarch48)) == CFDB_OK &&
+        cfdb_batch_set_config(b, hit->second[0], hit->second[1], hit->second[2]) == CFDB_OK)
+      return CFDB_OK;
   }
   cudaEvent_t e0, e1;
   CFDB_CUDA(ctx, cudaEventCreate(&e0));
@@ -774,7 +840,7 @@ extern "C" int cfdb_batch_tune(cfdb_batch* b, void* a, void* out, const char* ca
   // CTA, so it wants longer items and fewer, larger CTAs (shared memory
   // bounds them), and only configurations it takes are timed.
   for (int form : {kFormMarch, kFormMarch48, kFormRing}) {
-    b->staged = form;
+    if ((rc = cfdb_batch_set_staged(b, form))) break;
     const bool ring = form == kFormRing;
     const std::vector<int> cpis = ring ? std::vector<int>{2048, 8192, 32768, 131072}
                                        : std::vector<int>{512, 1024, 2048, 4096, 8192};
@@ -806,7 +872,7 @@ extern "C" int cfdb_batch_tune(cfdb_batch* b, void* a, void* out, const char* ca
   cudaEventDestroy(e1);
   if (!rc) rc = cfdb_check_device_error(ctx);  // a staged candidate whose wait ran out
   if (rc) return rc;
-  b->staged = bc[3];
+  if ((rc = cfdb_batch_set_staged(b, bc[3]))) return rc;
   if ((rc = cfdb_batch_set_config(b, bc[0], bc[1], bc[2]))) return rc;
   cache[key] = {bc[0], bc[1], bc[2], bc[3]};
   write_cache(cache_path, cache);
