@@ -259,6 +259,14 @@ int fused_heat_step(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, const void* T, void*
   p.cz = float(dt * k / (m->dz * m->dz));
   p.fixed = static_cast<const float*>(fixed);
   if (fixed) return dispatch_padded<HeatPhys<true>>(ctx, m, T, Tn, p);
+  // 128x24 tiles with 4 slots once rows are 128 wide: 768 threads (24 rows
+  // of 32, four z cells each), two CTAs per SM, 8 % y halo: 0.90 of HBM at
+  // 512^3 and 0.94 at 384^3 against 0.71 and 0.75 with 128x8 tiles and 6
+  // slots, the same at 256^3 (128x32: 0.74, 128x16: 0.70, 128x12: 0.78 at
+  // 512^3).  The heat step with the boundary copy keeps its tiles (taller
+  // ones measured slower there: 24 against 21 us per 200^3 step).
+  if (m->nz >= 128)
+    return stencil::launch_sweep<HeatPhys<false>, 128, 24, 4>(ctx, m, T, nullptr, nullptr, Tn, p, 0);
   return dispatch_tz<HeatPhys<false>, 6>(ctx, m, T, Tn, nullptr, p, 0);
 }
 
