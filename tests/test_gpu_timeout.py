@@ -57,3 +57,51 @@ def test_wait_limit_rejects_bad_arguments(cfdb, ctx):
         ctx.set_wait_limit(10)
     with pytest.raises(cfdb.CfdbError):
         ctx.set_wait_limit(1_000_000, missing_plane=-2)
+
+
+@pytest.mark.parametrize("kind", ["distorted", "euler"])
+def test_face_sweep_wait_runs_out_and_context_recovers(cfdb, kind):
+    """The same on the face-flux sweep (its own staging: the ghost plane's
+    geometry copy of a vertex mesh, derived values for Euler): the launch
+    ends by itself, cfdb_sync reports CFDB_ETIMEOUT, and the context then
+    runs the step with the correct result."""
+    ctx = cfdb.Context(0)
+    if kind == "distorted":
+        from cfdarcov2_b200.workloads import jittered_vertices
+        n = 32
+        m = cfdb.Mesh.from_vertices(ctx, n, n, n, 1 / n, 1 / n, 1 / n, jittered_vertices(n, seed=2))
+        q = torch.tensor(np.random.default_rng(13).standard_normal(4 * m.n), dtype=torch.float32, device=DEV)
+
+        def run(out):
+            ctx.wave_step(m, q, out, 0.4 / (3 * n), path=cfdb.FUSED)
+            return out
+    else:
+        from cfdarcov2_b200.workloads import sod_state
+        U0, (dx, dy, dz) = sod_state(64, 8, 8, 1.0, 0.125)
+        m = cfdb.Mesh.structured(ctx, 64, 8, 8, dx, dy, dz)
+        e = cfdb.Euler(ctx, m, dtype=cfdb.F32, path=cfdb.FUSED, gamma=1.4, cfl=0.4, t_end=0.2, max_steps=1000)
+        q = torch.tensor(U0, dtype=torch.float32, device=DEV)
+
+        def run(out):
+            a = q.clone()
+            e.begin(a)
+            for k in range(4):
+                e.step(a, out) if k % 2 == 0 else e.step(out, a)
+            return a
+
+    good = run(torch.empty_like(q)).clone()
+    ctx.sync()
+
+    ctx.set_wait_limit(1_000_000, missing_plane=1)
+    run(torch.zeros_like(q))
+    with pytest.raises(cfdb.CfdbError) as ei:
+        ctx.sync()
+    assert ei.value.code == cfdb.capi.ETIMEOUT
+
+    ctx.set_wait_limit()
+    again = run(torch.empty_like(q)).clone()
+    ctx.sync()
+    assert torch.equal(again, good)
+    if kind == "euler":
+        e.close()
+    ctx.close()
