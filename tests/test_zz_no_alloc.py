@@ -110,3 +110,31 @@ def test_noalloc_total_leaves_free_device_memory_unchanged(cfdb):
     free1, _ = torch.cuda.mem_get_info()
     assert free1 == free0
     assert float(out.item()) == pytest.approx(0.5 * float(f.double().sum()), rel=1e-12)
+
+
+def test_noalloc_total_records_into_a_cuda_graph(cfdb):
+    """After a first call, a call recorded into a CUDA graph (where any device
+    allocation would end the capture with an error) replays with the field's
+    current values."""
+    ctx = cfdb.Context(0)
+    nx, ny, nz = 48, 40, 36
+    dx, dy, dz = 1 / nx, 1 / ny, 1 / nz
+    mesh = cfdb.Mesh.structured(ctx, nx, ny, nz, dx, dy, dz)
+    f = torch.rand(nx * ny * nz, dtype=torch.float32, device="cuda:0")
+    out = torch.empty(1, dtype=torch.float64, device="cuda:0")
+    rc, _ = noalloc_total(cfdb, f, dx * dy * dz, out=out)  # resolves the scratch address
+    assert rc == 0, cfdb.capi.last_error()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        rc, _ = noalloc_total(cfdb, f, dx * dy * dz, out=out)
+    assert rc == 0, cfdb.capi.last_error()
+    for seed in (3, 4):
+        gen = torch.Generator(device="cuda:0").manual_seed(seed)
+        f.copy_(torch.rand(f.numel(), dtype=torch.float32, device="cuda:0", generator=gen) - 0.25)
+        out.fill_(float("nan"))
+        g.replay()
+        torch.cuda.synchronize()
+        assert float(out.item()) == pytest.approx(ctx.total_fp64(mesh, f), rel=1e-14)
+    del g
+    ctx.close()
