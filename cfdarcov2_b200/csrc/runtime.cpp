@@ -276,7 +276,7 @@ int cfdb_check_device_error(cfdb_ctx* ctx) {
   if (!err) return CFDB_OK;
   CFDB_CUDA(ctx, cudaMemsetAsync(ctx->d_error, 0, sizeof(int), ctx->stream));
   switch (err) {
-    case 1: return cfdb_fail(ctx, CFDB_ETIMEOUT, "a bounded device wait gave up (a staged copy never completed)");
+    case 1: return cfdb_fail(ctx, CFDB_ETIMEOUT, "a bounded device wait gave up (a staged copy or a neighbouring cluster's plane never arrived)");
     case 2: return cfdb_fail(ctx, CFDB_ECUDA, "a sweep kernel found its shared memory misaligned for TMA");
     case 3: return cfdb_fail(ctx, CFDB_ECUDA, "a sweep kernel was launched with less shared memory than its layout");
     default: return cfdb_fail(ctx, CFDB_ECUDA, "device error word %d", err);

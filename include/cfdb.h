@@ -115,8 +115,11 @@ int cfdb_ctx_trim(cfdb_ctx* ctx);
  * copies it issued land, and reports CFDB_ETIMEOUT through cfdb_sync; its
  * results are then invalid and the context stays usable.  missing_plane >= 0
  * is a test hook: the first CTA of every later sweep arms that plane's
- * barrier without issuing its copy, so the wait runs out without any fault
- * (-1 turns it off).  Drops the context's cached step graphs.  No reference
+ * barrier without issuing its copy, and the second cluster of the
+ * cluster-resident heat solver (cfdb_heat_run) does not publish its edge
+ * planes of that step, so a wait runs out without any fault (-1 turns it
+ * off).  The resident solver's waits (for a neighbouring cluster's planes)
+ * have the same bound.  Drops the context's cached step graphs.  No reference
  * counterpart: the reference's kernels have no waits, and gpuAssert exits
  * the process on any CUDA error (include/cuda_operators.hpp:29-36). */
 int cfdb_ctx_set_wait_limit(cfdb_ctx* ctx, int64_t cycles, int32_t missing_plane);

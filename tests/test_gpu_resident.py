@@ -1,8 +1,9 @@
 """Cluster-resident heat solver: cfdb_heat_run (fused FP32) on meshes whose
-field fits into one thread-block cluster's shared memory runs all steps in
-one launch.  It must give exactly the per-step TMA sweep's result (the same
-cell update, heat_update(), on the same operands) and match the FP64
-oracle to the fused path's 1e-5 bar.  Which path ran is visible from the
+field fits into the shared memory of one thread-block cluster, or of four
+co-resident clusters that hand their edge planes across through L2, runs
+all steps in one launch.  It must give exactly the per-step TMA sweep's
+result (the same cell update, heat_update(), on the same operands) and
+match the FP64 oracle to the fused path's 1e-5 bar.  Which path ran is visible from the
 buffer that does not hold the result: the resident solver leaves it
 untouched, the per-step ping-pong overwrites it."""
 from __future__ import annotations
@@ -28,7 +29,10 @@ def field(X, Y, Z, seed=1):
 
 
 @pytest.mark.parametrize("shape,steps", [((64, 64, 64), 200), ((64, 64, 64), 37), ((40, 36, 32), 12),
-                                         ((17, 24, 20), 9)])
+                                         ((17, 24, 20), 9),
+                                         # too large for one cluster: four clusters of 16 CTAs (two planes
+                                         # each), and four of 8 CTAs over uneven slabs of one or two planes
+                                         ((128, 64, 64), 23), ((40, 96, 64), 14)])
 def test_resident_equals_per_step_sweep(cfdb, ctx, shape, steps):
     X, Y, Z = shape
     m = cfdb.Mesh.structured(ctx, X, Y, Z, 1 / X, 1 / Y, 1 / Z)

@@ -105,3 +105,36 @@ def test_face_sweep_wait_runs_out_and_context_recovers(cfdb, kind):
     if kind == "euler":
         e.close()
     ctx.close()
+
+
+def test_resident_heat_wait_runs_out_and_context_recovers(cfdb):
+    """The cluster-resident heat solver on several clusters: with the hook
+    one cluster never publishes step 3's edge planes, so its neighbours'
+    bounded waits run out; the launch ends by itself (later waits are
+    skipped), cfdb_sync reports CFDB_ETIMEOUT, and the context then runs the
+    solve with the per-step sweep's result."""
+    ctx = cfdb.Context(0)
+    X, n = 128, 64  # too large for one cluster: four clusters of 16 CTAs, two planes each
+    m = cfdb.Mesh.structured(ctx, X, n, n, 1 / X, 1 / n, 1 / n)
+    T0 = torch.tensor(np.random.default_rng(14).uniform(0, 1, m.n), dtype=torch.float32, device=DEV)
+    k, dt, steps = 0.01, 0.1 / (X * X) / 0.01, 8
+    ref_a, ref_b = T0.clone(), torch.empty_like(T0)
+    p, q = ref_a, ref_b
+    for _ in range(steps):
+        ctx.heat_step(m, p, q, k, dt)
+        p, q = q, p
+    ctx.sync()
+
+    ctx.set_wait_limit(1_000_000, missing_plane=3)
+    a, b = T0.clone(), torch.empty_like(T0)
+    ctx.heat_run(m, a, b, k, dt, steps)
+    with pytest.raises(cfdb.CfdbError) as ei:
+        ctx.sync()
+    assert ei.value.code == cfdb.capi.ETIMEOUT
+
+    ctx.set_wait_limit()
+    a, b = T0.clone(), torch.empty_like(T0)
+    final = ctx.heat_run(m, a, b, k, dt, steps)
+    ctx.sync()
+    assert torch.equal(final, p)
+    ctx.close()
