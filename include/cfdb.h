@@ -318,9 +318,10 @@ int cfdb_wave_step(cfdb_ctx* ctx, cfdb_mesh* mesh, int dtype, int path, const vo
  * graph (after two eager steps that perform any one-time setup) and replays
  * it, so host launch latency never gaps the device.  Asynchronous.
  * cfdb_heat_run, fused FP32: a uniform mesh whose field fits twice into the
- * shared memory of one thread-block cluster (e.g. 64^3) runs all steps in one
- * cluster launch instead, field resident on chip; same arithmetic, same
- * result.  Only the buffer *final_in_b names is defined afterwards. */
+ * shared memory of one thread-block cluster (e.g. 64^3), or else of four
+ * co-resident clusters (e.g. 128 x 64 x 64), runs all steps in one launch
+ * instead, field resident on chip; same arithmetic, same result.  Only the
+ * buffer *final_in_b names is defined afterwards. */
 int cfdb_heat_run(cfdb_ctx* ctx, cfdb_mesh* mesh, int dtype, int path, void* T_a, void* T_b, double k, double dt,
                   int32_t steps, int use_graph, int* final_in_b);
 int cfdb_wave_run(cfdb_ctx* ctx, cfdb_mesh* mesh, int dtype, int path, void* q_a, void* q_b, const void* c_field,
