@@ -31,8 +31,10 @@ def field(X, Y, Z, seed=1):
 @pytest.mark.parametrize("shape,steps", [((64, 64, 64), 200), ((64, 64, 64), 37), ((40, 36, 32), 12),
                                          ((17, 24, 20), 9),
                                          # too large for one cluster: four clusters of 16 CTAs (two planes
-                                         # each), and four of 8 CTAs over uneven slabs of one or two planes
-                                         ((128, 64, 64), 23), ((40, 96, 64), 14)])
+                                         # each), and four of 8 CTAs over uneven slabs of one or two planes;
+                                         # one step (no wait), two (the result overwrites the input)
+                                         ((128, 64, 64), 23), ((40, 96, 64), 14), ((128, 64, 64), 1),
+                                         ((128, 64, 64), 2), ((40, 96, 64), 3)])
 def test_resident_equals_per_step_sweep(cfdb, ctx, shape, steps):
     X, Y, Z = shape
     m = cfdb.Mesh.structured(ctx, X, Y, Z, 1 / X, 1 / Y, 1 / Z)
