@@ -22,6 +22,42 @@ __device__ __forceinline__ void comp_add(double& s, double& c, double x) {
   s = t;
 }
 
+// Folds the per-CTA FP64 partials part[0 .. nblocks) into totals row `step`
+// with every thread of the calling CTA, in a fixed order: thread t takes
+// partials t, t + blockDim, ..., the lanes of each warp merge through
+// shuffles in a fixed pattern and thread 0 merges the warps in order, so the
+// totals do not depend on timing (one thread folding every partial serially
+// had cost ~13 us per step).
+__device__ void fold_partials(const Comp2* __restrict__ part, int nblocks, double* totals, long long step) {
+  __shared__ double sh[32][4];
+  double S0 = 0, C0 = 0, S1 = 0, C1 = 0;
+  for (int k = int(threadIdx.x); k < nblocks; k += int(blockDim.x)) {
+    const Comp2 q = part[k];
+    comp_add(S0, C0, q.s0); C0 += q.c0;
+    comp_add(S1, C1, q.s1); C1 += q.c1;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double a0 = __shfl_xor_sync(0xffffffffu, S0, o), b0 = __shfl_xor_sync(0xffffffffu, C0, o);
+    const double a1 = __shfl_xor_sync(0xffffffffu, S1, o), b1 = __shfl_xor_sync(0xffffffffu, C1, o);
+    comp_add(S0, C0, a0); C0 += b0;
+    comp_add(S1, C1, a1); C1 += b1;
+  }
+  const int w = int(threadIdx.x) >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    sh[w][0] = S0; sh[w][1] = C0; sh[w][2] = S1; sh[w][3] = C1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    S0 = C0 = S1 = C1 = 0;
+    for (int k = 0; k < int(blockDim.x / 32); ++k) {
+      comp_add(S0, C0, sh[k][0]); C0 += sh[k][1];
+      comp_add(S1, C1, sh[k][2]); C1 += sh[k][3];
+    }
+    totals[2 * step] = S0 + C0;
+    totals[2 * step + 1] = S1 + C1;
+  }
+}
+
 struct EulerPhys {
   static constexpr int NF = 5;
   static constexpr int MIN_BLOCKS = 2;  // 64x8 tile, 2 cells per thread: 256 threads at <= 128 registers
@@ -33,7 +69,8 @@ struct EulerPhys {
     double dx, dy, dz, cfl, t_end, vconst;
     EulerClock* clock;
     double* totals;
-    Comp2* part;
+    Comp2* part;      // two buffers of part_stride partials, launch s writes buffer s % 2
+    int part_stride;
     long long s;
     long long max_steps;
   };
@@ -46,14 +83,20 @@ struct EulerPhys {
     return blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0;
   }
 
+  // The clock of the new state is written when the step starts (it needs
+  // only dt); the totals of the previous launch's state are folded by this
+  // launch's first CTA while its first planes are in flight (prologue), or
+  // here when nothing is left to step.
   __device__ static bool begin(Params& p) {
     EulerClock* ck = p.clock;
     const int ts = int(p.s & 1);
     if (ck->finished[ts]) {
+      fold_previous(p);
       if (first_thread()) {
         ck->t[ts ^ 1] = ck->t[ts];
         ck->steps[ts ^ 1] = ck->steps[ts];
         ck->finished[ts ^ 1] = 1;
+        ck->pending[ts] = 0;
       }
       return false;
     }
@@ -65,10 +108,29 @@ struct EulerPhys {
     const double lam[3] = {bits_to_double(ck->lam[ls][0]), bits_to_double(ck->lam[ls][1]),
                            bits_to_double(ck->lam[ls][2])};
     bool last;
-    p.dt = float(euler_dt(lam, p.dx, p.dy, p.dz, p.cfl, ck->t[ts], p.t_end, &last));
+    const double t = ck->t[ts];
+    const double dt = euler_dt(lam, p.dx, p.dy, p.dz, p.cfl, t, p.t_end, &last);
+    p.dt = float(dt);
     for (int d = 0; d < 3; ++d) p.kd[d] = p.dt * p.ih[d];
+    if (first_thread()) {
+      const long long step = ck->steps[ts] + 1;
+      ck->t[ts ^ 1] = last ? p.t_end : t + dt;
+      ck->steps[ts ^ 1] = step;
+      ck->finished[ts ^ 1] = (last || !(t + dt < p.t_end) || step >= p.max_steps) ? 1 : 0;
+      ck->pending[ts] = step;
+    }
     return true;
   }
+  // The first CTA folds the partials the previous launch left (if it
+  // stepped) into that step's totals row.
+  __device__ static void fold_previous(const Params& p) {
+    if (blockIdx.x != 0 || blockIdx.y != 0 || p.s < 1) return;
+    const int prev = int((p.s - 1) & 1);
+    const long long step = p.clock->pending[prev];
+    if (step <= 0) return;
+    fold_partials(p.part + size_t(prev) * size_t(p.part_stride), int(gridDim.x * gridDim.y), p.totals, step);
+  }
+  __device__ static void prologue(const Params& p) { fold_previous(p); }
 
 
   // 1/rho and the sound speed with the approximate reciprocal and square
@@ -195,7 +257,6 @@ struct EulerPhys {
   __device__ static void finish(Acc& s, const Params& a, bool) {
     __shared__ double sh[32][4];
     __shared__ float shl[32][3];
-    __shared__ bool is_last;
     s.s0 *= a.vconst;
     s.s1 *= a.vconst;
     for (int o = 16; o > 0; o >>= 1) {
@@ -214,7 +275,6 @@ struct EulerPhys {
     }
     __syncthreads();
     EulerClock* ck = a.clock;
-    const unsigned nblocks = gridDim.x * gridDim.y;
     const unsigned bid = blockIdx.y * gridDim.x + blockIdx.x;
     if (threadIdx.x == 0) {
       double S0 = 0, C0 = 0, S1 = 0, C1 = 0;
@@ -224,63 +284,23 @@ struct EulerPhys {
         comp_add(S1, C1, sh[k][2]); C1 += sh[k][3];
         L0 = fmaxf(L0, shl[k][0]); L1 = fmaxf(L1, shl[k][1]); L2 = fmaxf(L2, shl[k][2]);
       }
-      a.part[bid] = Comp2{S0, C0, S1, C1};
+      a.part[size_t(a.s & 1) * size_t(a.part_stride) + bid] = Comp2{S0, C0, S1, C1};
       const int target = int((a.s + 1) % 3);
       atomicMax(&ck->lam[target][0], (unsigned long long)__double_as_longlong(double(L0)));
       atomicMax(&ck->lam[target][1], (unsigned long long)__double_as_longlong(double(L1)));
       atomicMax(&ck->lam[target][2], (unsigned long long)__double_as_longlong(double(L2)));
-      __threadfence();
-      is_last = atomicAdd(&ck->counter, 1u) == nblocks - 1;
-    }
-    __syncthreads();
-    // The last CTA folds the per-CTA partials with all its threads: thread t
-    // takes partials t, t + blockDim, ... in order, the lanes of each warp
-    // merge through shuffles in a fixed pattern and thread 0 merges the warps
-    // in order, so the totals do not depend on timing.  (One thread folding
-    // every partial serially kept all other SMs waiting for ~13 us per step;
-    // one warp, ~10 dependent loads per lane.)
-    if (is_last) {
-      __threadfence();
-      double S0 = 0, C0 = 0, S1 = 0, C1 = 0;
-      for (unsigned k = threadIdx.x; k < nblocks; k += blockDim.x) {
-        const Comp2 q = a.part[k];
-        comp_add(S0, C0, q.s0); C0 += q.c0;
-        comp_add(S1, C1, q.s1); C1 += q.c1;
-      }
-      for (int o = 16; o > 0; o >>= 1) {
-        const double a0 = __shfl_xor_sync(0xffffffffu, S0, o), b0 = __shfl_xor_sync(0xffffffffu, C0, o);
-        const double a1 = __shfl_xor_sync(0xffffffffu, S1, o), b1 = __shfl_xor_sync(0xffffffffu, C1, o);
-        comp_add(S0, C0, a0); C0 += b0;
-        comp_add(S1, C1, a1); C1 += b1;
-      }
-      if ((threadIdx.x & 31) == 0) {
-        sh[w][0] = S0; sh[w][1] = C0; sh[w][2] = S1; sh[w][3] = C1;
-      }
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        S0 = C0 = S1 = C1 = 0;
-        for (int k = 0; k < int(blockDim.x / 32); ++k) {
-          comp_add(S0, C0, sh[k][0]); C0 += sh[k][1];
-          comp_add(S1, C1, sh[k][2]); C1 += sh[k][3];
-        }
-        ck->counter = 0;
-        const int ts = int(a.s & 1);
-        const int ls = int(a.s % 3);
-        const double lam[3] = {bits_to_double(ck->lam[ls][0]), bits_to_double(ck->lam[ls][1]),
-                               bits_to_double(ck->lam[ls][2])};
-        bool last;
-        const double t = ck->t[ts];
-        const double dt = euler_dt(lam, a.dx, a.dy, a.dz, a.cfl, t, a.t_end, &last);
-        const long long step = ck->steps[ts] + 1;
-        ck->t[ts ^ 1] = last ? a.t_end : t + dt;
-        ck->steps[ts ^ 1] = step;
-        ck->finished[ts ^ 1] = (last || !(t + dt < a.t_end) || step >= a.max_steps) ? 1 : 0;
-        a.totals[2 * step] = S0 + C0;
-        a.totals[2 * step + 1] = S1 + C1;
-      }
     }
   }
 };
+
+// The fold of the partials the last launch left, for a reader of the totals
+// after the last step (cfdb_euler_totals, the run loop's health check).
+__global__ void euler_fold_k(EulerClock* ck, const Comp2* __restrict__ part, int stride, int nblocks,
+                             double* totals, int prev) {
+  const long long step = ck->pending[prev];
+  if (step <= 0) return;
+  fold_partials(part + size_t(prev) * size_t(stride), nblocks, totals, step);
+}
 
 constexpr int kEulerCtasPerSm = 2;
 constexpr int kEulerVZ = 2;
@@ -299,8 +319,16 @@ int launch_euler(cfdb_euler* e, const void* U, void* Un, int64_t s) {
   p.clock = e->clock; p.totals = e->totals; p.part = e->part;
   p.s = (long long)s;
   p.max_steps = (long long)e->max_steps;
+  p.part_stride = e->part_cap;
   const stencil::PaddedGeom none{nullptr, 0, 0, 0, 0};
-  return stencil::launch_face_sweep<EulerPhys, TZ, 8, 4, kEulerVZ>(e->ctx, m, U, none, Un, p, kEulerCtasPerSm);
+  int grid = 0;
+  const int rc =
+      stencil::launch_face_sweep<EulerPhys, TZ, 8, 4, kEulerVZ>(e->ctx, m, U, none, Un, p, kEulerCtasPerSm, &grid);
+  if (rc) return rc;
+  if (grid > e->part_cap) return cfdb_fail(e->ctx, CFDB_ECUDA, "fused Euler grid %d beyond its %d partials", grid, e->part_cap);
+  e->fused_grid = grid;
+  e->fused_threads = (TZ / kEulerVZ) * 8;
+  return CFDB_OK;
 }
 
 int tz_for(const cfdb_mesh* m) { return m->nz >= 64 ? 64 : 32; }
@@ -313,6 +341,18 @@ int euler_fused_grid(const cfdb_euler* e) {
   const int tz = tz_for(e->mesh);
   const stencil::SweepShape sh = stencil::sweep_shape(e->ctx, e->mesh, tz, 8, kEulerCtasPerSm);
   return sh.tiles * sh.chunks;
+}
+
+// Folds the partials the last fused launch left into its totals row (a
+// no-op when that launch already had its totals folded by a later one, or
+// did not step).
+int euler_fold_pending(cfdb_euler* e) {
+  if (e->path != CFDB_PATH_FUSED || e->launches < 1 || e->fused_grid < 1) return CFDB_OK;
+  const int prev = int((e->launches - 1) & 1);
+  euler_fold_k<<<1, e->fused_threads, 0, e->ctx->stream>>>(e->clock, e->part, e->part_cap, e->fused_grid, e->totals,
+                                                          prev);
+  CFDB_LAUNCHED(e->ctx);
+  return CFDB_OK;
 }
 
 int euler_fused_step(cfdb_euler* e, const void* U, void* Un, int64_t s) {
@@ -348,7 +388,7 @@ extern "C" int cfdb_euler_create(cfdb_ctx* ctx, cfdb_mesh* m, int dtype, int pat
   e->part_cap = grid;
   int rc = cfdb_dev_alloc(ctx, sizeof(EulerClock), reinterpret_cast<void**>(&e->clock));
   if (!rc) rc = cfdb_dev_alloc(ctx, int64_t(sizeof(double)) * 2 * (max_steps + 1), reinterpret_cast<void**>(&e->totals));
-  if (!rc) rc = cfdb_dev_alloc(ctx, int64_t(sizeof(Comp2)) * grid, reinterpret_cast<void**>(&e->part));
+  if (!rc) rc = cfdb_dev_alloc(ctx, int64_t(sizeof(Comp2)) * grid * 2, reinterpret_cast<void**>(&e->part));
   if (rc) {
     cfdb_euler_destroy(e);
     return rc;
@@ -411,6 +451,7 @@ extern "C" int cfdb_euler_totals(cfdb_euler* e, double* out, int64_t max_rows, i
   if (!e || !e->ctx || !out || max_rows < 0)
     return cfdb_fail(e ? e->ctx : nullptr, CFDB_EINVAL, "cfdb_euler_totals: bad arguments");
   int64_t steps = 0;
+  if (int rc = euler_fold_pending(e)) return rc;
   if (int rc = cfdb_euler_status(e, nullptr, &steps, nullptr)) return rc;
   const int64_t n = std::min<int64_t>(steps + 1, max_rows);
   if (n > 0) CFDB_CUDA(e->ctx, cudaMemcpy(out, e->totals, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost));
@@ -432,6 +473,7 @@ extern "C" int cfdb_euler_run(cfdb_euler* e, void* Ua, void* Ub, int64_t check_e
       const bool even = (e->launches & 1) == 0;
       if (int rc = cfdb_euler_step(e, even ? Ua : Ub, even ? Ub : Ua)) return rc;
     }
+    if (int rc = euler_fold_pending(e)) return rc;
     if (int rc = cfdb_euler_status(e, nullptr, &steps, &finished)) return rc;
     // the conservation totals of the latest step double as the health check:
     // a NaN or Inf anywhere in the state reaches them (and would otherwise

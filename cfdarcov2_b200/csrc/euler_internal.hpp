@@ -5,11 +5,15 @@
 // slot s%3 (the state it advances), computes
 //   dt = cfl / (lam_x/dx + lam_y/dy + lam_z/dz), clipped onto t_end,
 // writes the speeds of the new state into ring slot (s+1)%3 and zeroes slot
-// (s+2)%3 for launch s+1; the last CTA to finish advances the clock into slot
-// (s+1)%2 and writes the FP64 Neumaier totals of the new state.  Once t_end is
-// reached every further launch only copies the clock forward, so the host can
-// enqueue steps without reading dt back (the reference syncs and copies a
-// scalar every step, src/fvm3d.cpp:641-662, src/cuda_operators.cu:184-189).
+// (s+2)%3 for launch s+1, and advances the clock into slot (s+1)%2.  The
+// FP64 Neumaier totals of the new state: the plain path's reduction launch
+// folds them itself (its last CTA); a fused launch leaves per-CTA partials
+// (buffer s%2) and records its step in pending[s%2], and the next launch, or
+// cfdb_euler_fold before the host reads the totals, folds them, so no launch
+// ends waiting for a fold.  Once t_end is reached every further launch only
+// copies the clock forward, so the host can enqueue steps without reading dt
+// back (the reference syncs and copies a scalar every step,
+// src/fvm3d.cpp:641-662, src/cuda_operators.cu:184-189).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -23,8 +27,9 @@ struct EulerClock {
   unsigned long long lam[3][3];  // non-negative doubles as ordered bit patterns
   long long steps[2];
   int finished[2];
-  unsigned int counter;  // last-CTA counter, reset by the last CTA
+  unsigned int counter;  // last-CTA counter of the plain path's reduction, reset by the last CTA
   int pad;
+  long long pending[2];  // fused launch s: the step whose partials (buffer s%2) are not folded yet, 0 for none
 };
 
 // Neumaier pair, two fields (rho, E).
@@ -41,8 +46,10 @@ struct cfdb_euler {
   int64_t max_steps = 0;
   EulerClock* clock = nullptr;
   double* totals = nullptr;  // 2 * (max_steps + 1)
-  Comp2* part = nullptr;     // per-CTA partials
+  Comp2* part = nullptr;     // per-CTA partials: two buffers of part_cap (the fused path alternates them)
   int part_cap = 0;
+  int fused_grid = 0;     // CTAs of the last fused launch (the partials it left)
+  int fused_threads = 0;  // and their size (the fold runs in the same order)
   int64_t launches = 0;
 };
 

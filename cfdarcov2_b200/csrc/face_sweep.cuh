@@ -54,6 +54,8 @@
 //                                 const float dF[3][NF], const Params&, float out[NF]);  dF[d] = F(d+) - F(d-)
 //   __device__ static void acc_init(Acc&), acc_cell(Acc&, const float out[NF], const Params&),
 //                          finish(Acc&, const Params&, bool thread_active);
+//   optionally __device__ static void prologue(const Params&), called by every thread once the
+//   first planes' copies are issued (work that needs no plane, hidden behind their latency);
 // (array extents of size 0 are passed as 1), and optionally, with two cells
 // per thread (VZ == 2), the same operations on (cell 0, cell 1) pairs
 // (Phys::PAIRED; derived values, no per-cell geometry), which the physics
@@ -79,6 +81,8 @@ struct PaddedGeom {
 
 template <class P, class = void> struct face_paired { static constexpr bool value = false; };
 template <class P> struct face_paired<P, decltype(void(P::PAIRED))> { static constexpr bool value = P::PAIRED; };
+template <class P, class = void> struct face_prologue { static constexpr bool value = false; };
+template <class P> struct face_prologue<P, decltype(void(&P::prologue))> { static constexpr bool value = true; };
 
 // The physics operations on a thread's VZ cells ([field][cell] arrays), as
 // loops over the cells.  Paired physics (PAIR) run a path of their own in the
@@ -254,6 +258,9 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
   };
   if (threadIdx.x == 0)
     for (int k = 0; k < S; ++k) issue(k);
+  // work of the physics that needs no plane, done while the first planes are
+  // in flight (every thread of every CTA calls it)
+  if constexpr (face_prologue<Phys>::value) Phys::prologue(P);
 
   uint32_t parity = 0;
   auto wait_plane = [&](int k) {
