@@ -222,7 +222,6 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
     }
   }
   typename Phys::Params P = prm;
-  if (!Phys::begin(P)) return;
 
   const int tz = threadIdx.x % (TZ / VZ);
   const int ty = threadIdx.x / (TZ / VZ);
@@ -256,8 +255,22 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
     if (x >= 0) tma_load_4d(dst, &tm_q, z0 - 4, y0 - 1, x, 0, &bars[s]);
     if constexpr (NG > 0) tma_load_4d(dst + L::G_OFF, &tm_g, z0, y0, x + 1, 0, &bars[s]);
   };
+  uint32_t first_issued = 0;  // thread 0: the slots of the first planes actually issued
   if (threadIdx.x == 0)
-    for (int k = 0; k < S; ++k) issue(k);
+    for (int k = 0; k < S; ++k) {
+      const int before = last_issued;
+      issue(k);
+      if (last_issued != before) first_issued |= 1u << k;
+    }
+  // The physics' per-launch set-up (reads of device state such as a clock)
+  // runs while the first planes are in flight; a launch with nothing to do
+  // lets the copies it issued land before it exits.
+  if (!Phys::begin(P)) {
+    if (threadIdx.x == 0)
+      for (int k = 0; k < S; ++k)
+        if ((first_issued >> k) & 1u) mbar_wait_bounded(&bars[k], 0u, g.wait_cycles);
+    return;
+  }
   // work of the physics that needs no plane, done while the first planes are
   // in flight (every thread of every CTA calls it)
   if constexpr (face_prologue<Phys>::value) Phys::prologue(P);
