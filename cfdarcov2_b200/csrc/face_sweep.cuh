@@ -207,6 +207,18 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
   const int x0 = int((long long)blockIdx.y * g.X / g.chunks);
   const int x1 = int((long long)(blockIdx.y + 1) * g.X / g.chunks);
   if (x0 >= x1) return;
+  // Set-up that touches no global memory runs before the wait for the
+  // previous kernel, overlapping its last CTAs: the ring's barriers and the
+  // tensor maps' descriptors.
+  if (threadIdx.x == 0) {
+    prefetch_tmap(&tm_q);
+    if constexpr (NG > 0) prefetch_tmap(&tm_g);
+    for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+    fence_mbar_init();
+    last_issued = -1;
+    drain = 0;
+  }
+  __syncthreads();
   grid_dep_wait();
   grid_dep_launch();
   if (smem_u32(smem) & 127u) {
@@ -229,14 +241,6 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
   const int zb = z0 + VZ * tz;
   const bool active = (y < g.Y) && (zb < g.Z);
   const int kmax = x1 - x0 + 1;  // plane k <-> x = x0 - 1 + k
-
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
-    fence_mbar_init();
-    last_issued = -1;
-    drain = 0;
-  }
-  __syncthreads();
 
   // A wait that gives up ends the staging exactly as in the stencil sweep:
   // nothing more is issued, later waits are skipped, the copies in flight are

@@ -31,6 +31,11 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
 __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+// Brings a tensor map (a __grid_constant__ kernel parameter) into the TMA
+// unit's descriptor cache ahead of its first copy.
+__device__ __forceinline__ void prefetch_tmap(const CUtensorMap* m) {
+  asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(m)) : "memory");
+}
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
@@ -228,6 +233,19 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
   const int x0 = int((long long)blockIdx.y * g.X / g.chunks);
   const int x1 = int((long long)(blockIdx.y + 1) * g.X / g.chunks);
   if (x0 >= x1) return;
+  // Set-up that touches no global memory runs before the wait for the
+  // previous kernel, overlapping its last CTAs: the ring's barriers and the
+  // tensor maps' descriptors.
+  if (threadIdx.x == 0) {
+    prefetch_tmap(&tm_q);
+    if constexpr (NA > 0) prefetch_tmap(&tm_a);
+    if constexpr (Phys::HAS_C) prefetch_tmap(&tm_c);
+    for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+    fence_mbar_init();
+    last_issued = -1;
+    drain = 0;
+  }
+  __syncthreads();
   grid_dep_wait();
   grid_dep_launch();
   if (smem_u32(smem) & 127u) {
@@ -252,14 +270,6 @@ __global__ void __launch_bounds__((TZ / VZ) * TY, Phys::MIN_BLOCKS)
   const int zb = z0 + VZ * tz;
   const bool active = (y < g.Y) && (zb < g.Z);
   const int kmax = x1 - x0 + 1;  // plane k <-> x = x0 - 1 + k
-
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
-    fence_mbar_init();
-    last_issued = -1;
-    drain = 0;
-  }
-  __syncthreads();
 
   // A wait that gives up (bad) ends the staging: the issuing thread (0)
   // issues nothing more and lets the copies it already issued land before
