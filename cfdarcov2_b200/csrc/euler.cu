@@ -136,10 +136,14 @@ struct EulerPhys {
   // 1/rho and the sound speed with the approximate reciprocal and square
   // root of the SFU (relative error ~1e-7, far inside the FP32 solver's
   // 1e-5 error bar against FP64; the FP64 path keeps IEEE division).
-  __device__ static float fast_rcp(float x) { return __fdividef(1.0f, x); }
+  __device__ static float fast_rcp(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+  }
   __device__ static float fast_sqrt(float x) {
     float r;
-    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
     return r;
   }
 
