@@ -109,10 +109,12 @@ struct DistFacePhys {
   };
   struct Acc {};
   // |S| of a face: the PTX approximate square root (relative error ~2^-22,
-  // far inside the FP32 path's 1e-5 bar) instead of the IEEE sequence
+  // far inside the FP32 path's 1e-5 bar) instead of the IEEE sequence, in
+  // its flush-to-zero form (no subnormal handling: |S|^2 of any face longer
+  // than ~1e-9 is far above FP32's smallest normal)
   __device__ static float fast_sqrt(float x) {
     float r;
-    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
     return r;
   }
   __device__ static bool begin(Params&) { return true; }
