@@ -591,7 +591,7 @@ def bench_wave_distorted(ctx, cfdb, dev, flush, S, n=128, tsteps=None):
                                f"{n}^3 jittered wave, 2 steps, FP32 operator-by-operator"))
     m.close()
     return _line(S, f"wave3d_rusanov_{n}^3_x{T}_steps_jittered_0.2dx", res["fp32_fused"][0], res["fp32_fused"][1],
-                 {"mesh": [n] * 3, "jitter": "U(-0.2,0.2) dx, seed 2", "path": "compact area-vector gather"}, 72,
+                 {"mesh": [n] * 3, "jitter": "U(-0.2,0.2) dx, seed 2", "path": "face-flux TMA sweep, padded area-vector geometry"}, 72,
                  n ** 3, T, extra, launches=res["fp32_fused"][3],
                  traffic_profile="distorted_sweep_128.txt" if n == 128 else None)
 
