@@ -22,6 +22,21 @@ struct CompactArgs {
   long long n;
 };
 
+// Approximate (SFU) square root and reciprocal in their flush-to-zero
+// forms: |S| and 1/|S|^2 of faces, which are never subnormal; the IEEE
+// sequences would add fix-up paths, and the division a slow path for
+// subnormal numerators (the far tails of a smooth pulse).
+__device__ __forceinline__ float face_sqrt(float x) {
+  float r;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float face_rcp(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 __global__ void __launch_bounds__(kThreads)
     compact_wave_k(CompactArgs g, const float* __restrict__ q, float* __restrict__ qn, const float* __restrict__ cf,
                    float cconst, int mode, float dt) {
@@ -58,14 +73,15 @@ __global__ void __launch_bounds__(kThreads)
           const long long pj = pi - pstride[d];
           Sx = -g.S[(3 * d + 0) * g.np + pj]; Sy = -g.S[(3 * d + 1) * g.np + pj]; Sz = -g.S[(3 * d + 2) * g.np + pj];
         }
-        const float A = sqrtf(Sx * Sx + Sy * Sy + Sz * Sz);
+        const float S2 = Sx * Sx + Sy * Sy + Sz * Sz;
+        const float A = face_sqrt(S2);
         const float unPA = uP * Sx + vP * Sy + wP * Sz;
         float pN, uN, vN, wN, cN;
         if (!wall) {
           pN = q[j]; uN = q[n + j]; vN = q[2 * n + j]; wN = q[3 * n + j];
           cN = cf ? cf[j] : cconst;
         } else {
-          const float k2 = 2.f * unPA / (A * A);  // reflect about the unit normal S/A
+          const float k2 = 2.f * unPA * face_rcp(S2);  // reflect about the unit normal S/A
           pN = pP; uN = uP - k2 * Sx; vN = vP - k2 * Sy; wN = wP - k2 * Sz; cN = cP;
         }
         const float unNA = uN * Sx + vN * Sy + wN * Sz;
@@ -109,19 +125,10 @@ struct DistFacePhys {
   };
   struct Acc {};
   // |S| of a face: the PTX approximate square root (relative error ~2^-22,
-  // far inside the FP32 path's 1e-5 bar) instead of the IEEE sequence, in
-  // its flush-to-zero form (no subnormal handling: |S|^2 of any face longer
-  // than ~1e-9 is far above FP32's smallest normal)
-  __device__ static float fast_sqrt(float x) {
-    float r;
-    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return r;
-  }
-  __device__ static float fast_rcp(float x) {
-    float r;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return r;
-  }
+  // far inside the FP32 path's 1e-5 bar) in its flush-to-zero form (|S|^2 of
+  // any face longer than ~1e-9 is far above FP32's smallest normal)
+  __device__ static float fast_sqrt(float x) { return face_sqrt(x); }
+  __device__ static float fast_rcp(float x) { return face_rcp(x); }
   __device__ static bool begin(Params&) { return true; }
   __device__ static void flux(const float L[NF], const float*, const float R[NF], const float*, const float S[NGF],
                               int, const Params& a, float F[NF]) {
